@@ -1,0 +1,337 @@
+// ORACLE — test infrastructure only. C entry points over the CPU restatement,
+// loaded by the tests (ctypes) as the checker for the GPU backend. Buffers the
+// oracle returns are malloc'ed and released with orc_free.
+#include <cstdlib>
+#include <cstring>
+#include <exception>
+#include <vector>
+
+#include "pipeline.hpp"
+#include "stark.hpp"
+
+using namespace orc;
+
+namespace {
+uint8_t* dupBytes(const std::vector<uint8_t>& v, size_t* out_len) {
+  uint8_t* p = (uint8_t*)std::malloc(v.empty() ? 1 : v.size());
+  if (!v.empty()) std::memcpy(p, v.data(), v.size());
+  *out_len = v.size();
+  return p;
+}
+QM31 q4(const uint32_t* w) { return QM31::make(w[0], w[1], w[2], w[3]); }
+void put4(const QM31& v, uint32_t* w) {
+  w[0] = v.a.c0.v;
+  w[1] = v.a.c1.v;
+  w[2] = v.b.c0.v;
+  w[3] = v.b.c1.v;
+}
+}  // namespace
+
+extern "C" {
+
+void orc_free(void* p) { std::free(p); }
+
+void orc_blake3(const uint8_t* msg, size_t len, uint8_t* out32) { blake3Hash(msg, len, out32); }
+
+void orc_hash2(const uint8_t* a, const uint8_t* b, uint8_t* out32) {
+  Digest x, y;
+  std::memcpy(x.data(), a, 32);
+  std::memcpy(y.data(), b, 32);
+  Digest d = hash2(x, y);
+  std::memcpy(out32, d.data(), 32);
+}
+
+void orc_hash_qm31(const uint32_t* v, size_t n, uint8_t* out) {
+  for (size_t i = 0; i < n; ++i) {
+    Digest d = hashQM31(q4(v + 4 * i));
+    std::memcpy(out + 32 * i, d.data(), 32);
+  }
+}
+
+// Row leaves: values laid out row-major (n_rows x n_cols).
+void orc_hash_m31_rows(const uint32_t* v, size_t n_rows, size_t n_cols, uint8_t* out) {
+  std::vector<M31> row(n_cols);
+  for (size_t r = 0; r < n_rows; ++r) {
+    for (size_t c = 0; c < n_cols; ++c) row[c] = M31(v[r * n_cols + c]);
+    Digest d = hashM31s(row.data(), n_cols);
+    std::memcpy(out + 32 * r, d.data(), 32);
+  }
+}
+
+// op: 0 add, 1 sub, 2 mul, 3 neg, 4 inv
+void orc_m31_op(int op, const uint32_t* a, const uint32_t* b, uint32_t* out, size_t n) {
+  for (size_t i = 0; i < n; ++i) {
+    M31 x(a[i]), y(b ? b[i] : 0);
+    M31 r;
+    switch (op) {
+      case 0: r = x.add(y); break;
+      case 1: r = x.sub(y); break;
+      case 2: r = x.mul(y); break;
+      case 3: r = x.neg(); break;
+      default: r = x.inv(); break;
+    }
+    out[i] = r.v;
+  }
+}
+
+void orc_qm31_op(int op, const uint32_t* a, const uint32_t* b, uint32_t* out, size_t n) {
+  for (size_t i = 0; i < n; ++i) {
+    QM31 x = q4(a + 4 * i), y = b ? q4(b + 4 * i) : QM31::zero();
+    QM31 r;
+    switch (op) {
+      case 0: r = x.add(y); break;
+      case 1: r = x.sub(y); break;
+      case 2: r = x.mul(y); break;
+      case 3: r = x.neg(); break;
+      default: r = x.inv(); break;
+    }
+    put4(r, out + 4 * i);
+  }
+}
+
+void orc_qm31_pow(const uint32_t* a, uint64_t e, uint32_t* out) { put4(q4(a).pow(e), out); }
+void orc_qm31_root(unsigned log_size, uint32_t* out) { put4(QM31::primitiveRootOfUnity(log_size), out); }
+
+void orc_circle_generator_mul(uint64_t scalar, uint32_t* out_xy) {
+  CirclePoint p = CirclePoint::generator().mulScalar(scalar);
+  out_xy[0] = p.x.v;
+  out_xy[1] = p.y.v;
+}
+
+// Natural-order points of the domain canonicHalf(log_n) ++ conjugate.
+void orc_circle_domain(unsigned log_n, uint32_t* xs, uint32_t* ys) {
+  CircleCoset hc = CircleCoset::canonicHalf(log_n);
+  size_t n = (size_t)1 << log_n;
+  for (size_t i = 0; i < n; ++i) {
+    CirclePoint p = circleDomainPoint(hc, i);
+    xs[i] = p.x.v;
+    ys[i] = p.y.v;
+  }
+}
+
+// circleFFT / circleIFFT on canonicHalf(log_n); coefficients A-then-B.
+void orc_circle_fft(const uint32_t* coeffs, unsigned log_n, uint32_t* evals, int faithful) {
+  size_t n = (size_t)1 << log_n;
+  std::vector<M31> c(n);
+  for (size_t i = 0; i < n; ++i) c[i] = M31(coeffs[i]);
+  std::vector<M31> e = circleFFT(c, CircleCoset::canonicHalf(log_n), nullptr, faithful != 0);
+  for (size_t i = 0; i < n; ++i) evals[i] = e[i].v;
+}
+void orc_circle_ifft(const uint32_t* evals, unsigned log_n, uint32_t* coeffs, int faithful) {
+  size_t n = (size_t)1 << log_n;
+  std::vector<M31> e(n);
+  for (size_t i = 0; i < n; ++i) e[i] = M31(evals[i]);
+  std::vector<M31> c = circleIFFT(e, CircleCoset::canonicHalf(log_n), nullptr, faithful != 0);
+  for (size_t i = 0; i < n; ++i) coeffs[i] = c[i].v;
+}
+uint32_t orc_circle_eval_at(const uint32_t* coeffs, unsigned log_n, uint32_t x, uint32_t y) {
+  size_t n = (size_t)1 << log_n;
+  std::vector<M31> c(n);
+  for (size_t i = 0; i < n; ++i) c[i] = M31(coeffs[i]);
+  return circleEvalAtPoint(c, CirclePoint(M31(x), M31(y))).v;
+}
+// The twiddle tree of canonicHalf(log_n) (length 2^(log_n-1)), as circle.zig:69-82 builds it.
+void orc_circle_twiddles(unsigned log_n, uint32_t* out) {
+  std::vector<M31> t = precomputeTwiddles(CircleCoset::canonicHalf(log_n), false);
+  for (size_t i = 0; i < t.size(); ++i) out[i] = t[i].v;
+}
+
+// Merkle root over 32-byte leaves; optionally the full opening path of `index`.
+void orc_merkle_root(const uint8_t* leaves, size_t n, uint8_t* out32) {
+  std::vector<Digest> l(n);
+  for (size_t i = 0; i < n; ++i) std::memcpy(l[i].data(), leaves + 32 * i, 32);
+  MerkleTree t(l);
+  std::memcpy(out32, t.root().data(), 32);
+}
+
+// Interpolation (O(n^2) reference algorithm or NTT) on H = <w_n>, n = 2^log_n.
+void orc_interpolate_subgroup(const uint32_t* ys, unsigned log_n, int use_ntt, uint32_t* coeffs) {
+  size_t n = (size_t)1 << log_n;
+  std::vector<QM31> y(n);
+  for (size_t i = 0; i < n; ++i) y[i] = q4(ys + 4 * i);
+  std::vector<QM31> c;
+  if (use_ntt) {
+    c = interpolateSubgroupNtt(y, log_n);
+  } else {
+    std::vector<QM31> xs(n);
+    QM31 w = QM31::primitiveRootOfUnity(log_n), acc = QM31::one();
+    for (size_t i = 0; i < n; ++i) {
+      xs[i] = acc;
+      acc = acc.mul(w);
+    }
+    c = interpolateLagrange(xs, y);
+  }
+  for (size_t i = 0; i < n; ++i) put4(c[i], coeffs + 4 * i);
+}
+
+// Evaluations of `coeffs` on FRI_OFFSET * <w_N> (Horner or NTT).
+void orc_evaluate_coset(const uint32_t* coeffs, size_t n, unsigned log_N, int use_ntt, uint32_t* out) {
+  std::vector<QM31> c(n);
+  for (size_t i = 0; i < n; ++i) c[i] = q4(coeffs + 4 * i);
+  size_t N = (size_t)1 << log_N;
+  std::vector<QM31> e;
+  if (use_ntt) {
+    e = evaluateCosetNtt(c, friOffset(), log_N);
+  } else {
+    e.resize(N);
+    QM31 w = QM31::primitiveRootOfUnity(log_N), d = friOffset();
+    for (size_t i = 0; i < N; ++i) {
+      e[i] = evalHorner(c, d);
+      d = d.mul(w);
+    }
+  }
+  for (size_t i = 0; i < N; ++i) put4(e[i], out + 4 * i);
+}
+
+// Channel script: absorbs `absorb` (raw bytes), then samples n_qm31 QM31 words
+// followed by n_idx indices below `idx_bound`.
+void orc_channel_script(const uint8_t* sep, size_t sep_len, const uint8_t* absorb, size_t absorb_len,
+                        size_t n_qm31, uint32_t* out_qm31, size_t n_idx, uint64_t idx_bound,
+                        uint64_t* out_idx) {
+  Channel ch(sep, sep_len);
+  ch.absorbBytes(absorb, absorb_len);
+  for (size_t i = 0; i < n_qm31; ++i) put4(ch.sampleQM31(), out_qm31 + 4 * i);
+  for (size_t i = 0; i < n_idx; ++i) out_idx[i] = ch.sampleIndex(idx_bound);
+}
+
+// FRI prove over an explicit codeword; returns the serialized Fri.Proof.
+int orc_fri_prove_codeword(uint8_t log_size, uint8_t log_blowup, uint64_t num_queries,
+                           uint8_t remainder_log, const uint32_t* codeword, const uint8_t* sep,
+                           size_t sep_len, uint8_t** out, size_t* out_len) {
+  try {
+    FriParams p;
+    p.log_size = log_size;
+    p.log_blowup = log_blowup;
+    p.num_queries = num_queries;
+    p.remainder_log = remainder_log;
+    size_t n0 = (size_t)1 << p.domainLogSize();
+    std::vector<QM31> cw(n0);
+    for (size_t i = 0; i < n0; ++i) cw[i] = q4(codeword + 4 * i);
+    Channel ch(sep, sep_len);
+    FriProof f = friProveCodeword(p, cw, ch);
+    Writer w;
+    f.write(w);
+    *out = dupBytes(w.out, out_len);
+    return 0;
+  } catch (const WireError& e) {
+    return e.code;
+  } catch (...) {
+    return -1;
+  }
+}
+
+int orc_fri_verify(uint8_t log_size, uint8_t log_blowup, uint64_t num_queries, uint8_t remainder_log,
+                   const uint8_t* proof, size_t proof_len, const uint8_t* sep, size_t sep_len, int* ok) {
+  try {
+    FriParams p;
+    p.log_size = log_size;
+    p.log_blowup = log_blowup;
+    p.num_queries = num_queries;
+    p.remainder_log = remainder_log;
+    Reader r(proof, proof_len);
+    FriProof f = FriProof::read(r);
+    r.end();
+    Channel ch(sep, sep_len);
+    *ok = friVerify(p, f, ch) ? 1 : 0;
+    return 0;
+  } catch (const WireError& e) {
+    return e.code;
+  } catch (...) {
+    return -1;
+  }
+}
+
+// GenericStark(Air).proveWithPreprocessed. params: wire StarkParams; columns in
+// wire form []const []const QM31; mode 0 = reference interpolation, 1 = NTT.
+int orc_prove(uint32_t air_id, const uint8_t* params, size_t params_len, const uint8_t* pi,
+              size_t pi_len, const uint8_t* pre, size_t pre_len, const uint8_t* trace,
+              size_t trace_len, const uint8_t* sep, size_t sep_len, int mode, uint8_t** out,
+              size_t* out_len) {
+  try {
+    Reader pr(params, params_len);
+    StarkParams sp = StarkParams::read(pr);
+    pr.end();
+    auto air = makeAir(air_id, pi, pi_len);
+    auto pcols = readColumns(pre, pre_len);
+    auto tcols = readColumns(trace, trace_len);
+    Stark st(*air);
+    Channel ch(sep, sep_len);
+    StarkProof proof = st.prove(sp, pcols, tcols, ch, mode ? Mode::Ntt : Mode::Lagrange);
+    *out = dupBytes(proof.serialize(), out_len);
+    return 0;
+  } catch (const WireError& e) {
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return -3;
+  } catch (...) {
+    return -1;
+  }
+}
+
+int orc_verify(uint32_t air_id, const uint8_t* params, size_t params_len, const uint8_t* pi,
+               size_t pi_len, const uint8_t* proof, size_t proof_len, const uint8_t* sep,
+               size_t sep_len, int* ok) {
+  try {
+    Reader pr(params, params_len);
+    StarkParams sp = StarkParams::read(pr);
+    pr.end();
+    auto air = makeAir(air_id, pi, pi_len);
+    StarkProof p = StarkProof::deserialize(proof, proof_len);
+    Stark st(*air);
+    Channel ch(sep, sep_len);
+    *ok = st.verify(sp, p, ch) ? 1 : 0;
+    return 0;
+  } catch (const WireError& e) {
+    return e.code;
+  } catch (...) {
+    return -1;
+  }
+}
+
+// Re-serializes a proof after a round trip through the wire reader.
+int orc_proof_roundtrip(const uint8_t* proof, size_t proof_len, uint8_t** out, size_t* out_len) {
+  try {
+    StarkProof p = StarkProof::deserialize(proof, proof_len);
+    *out = dupBytes(p.serialize(), out_len);
+    return 0;
+  } catch (const WireError& e) {
+    return e.code;
+  } catch (...) {
+    return -1;
+  }
+}
+
+// The circle commit workload. trace: n_cols x 2^log_rows column-major.
+// gammas: n_cols QM31, alphas: n_folds QM31. Outputs: lde_root (32 B),
+// layer_roots (32 B x n_folds), final_layer (QM31 x 2^(log_rows+log_blowup-n_folds)),
+// optional lde (n_cols x 2^(log_rows+log_blowup)) and g (QM31 x 2^(...)).
+int orc_circle_commit(const uint32_t* trace, uint32_t n_cols, uint32_t log_rows, uint32_t log_blowup,
+                      const uint32_t* gammas, const uint32_t* alphas, uint32_t n_folds, int faithful,
+                      int threads, uint8_t* lde_root, uint8_t* layer_roots, uint32_t* final_layer,
+                      uint32_t* lde_out, uint32_t* g_out) {
+  try {
+    size_t n = (size_t)1 << log_rows;
+    std::vector<std::vector<M31>> cols(n_cols, std::vector<M31>(n));
+    for (size_t c = 0; c < n_cols; ++c)
+      for (size_t i = 0; i < n; ++i) cols[c][i] = M31(trace[c * n + i]);
+    std::vector<QM31> gs(n_cols), as(n_folds);
+    for (size_t c = 0; c < n_cols; ++c) gs[c] = q4(gammas + 4 * c);
+    for (size_t i = 0; i < n_folds; ++i) as[i] = q4(alphas + 4 * i);
+    CommitResult r = circleCommit(cols, log_rows, log_blowup, gs, as, faithful != 0,
+                                  lde_out != nullptr || g_out != nullptr, threads);
+    std::memcpy(lde_root, r.lde_root.data(), 32);
+    for (size_t i = 0; i < r.layer_roots.size(); ++i) std::memcpy(layer_roots + 32 * i, r.layer_roots[i].data(), 32);
+    for (size_t i = 0; i < r.final_layer.size(); ++i) put4(r.final_layer[i], final_layer + 4 * i);
+    size_t N = (size_t)1 << (log_rows + log_blowup);
+    if (lde_out)
+      for (size_t c = 0; c < n_cols; ++c)
+        for (size_t i = 0; i < N; ++i) lde_out[c * N + i] = r.lde[c][i].v;
+    if (g_out)
+      for (size_t i = 0; i < N; ++i) put4(r.g[i], g_out + 4 * i);
+    return 0;
+  } catch (...) {
+    return -1;
+  }
+}
+
+}  // extern "C"

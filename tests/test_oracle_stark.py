@@ -1,0 +1,232 @@
+"""Oracle FRI and GenericStark against the reference's own protocol tests.
+
+Restates src/m31/fri.zig:349-440, src/m31/stark.zig:933-1321,
+tests/e2e_tests.zig:10-45,501-532 and src/core/serialization.zig:220-250, and pins the
+NTT prover mode byte-for-byte to the reference's O(n^2) mode.
+"""
+import struct
+
+import numpy as np
+import pytest
+
+from zs_b200 import wire
+from zs_b200 import workload as wl
+
+P = 2**31 - 1
+rng = np.random.default_rng(44)
+
+
+def test_golden_wire_layout():
+    # serialization.zig:220-250, encoded with the same rules wire.py uses
+    expected = bytes([ord("a"), ord("b"), ord("c"), 0x04, 0x03, 0x02, 0x01,
+                      0x02, 0, 0, 0, 0, 0, 0, 0, 0x02, 0x01, 0x04, 0x03, 0x01, 0x01, 0xDE, 0xAD])
+    enc = b"abc" + struct.pack("<I", 0x01020304) + wire.u64(2) + struct.pack("<2H", 0x0102, 0x0304) \
+        + wire.u8(1) + wire.u8(1) + bytes([0xDE, 0xAD])
+    assert enc == expected
+
+
+def _fri_coeffs(log_size, seed):
+    r = np.random.default_rng(seed)
+    return r.integers(0, P, (1 << log_size, 4), dtype=np.uint32)
+
+
+def test_fri_fold_halves_degree(orc):
+    # fri.zig:349-380: f = 1 + x + 2x^2 + 3x^3, log_size 2, blowup 0
+    alpha = rng.integers(0, P, 4, dtype=np.uint32)
+    f = np.array([[1, 0, 0, 0], [1, 0, 0, 0], [2, 0, 0, 0], [3, 0, 0, 0]], dtype=np.uint32)
+    ev = orc.evaluate_coset(f, 2)
+    # domain D_0 = FRI_OFFSET <w_2>; FRI_OFFSET = {a = 1, b = 1} = 1 + j (fri.zig:36)
+    off = np.array([1, 0, 1, 0], dtype=np.uint32)
+    w = orc.qm31_root(2)
+    dom = [off]
+    for _ in range(3):
+        dom.append(orc.qm31_op("mul", dom[-1], w))
+    inv2 = orc.m31_op("inv", [2])[0]
+    half = np.array([inv2, 0, 0, 0], dtype=np.uint32)
+    folded = np.array([orc.qm31_op("add", f[0], orc.qm31_op("mul", alpha, f[1])),
+                       orc.qm31_op("add", f[2], orc.qm31_op("mul", alpha, f[3]))])
+    d1 = orc.qm31_op("mul", off, off)
+    w1 = orc.qm31_pow(w, 2)
+    for j in range(2):
+        y0, y1 = ev[j], ev[j + 2]
+        hs = orc.qm31_op("mul", orc.qm31_op("add", y0, y1), half)
+        hd = orc.qm31_op("mul", orc.qm31_op("mul", orc.qm31_op("sub", y0, y1), orc.qm31_op("inv", dom[j])), half)
+        v = orc.qm31_op("add", hs, orc.qm31_op("mul", alpha, hd))
+        x = orc.qm31_op("mul", d1, orc.qm31_pow(w1, j))
+        want = orc.qm31_op("add", folded[0], orc.qm31_op("mul", folded[1], x))
+        assert np.array_equal(v, want)
+
+
+def _fri_proof(orc, seed=42):
+    coeffs = _fri_coeffs(4, seed)
+    cw = orc.evaluate_coset(coeffs, 7, use_ntt=False)
+    return orc.fri_prove_codeword(4, 3, 8, 3, cw, b"zig-stark:fri:test")
+
+
+def test_fri_round_trip(orc):
+    # fri.zig:382-398
+    proof = _fri_proof(orc)
+    assert orc.fri_verify(4, 3, 8, 3, proof, b"zig-stark:fri:test")
+    fp = wire.FriProof.read(wire.Reader(proof))
+    assert fp.encode() == proof
+
+
+def test_fri_rejects_tampered_remainder(orc):
+    # fri.zig:400-419
+    fp = wire.FriProof.read(wire.Reader(_fri_proof(orc, 43)))
+    r0 = fp.remainder[0]
+    fp.remainder[0] = ((r0[0] + 1) % P,) + tuple(r0[1:])
+    assert not orc.fri_verify(4, 3, 8, 3, fp.encode(), b"zig-stark:fri:test")
+
+
+def test_fri_rejects_tampered_leaf(orc):
+    # fri.zig:421-440
+    fp = wire.FriProof.read(wire.Reader(_fri_proof(orc, 44)))
+    v = fp.queries[0].pairs[0].value0
+    fp.queries[0].pairs[0].value0 = ((v[0] + 1) % P,) + tuple(v[1:])
+    assert not orc.fri_verify(4, 3, 8, 3, fp.encode(), b"zig-stark:fri:test")
+
+
+def _fib(orc, trace_log, log_blowup, nq, sep, mode, tamper_claim=False):
+    params = wire.StarkParams(trace_log, log_blowup, nq, 3)
+    tr = wl.fib_trace(1 << trace_log)
+    claimed = tuple(int(x) for x in tr[0][-1])
+    if tamper_claim:
+        claimed = ((claimed[0] + 1) % P,) + claimed[1:]
+    pi = wire.qm31(claimed)
+    proof = orc.prove(wl.AIR_FIB, params.encode(), pi, b"", wire.columns(tr), sep, mode=mode)
+    return params, pi, proof
+
+
+def test_stark_fib_round_trip(orc):
+    # stark.zig:933-951
+    params, pi, proof = _fib(orc, 4, 3, 12, b"zig-stark:stark:fib", mode=0)
+    assert orc.verify(wl.AIR_FIB, params.encode(), pi, proof, b"zig-stark:stark:fib")
+
+
+def test_stark_rejects_wrong_claim(orc):
+    # stark.zig:1282-1299
+    params, pi, proof = _fib(orc, 4, 3, 12, b"zig-stark:stark:fib", mode=0, tamper_claim=True)
+    assert not orc.verify(wl.AIR_FIB, params.encode(), pi, proof, b"zig-stark:stark:fib")
+
+
+def test_stark_rejects_tampered_trace_value(orc):
+    # stark.zig:1301-1321
+    params, pi, proof = _fib(orc, 4, 3, 12, b"zig-stark:stark:fib", mode=0)
+    sp = wire.StarkProof.decode(proof)
+    v = sp.queries[0].values[0]
+    sp.queries[0].values[0] = ((v[0] + 1) % P,) + tuple(v[1:])
+    assert not orc.verify(wl.AIR_FIB, params.encode(), pi, sp.encode(), b"zig-stark:stark:fib")
+
+
+@pytest.mark.parametrize("trace_log", [8, 4])
+def test_e2e_fib(orc, trace_log):
+    # tests/e2e_tests.zig:10-45
+    params, pi, proof = _fib(orc, trace_log, 3, 16, b"zig-stark:e2e", mode=1)
+    assert orc.verify(wl.AIR_FIB, params.encode(), pi, proof, b"zig-stark:e2e")
+    params, pi, proof = _fib(orc, trace_log, 3, 16, b"zig-stark:e2e", mode=1, tamper_claim=True)
+    assert not orc.verify(wl.AIR_FIB, params.encode(), pi, proof, b"zig-stark:e2e")
+
+
+def test_e2e_serialization_round_trip(orc):
+    # tests/e2e_tests.zig:501-532
+    params, pi, proof = _fib(orc, 6, 3, 16, b"zig-stark:e2e-ser", mode=1)
+    assert orc.proof_roundtrip(proof) == proof
+    assert wire.StarkProof.decode(proof).encode() == proof
+    assert orc.verify(wl.AIR_FIB, params.encode(), pi, proof, b"zig-stark:e2e-ser")
+
+
+LOOKUPS = [(wl.AIR_RANGE_CHECK, wl.range_check_trace, 0),
+           (wl.AIR_AND_TABLE, wl.and_table_trace, 0),
+           (wl.AIR_MULTIPLICITY, wl.multiplicity_trace, 1)]
+
+
+@pytest.mark.parametrize("air,gen,tamper", LOOKUPS)
+def test_lookup_round_trip_and_tamper(orc, air, gen, tamper):
+    # stark.zig:1218-1280
+    params = wire.StarkParams(4, 3, 16, 3)
+    tr, table = gen(16)
+    sep = b"zig-stark:stark:lookup"
+    proof = orc.prove(air, params.encode(), b"", wire.columns(table), wire.columns(tr), sep, mode=0)
+    assert orc.verify(air, params.encode(), b"", proof, sep)
+    sp = wire.StarkProof.decode(proof)
+    assert sp.preprocessed_roots is not None and sp.accumulator_roots is not None
+    v = sp.queries[0].values[tamper]
+    sp.queries[0].values[tamper] = ((v[0] + 1) % P,) + tuple(v[1:])
+    assert not orc.verify(air, params.encode(), b"", sp.encode(), sep)
+
+
+def test_rescue_example(orc):
+    # examples/rescue/src/main.zig:146-211
+    params = wire.StarkParams(3, 3, 16, 3)
+    tr, pi = wl.rescue_example()
+    sep = b"zig-stark:rescue:example"
+    p0 = orc.prove(wl.AIR_RESCUE_EXAMPLE, params.encode(), pi, b"", wire.columns(tr), sep, mode=0)
+    p1 = orc.prove(wl.AIR_RESCUE_EXAMPLE, params.encode(), pi, b"", wire.columns(tr), sep, mode=1)
+    assert p0 == p1
+    assert orc.verify(wl.AIR_RESCUE_EXAMPLE, params.encode(), pi, p0, sep)
+    bad = bytearray(pi)
+    bad[64] = (bad[64] + 1) % 256  # final[0] += 1
+    assert not orc.verify(wl.AIR_RESCUE_EXAMPLE, params.encode(), bytes(bad), p0, sep)
+
+
+def test_linear_example(orc):
+    # examples/ml_linear/src/main.zig:118-172
+    params = wire.StarkParams(3, 3, 16, 3)
+    tr, pi = wl.linear_example()
+    sep = b"zig-stark:ml_linear:example"
+    p0 = orc.prove(wl.AIR_LINEAR_EXAMPLE, params.encode(), pi, b"", wire.columns(tr), sep, mode=0)
+    assert p0 == orc.prove(wl.AIR_LINEAR_EXAMPLE, params.encode(), pi, b"", wire.columns(tr), sep, mode=1)
+    assert orc.verify(wl.AIR_LINEAR_EXAMPLE, params.encode(), pi, p0, sep)
+    bad = bytearray(pi)
+    bad[-16] = (bad[-16] + 1) % 256  # claimed_y += 1
+    assert not orc.verify(wl.AIR_LINEAR_EXAMPLE, params.encode(), bytes(bad), p0, sep)
+
+
+@pytest.mark.parametrize("trace_log,log_blowup", [(1, 2), (2, 1), (3, 2), (4, 3), (5, 2), (6, 1), (7, 2)])
+def test_ntt_mode_equals_reference_mode_fib(orc, trace_log, log_blowup):
+    rem = min(3, trace_log + log_blowup - 1)
+    rem = max(rem, log_blowup)
+    params = wire.StarkParams(trace_log, log_blowup, 16, rem)
+    tr, pi = wl.seeded_fib(trace_log)
+    a = orc.prove(wl.AIR_SEEDED_FIB, params.encode(), pi, b"", wire.columns(tr), b"s", mode=0)
+    b = orc.prove(wl.AIR_SEEDED_FIB, params.encode(), pi, b"", wire.columns(tr), b"s", mode=1)
+    assert a == b
+    assert orc.verify(wl.AIR_SEEDED_FIB, params.encode(), pi, a, b"s")
+
+
+@pytest.mark.parametrize("air,gen,_t", LOOKUPS)
+@pytest.mark.parametrize("trace_log,log_blowup", [(3, 2), (4, 2), (5, 3), (6, 2)])
+def test_ntt_mode_equals_reference_mode_lookup(orc, air, gen, _t, trace_log, log_blowup):
+    params = wire.StarkParams(trace_log, log_blowup, 16, 3)
+    tr, table = gen(1 << trace_log)
+    a = orc.prove(air, params.encode(), b"", wire.columns(table), wire.columns(tr), b"lk", mode=0)
+    b = orc.prove(air, params.encode(), b"", wire.columns(table), wire.columns(tr), b"lk", mode=1)
+    assert a == b
+    # MultiplicityAir's trace/table (stark.zig:1170-1205) only balance at n = 16; at
+    # other sizes the statement is false and the verifier must reject it.
+    valid = air != wl.AIR_MULTIPLICITY or trace_log == 4
+    assert orc.verify(air, params.encode(), b"", a, b"lk") == valid
+
+
+def test_seeded_fib_config_params(orc):
+    # the 2^12-row Fibonacci workload parameters at a reduced size: blowup 4,
+    # default queries and remainder, example channel seed
+    params = wire.StarkParams(8, 2, 16, 3)
+    tr, pi = wl.seeded_fib(8)
+    sep = b"zig-stark:fibonacci:example"
+    a = orc.prove(wl.AIR_SEEDED_FIB, params.encode(), pi, b"", wire.columns(tr), sep, mode=0)
+    assert a == orc.prove(wl.AIR_SEEDED_FIB, params.encode(), pi, b"", wire.columns(tr), sep, mode=1)
+    assert orc.verify(wl.AIR_SEEDED_FIB, params.encode(), pi, a, sep)
+
+
+def test_malformed_inputs_rejected(orc):
+    params = wire.StarkParams(4, 3, 16, 3)
+    tr = wl.fib_trace(16)
+    with pytest.raises(RuntimeError, match="-2"):
+        orc.prove(wl.AIR_FIB, params.encode(), b"\x00" * 15, b"", wire.columns(tr), b"x")
+    with pytest.raises(RuntimeError, match="-2"):
+        orc.prove(wl.AIR_FIB, params.encode(), wl.fib_public(tr), b"", wire.columns(tr)[:-1], b"x")
+    _, pi, proof = _fib(orc, 4, 3, 12, b"x", mode=1)
+    assert not orc.verify(wl.AIR_FIB, params.encode(), pi, proof + b"\x00", b"x")
+    assert not orc.verify(wl.AIR_FIB, params.encode(), pi, proof[:-1], b"x")
