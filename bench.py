@@ -1,0 +1,283 @@
+"""Benchmark of the circle commit workload on B200.
+
+Workload (one step): 64 columns x 2^20 rows of uniform M31 values; circle IFFT on the
+canonic 2^20 domain, circle FFT on the canonic 2^22 domain (blowup 4), Blake3 row
+leaves (hashM31s of each 64-value row) and the full Merkle tree, the QM31 combination
+g = sum_c gamma_c * LDE_c, then 16 FRI folds 2^22 -> 2^6 with seeded challenges, each
+layer committed (hashQM31 leaves + tree) before it is folded.
+
+Metric: trace rows per second of the whole step (value = 2^20 * n_gpus / step time).
+Inputs (256 MiB trace, 1 GiB LDE) are larger than the 126 MB L2, so no flush is needed
+between steps. `e2e` times the same step through the C ABI with the host trace copied
+from pinned memory every step and the roots / final layer read back.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "zig-stark_b200"))
+
+N_COLS, LOG_ROWS, LOG_BLOWUP, N_FOLDS = 64, 20, 2, 16
+METRIC = "M31 LDE+Merkle commit rows/s (64 cols x 2^20, blowup 4, + 16-fold FRI chain)"
+UNIT = "rows/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks / throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
+        mx = max(float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline_sample(threads):
+    """The oracle restatement on a bounded sample of the workload: all 64 columns at
+    2^16 rows, blowup 4, 10 folds, with the reference's per-call twiddle recomputation."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from zs_b200 import workload as wl
+    log_rows, folds = 16, 10
+    trace, gammas, alphas = wl.commit_inputs(N_COLS, log_rows, folds)
+    oracle.circle_commit(trace[:, :1 << 10][:8], LOG_BLOWUP, gammas[:8], alphas[:4], faithful=True, threads=threads)
+    t0 = time.perf_counter()
+    oracle.circle_commit(trace, LOG_BLOWUP, gammas, alphas, faithful=True, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": (1 << log_rows) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"64 cols x 2^{log_rows} rows, blowup 4, {folds} folds (per-call twiddles as the "
+                      f"reference computes them), {dt:.2f} s"}
+
+
+def run_reference(args, world, rank):
+    """The reference's CPU path (restated: Zig is not available) on the host cores."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    samples = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline_sample(threads)
+        if i >= args.warmup:
+            samples.append(cb["value"])
+    v = sum(samples) / len(samples)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": (1 << 16) / v * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31)", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "circle commit, CPU restatement of the reference on a bounded sample",
+                       "columns": N_COLS, "log_rows": 16, "log_blowup": LOG_BLOWUP, "folds": 10},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        barrier(world)
+        return
+    import numpy as np
+    import torch
+    from zs_b200 import native
+    from zs_b200 import workload as wl
+
+    torch.cuda.set_device(local)
+    trace, gammas, alphas = wl.commit_inputs(N_COLS, LOG_ROWS, N_FOLDS)
+    plan = native.CommitPlan(N_COLS, LOG_ROWS, LOG_BLOWUP, N_FOLDS)
+    plan.set_challenges(gammas, alphas)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    pinned = torch.from_numpy(trace.view(np.int32)).pin_memory()
+    plan.upload(pinned.data_ptr(), sp)
+    torch.cuda.synchronize()
+
+    # correctness of the timed configuration: the first run against a stored digest
+    plan.run(None, sp)
+    ref_root = plan.results(sp)["lde_root"]
+
+    def timed(fn, k):
+        barrier(world)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(k):
+            fn()
+        end.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return start.elapsed_time(end)
+
+    # device-resident step
+    for _ in range(args.warmup):
+        plan.run(None, sp)
+    with ClockSampler(local) as clocks:
+        ms = timed(lambda: plan.run(None, sp), args.steps)
+    ms = max_over_ranks(ms, world)
+    ms_step = ms / args.steps
+
+    # per-phase breakdown with events on the launching stream
+    phase_ms = {}
+    for ph, name in enumerate(native.CommitPlan.PHASES):
+        evs = []
+        for _ in range(max(1, args.steps // 2)):
+            for p2 in range(ph):
+                plan.run_phase(p2, None, sp)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            plan.run_phase(ph, None, sp)
+            b.record(stream)
+            for p2 in range(ph + 1, 3):
+                plan.run_phase(p2, None, sp)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        phase_ms[name] = sum(a.elapsed_time(b) for a, b in evs) / len(evs)
+
+    # end to end through the C ABI: H2D of the trace from pinned memory, run, read back
+    h2d = trace.nbytes
+    d2h = 32 + 32 * N_FOLDS + (1 << (LOG_ROWS + LOG_BLOWUP - N_FOLDS)) * 16
+    for _ in range(args.warmup):
+        plan.upload(pinned.data_ptr(), sp)
+        plan.run(None, sp)
+        plan.results(sp)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        plan.upload(pinned.data_ptr(), sp)
+        plan.run(None, sp)
+        r = plan.results(sp)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world) / args.steps
+    assert r["lde_root"] == ref_root, "e2e run changed the LDE root"
+
+    rows = (1 << LOG_ROWS) * world
+    value = rows / (ms_step / 1e3)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    # dominant phase and its algorithmic bytes (inputs and outputs it must touch)
+    n, N = 1 << LOG_ROWS, 1 << (LOG_ROWS + LOG_BLOWUP)
+    alg = {
+        "lde": N_COLS * (n + N) * 4,                      # read trace, write LDE
+        "row_tree": N_COLS * N * 4 + (2 * N - 1) * 32 * 2 + N * 16,  # read LDE, write 2 trees + g
+        "folds": sum((N >> i) * 16 + (N >> (i + 1)) * 16 + (2 * (N >> (i + 1)) - 1) * 32 for i in range(N_FOLDS)),
+    }
+    dom = max(phase_ms, key=phase_ms.get)
+    achieved = alg[dom] / (phase_ms[dom] / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 (M31 / QM31 exact)", "data": "synthetic (SplitMix64 seeded)",
+        "config": {"workload": "circle commit: 64 cols x 2^20 M31, blowup 4, row-leaf Blake3 Merkle, "
+                               "16-fold QM31 FRI chain with per-layer commits",
+                   "columns": N_COLS, "log_rows": LOG_ROWS, "log_blowup": LOG_BLOWUP, "folds": N_FOLDS,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)"},
+        "phases_ms": phase_ms,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": None,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                     "algorithmic_bytes": alg[dom]},
+        "commit_bytes_per_row": 1536,
+        "e2e": {"value": rows / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": plan.launches() * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(os.cpu_count() or 1)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,125 @@
+/* zs_m31.h — C ABI of the B200 (sm_100a) backend for zig-stark's M31 DEEP-FRI
+ * commitment path.
+ *
+ * Conventions follow zig-capi.h (the reference's only C ABI, for the Binius STARK):
+ *   - byte buffers use the canonical wire format of docs/wire.md
+ *     (src/core/serialization.zig:58-190): little-endian, QM31 = 16 bytes
+ *     (a.c0 | a.c1 | b.c0 | b.c1), slices u64-length prefixed, usize = 8 bytes,
+ *     optionals with a 1-byte presence flag;
+ *   - buffers returned by the library are allocated with the caller's
+ *     zs_host_allocator and released with zs_free (zig-capi.h:15-18);
+ *   - input buffers are borrowed for the duration of the call;
+ *   - return codes: 0 ok, -1 generic, -2 malformed input, -3 out of memory,
+ *     -4 protocol error (zig-capi.h:20-21), and -5 device error.
+ *
+ * Every entry point runs its hot path on the GPU; there is no CPU fallback. Without a
+ * usable CUDA device the calls return -5.
+ */
+#ifndef ZS_M31_H
+#define ZS_M31_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Host memory callbacks; the same layout as zs_host_allocator in zig-capi.h:35-39. */
+typedef struct {
+    void *ctx;
+    void *(*alloc)(void *ctx, size_t size);
+    void (*free)(void *ctx, void *ptr, size_t size);
+} zs_host_allocator;
+
+/* Compiled-in AIRs. A comptime Zig AIR type (src/m31/stark.zig:45-74) cannot cross
+ * a C ABI, so the AIR is chosen by id; its PublicInputs struct is passed in wire form.
+ *   ZS_AIR_FIB             FibAir, stark.zig:877-931            PI {claimed_fib: QM31}
+ *   ZS_AIR_SEEDED_FIB      FibAir with public a_0, a_1          PI {a0, a1, claimed: QM31}
+ *   ZS_AIR_RANGE_CHECK     RangeCheckAir, stark.zig:964-1041    PI {}
+ *   ZS_AIR_AND_TABLE       AndTableAir, stark.zig:1048-1131     PI {}
+ *   ZS_AIR_MULTIPLICITY    MultiplicityAir, stark.zig:1139-1216 PI {}
+ *   ZS_AIR_RESCUE_EXAMPLE  examples/rescue (8 rows)             PI {initial: [4]QM31, final: [4]QM31}
+ *   ZS_AIR_LINEAR_EXAMPLE  examples/ml_linear (8 rows)          PI {x: []QM31, claimed_y: QM31} */
+enum {
+    ZS_AIR_FIB = 0,
+    ZS_AIR_SEEDED_FIB = 1,
+    ZS_AIR_RANGE_CHECK = 2,
+    ZS_AIR_AND_TABLE = 3,
+    ZS_AIR_MULTIPLICITY = 4,
+    ZS_AIR_RESCUE_EXAMPLE = 5,
+    ZS_AIR_LINEAR_EXAMPLE = 6
+};
+
+/* ---- circle FFT -------------------------------------------------------------
+ * Replaces src/cuda/circlefft_gpu.zig:46-108 circleFFT(allocator, coeffs, half_coset,
+ * evals) and :111-175 circleIFFT(...), themselves GPU versions of
+ * src/m31/ntt/circle.zig:195-246 / 272-346. The half coset is given by its offset
+ * point, step point and log size (CircleCoset, coset.zig:10-14); the domain is
+ * half_coset ++ conjugate, coefficients use the A-then-B layout, evaluations are in
+ * natural domain order. n = 2^(log_half + 1) words, n_columns transforms in a row
+ * (column c at offset c * n). Host buffers. Bit-identical to the CPU transform for
+ * every size (the reference falls back to the CPU below 8 points; this does not). */
+int32_t zs_m31_circle_fft(const uint32_t *coeffs, uint32_t n_columns, uint32_t offset_x, uint32_t offset_y,
+                          uint32_t step_x, uint32_t step_y, uint32_t log_half, uint32_t *evals);
+int32_t zs_m31_circle_ifft(const uint32_t *evals, uint32_t n_columns, uint32_t offset_x, uint32_t offset_y,
+                           uint32_t step_x, uint32_t step_y, uint32_t log_half, uint32_t *coeffs);
+
+/* ---- circle commit (the 64 x 2^20 LDE + Merkle + fold chain workload) --------
+ * Composes reference primitives: per column circleIFFT on canonicHalf(log_rows),
+ * zero-padding of A and B, circleFFT on canonicHalf(log_rows + log_blowup)
+ * (ntt/circle.zig); row leaves hashM31s over all columns (m31/hash.zig:15-25) and a
+ * Merkle tree (core/merkle/merkle.zig:17-45); the combination
+ * g[r] = sum_c gamma_c * LDE_c[r]; then n_folds FRI folds of g on the fri.zig domains
+ * of size 2^(log_rows + log_blowup) with the given fold challenges, each layer
+ * committed with hashQM31 leaves before it is folded (fri.zig:195-220).
+ *
+ * A plan owns every device buffer of one configuration. Typical use:
+ *   create -> set_challenges -> (upload | run_device)* -> results -> destroy. */
+typedef struct zs_commit_plan zs_commit_plan;
+
+int32_t zs_m31_commit_plan_create(uint32_t n_columns, uint32_t log_rows, uint32_t log_blowup, uint32_t n_folds,
+                                  zs_commit_plan **out);
+void zs_m31_commit_plan_destroy(zs_commit_plan *plan);
+/* gammas: n_columns QM31 (4 words each); alphas: n_folds QM31. Host buffers. */
+int32_t zs_m31_commit_plan_set_challenges(zs_commit_plan *plan, const uint32_t *gammas, const uint32_t *alphas);
+/* Device pointer to the plan's own trace buffer (n_columns x 2^log_rows words,
+ * column-major), for callers that fill it on the device. */
+uint32_t *zs_m31_commit_plan_trace_buffer(zs_commit_plan *plan);
+/* Copies a host trace into the plan's trace buffer (pinned or pageable memory) on `stream`. */
+int32_t zs_m31_commit_plan_upload(zs_commit_plan *plan, const uint32_t *host_trace, void *stream);
+/* Runs the whole workload on `stream` (a cudaStream_t; NULL = default stream) over a
+ * device trace (NULL = the plan's own trace buffer). Asynchronous. */
+int32_t zs_m31_commit_plan_run_device(zs_commit_plan *plan, const uint32_t *d_trace, void *stream);
+/* Runs one phase of run_device: 0 = circle LDE of all columns, 1 = row-leaf Merkle
+ * tree with the gamma combination and the layer-0 tree, 2 = the fold chain. Running
+ * 0, 1, 2 in order equals one run_device call. */
+int32_t zs_m31_commit_plan_run_phase(zs_commit_plan *plan, int32_t phase, const uint32_t *d_trace, void *stream);
+/* Synchronizes `stream` and copies the LDE root (32 bytes), the n_folds layer roots
+ * (32 bytes each) and the final layer (2^(log_rows+log_blowup-n_folds) QM31) to host
+ * buffers; any pointer may be NULL. */
+int32_t zs_m31_commit_plan_results(zs_commit_plan *plan, void *stream, uint8_t *lde_root, uint8_t *layer_roots,
+                                   uint32_t *final_layer);
+/* Copies the low-degree extension (n_columns x 2^(log_rows+log_blowup) words), or
+ * fold layer `layer` (0 = the combination g; 2^(log_rows+log_blowup-layer) QM31) to host. */
+int32_t zs_m31_commit_plan_copy_lde(zs_commit_plan *plan, uint32_t *host_out);
+int32_t zs_m31_commit_plan_copy_layer(zs_commit_plan *plan, uint32_t layer, uint32_t *host_out);
+/* Number of this library's kernel launches in one run_device call. */
+uint32_t zs_m31_commit_plan_launches(const zs_commit_plan *plan);
+
+/* One-shot host-buffer version: creates a plan, uploads, runs, copies the results. */
+int32_t zs_m31_circle_commit(const uint32_t *trace, uint32_t n_columns, uint32_t log_rows, uint32_t log_blowup,
+                             const uint32_t *gammas, const uint32_t *alphas, uint32_t n_folds, uint8_t *lde_root,
+                             uint8_t *layer_roots, uint32_t *final_layer);
+
+/* Release a buffer returned by the ABI (zig-capi.h:73-74). */
+void zs_free(zs_host_allocator host, uint8_t *ptr, size_t len);
+
+/* Version / configuration string (zig-capi.h:76-77). */
+const char *zs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ZS_M31_H */

@@ -1,0 +1,45 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares (CPU only)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(zs_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "zs_m31_circle_fft" in names and "zs_m31_commit_plan_create" in names and "zs_free" in names
+
+
+def test_library_exports_every_declared_symbol():
+    from zs_b200 import native
+    lib = native.lib()
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert "sm_100a" in native.version()
+
+
+def test_library_is_in_tree():
+    from zs_b200 import native
+    assert os.path.dirname(native.LIB_PATH).startswith(os.path.join(ROOT, "zig-stark_b200"))
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    from zs_b200 import native
+    monkeypatch.setattr(native, "_lib", None)
+    monkeypatch.setattr(native, "LIB_PATH", str(tmp_path / "absent.so"))
+    with pytest.raises(ImportError):
+        native.lib()

@@ -1,0 +1,186 @@
+// extern "C" entry points declared in include/zs_m31.h.
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "../../include/zs_m31.h"
+#include "circle.cuh"
+#include "commit.cuh"
+
+using namespace zs;
+
+namespace {
+
+template <typename F>
+int32_t guarded(F&& f) {
+  try {
+    f();
+    return ZS_OK;
+  } catch (const Error& e) {
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return ZS_ENOMEM;
+  } catch (...) {
+    return ZS_EGENERIC;
+  }
+}
+
+void ensure_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw Error(ZS_EDEVICE, "no CUDA device");
+}
+
+struct DeviceBuffer {
+  void* p = nullptr;
+  explicit DeviceBuffer(size_t bytes) { ZS_CUDA(cudaMalloc(&p, bytes ? bytes : 4)); }
+  ~DeviceBuffer() { cudaFree(p); }
+  template <typename T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+int32_t circle_transform(const uint32_t* in, uint32_t n_columns, uint32_t ox, uint32_t oy, uint32_t sx, uint32_t sy,
+                         uint32_t log_half, uint32_t* out, bool inverse) {
+  return guarded([&] {
+    if (!in || !out || n_columns == 0) throw Error(ZS_EMALFORMED, "null buffer or no columns");
+    if (log_half > 27) throw Error(ZS_EMALFORMED, "log_half above 27");
+    if (ox >= P || oy >= P || sx >= P || sy >= P) throw Error(ZS_EMALFORMED, "non-canonical coset point");
+    ensure_device();
+    const unsigned lg = log_half + 1;
+    const size_t n = (size_t)1 << lg;
+    cudaStream_t st = nullptr;
+    CircleDomain dom(lg, cpoint{ox, oy}, cpoint{sx, sy}, st);
+    DeviceBuffer a(n * n_columns * 4), b(n * n_columns * 4), s(n * n_columns * 4);
+    ZS_CUDA(cudaMemcpy(a.p, in, n * n_columns * 4, cudaMemcpyHostToDevice));
+    if (inverse)
+      circle_ifft(a.as<uint32_t>(), b.as<uint32_t>(), n_columns, dom, s.as<uint32_t>(), st);
+    else
+      circle_fft(a.as<uint32_t>(), b.as<uint32_t>(), n_columns, dom, s.as<uint32_t>(), st);
+    ZS_CUDA(cudaMemcpy(out, b.p, n * n_columns * 4, cudaMemcpyDeviceToHost));
+  });
+}
+
+}  // namespace
+
+struct zs_commit_plan {
+  std::unique_ptr<CommitPlan> plan;
+};
+
+extern "C" {
+
+int32_t zs_m31_circle_fft(const uint32_t* coeffs, uint32_t n_columns, uint32_t offset_x, uint32_t offset_y,
+                          uint32_t step_x, uint32_t step_y, uint32_t log_half, uint32_t* evals) {
+  return circle_transform(coeffs, n_columns, offset_x, offset_y, step_x, step_y, log_half, evals, false);
+}
+
+int32_t zs_m31_circle_ifft(const uint32_t* evals, uint32_t n_columns, uint32_t offset_x, uint32_t offset_y,
+                           uint32_t step_x, uint32_t step_y, uint32_t log_half, uint32_t* coeffs) {
+  return circle_transform(evals, n_columns, offset_x, offset_y, step_x, step_y, log_half, coeffs, true);
+}
+
+int32_t zs_m31_commit_plan_create(uint32_t n_columns, uint32_t log_rows, uint32_t log_blowup, uint32_t n_folds,
+                                  zs_commit_plan** out) {
+  return guarded([&] {
+    if (!out) throw Error(ZS_EMALFORMED, "null out");
+    ensure_device();
+    auto p = std::make_unique<zs_commit_plan>();
+    p->plan = std::make_unique<CommitPlan>(n_columns, log_rows, log_blowup, n_folds);
+    *out = p.release();
+  });
+}
+
+void zs_m31_commit_plan_destroy(zs_commit_plan* plan) { delete plan; }
+
+int32_t zs_m31_commit_plan_set_challenges(zs_commit_plan* plan, const uint32_t* gammas, const uint32_t* alphas) {
+  return guarded([&] {
+    if (!plan || !gammas || (!alphas && plan->plan->F > 0)) throw Error(ZS_EMALFORMED, "null argument");
+    plan->plan->set_challenges(gammas, alphas);
+  });
+}
+
+uint32_t* zs_m31_commit_plan_trace_buffer(zs_commit_plan* plan) { return plan ? plan->plan->trace : nullptr; }
+
+int32_t zs_m31_commit_plan_upload(zs_commit_plan* plan, const uint32_t* host_trace, void* stream) {
+  return guarded([&] {
+    if (!plan || !host_trace) throw Error(ZS_EMALFORMED, "null argument");
+    CommitPlan& p = *plan->plan;
+    ZS_CUDA(cudaMemcpyAsync(p.trace, host_trace, ((size_t)p.C << p.L) * 4, cudaMemcpyHostToDevice,
+                            (cudaStream_t)stream));
+  });
+}
+
+int32_t zs_m31_commit_plan_run_device(zs_commit_plan* plan, const uint32_t* d_trace, void* stream) {
+  return guarded([&] {
+    if (!plan) throw Error(ZS_EMALFORMED, "null plan");
+    plan->plan->run(d_trace, (cudaStream_t)stream);
+  });
+}
+
+int32_t zs_m31_commit_plan_run_phase(zs_commit_plan* plan, int32_t phase, const uint32_t* d_trace, void* stream) {
+  return guarded([&] {
+    if (!plan) throw Error(ZS_EMALFORMED, "null plan");
+    plan->plan->run_phase(phase, d_trace, (cudaStream_t)stream);
+  });
+}
+
+int32_t zs_m31_commit_plan_results(zs_commit_plan* plan, void* stream, uint8_t* lde_root, uint8_t* layer_roots,
+                                   uint32_t* final_layer) {
+  return guarded([&] {
+    if (!plan) throw Error(ZS_EMALFORMED, "null plan");
+    CommitPlan& p = *plan->plan;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (lde_root) ZS_CUDA(cudaMemcpyAsync(lde_root, p.row_tree.root(), 32, cudaMemcpyDeviceToHost, st));
+    if (layer_roots)
+      for (unsigned i = 0; i < p.F; ++i)
+        ZS_CUDA(cudaMemcpyAsync(layer_roots + 32 * i, p.layer_trees[i].root(), 32, cudaMemcpyDeviceToHost, st));
+    if (final_layer)
+      ZS_CUDA(cudaMemcpyAsync(final_layer, p.layers[p.F], ((size_t)1 << (p.L + p.B - p.F)) * sizeof(qm31),
+                              cudaMemcpyDeviceToHost, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int32_t zs_m31_commit_plan_copy_lde(zs_commit_plan* plan, uint32_t* host_out) {
+  return guarded([&] {
+    if (!plan || !host_out) throw Error(ZS_EMALFORMED, "null argument");
+    CommitPlan& p = *plan->plan;
+    ZS_CUDA(cudaDeviceSynchronize());
+    ZS_CUDA(cudaMemcpy(host_out, p.lde, ((size_t)p.C << (p.L + p.B)) * 4, cudaMemcpyDeviceToHost));
+  });
+}
+
+int32_t zs_m31_commit_plan_copy_layer(zs_commit_plan* plan, uint32_t layer, uint32_t* host_out) {
+  return guarded([&] {
+    if (!plan || !host_out) throw Error(ZS_EMALFORMED, "null argument");
+    CommitPlan& p = *plan->plan;
+    if (layer > p.F) throw Error(ZS_EMALFORMED, "layer index above n_folds");
+    ZS_CUDA(cudaDeviceSynchronize());
+    ZS_CUDA(cudaMemcpy(host_out, p.layers[layer], ((size_t)1 << (p.L + p.B - layer)) * sizeof(qm31),
+                       cudaMemcpyDeviceToHost));
+  });
+}
+
+uint32_t zs_m31_commit_plan_launches(const zs_commit_plan* plan) { return plan ? plan->plan->launches() : 0; }
+
+int32_t zs_m31_circle_commit(const uint32_t* trace, uint32_t n_columns, uint32_t log_rows, uint32_t log_blowup,
+                             const uint32_t* gammas, const uint32_t* alphas, uint32_t n_folds, uint8_t* lde_root,
+                             uint8_t* layer_roots, uint32_t* final_layer) {
+  zs_commit_plan* plan = nullptr;
+  int32_t rc = zs_m31_commit_plan_create(n_columns, log_rows, log_blowup, n_folds, &plan);
+  if (rc != 0) return rc;
+  rc = zs_m31_commit_plan_set_challenges(plan, gammas, alphas);
+  if (rc == 0) rc = zs_m31_commit_plan_upload(plan, trace, nullptr);
+  if (rc == 0) rc = zs_m31_commit_plan_run_device(plan, nullptr, nullptr);
+  if (rc == 0) rc = zs_m31_commit_plan_results(plan, nullptr, lde_root, layer_roots, final_layer);
+  zs_m31_commit_plan_destroy(plan);
+  return rc;
+}
+
+void zs_free(zs_host_allocator host, uint8_t* ptr, size_t len) {
+  if (ptr && host.free) host.free(host.ctx, ptr, len);
+}
+
+const char* zs_version(void) { return "zs-b200 0.1.0 (sm_100a, M31 DEEP-FRI commitment path)"; }
+
+}  // extern "C"

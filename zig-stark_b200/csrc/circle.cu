@@ -1,0 +1,472 @@
+// Circle FFT over M31 on the device: twiddle tables, the standalone forward and
+// inverse transforms, and the fused low-degree extension (interpolate on the
+// canonic trace domain, evaluate on the 2^B-times larger canonic domain).
+//
+// Reference semantics (src/m31/ntt/circle.zig):
+//   circleFFT 195-246: interleave A/B, line layers i = lg-1 .. 1 (DIF, one twiddle
+//     per block of 2^(i+1)), the circle layer i = 0, then bit-reverse.
+//   circleIFFT 272-346: bit-reverse, circle layer, line layers 1 .. lg-1 with
+//     inverted twiddles (ibutterfly), scale by 1/n, de-interleave.
+//   Twiddles 65-106: the tree of bit-reversed x-coordinates of the halved cosets,
+//     and the circle layer [y, -y, -x, x] derived from its first level.
+//
+// Device layout of a domain's twiddles (flat, n - 1 words used): the twiddle of
+// block b at layer i is TW[n - (n >> i) + b]; layer 0 (the circle layer) occupies
+// [0, n/2), layer i >= 1 the 2^(lg-1-i) words after it. The inverse table holds the
+// elementwise M31 inverses. Tables are generated on the device once per domain.
+//
+// Each transform is split into HBM passes over groups held in shared memory: the
+// butterflies of layers [0, K) connect elements inside aligned runs of 2^K
+// positions, layers [K, lg) connect elements that share the low K position bits.
+// Inside a pass, each thread moves 2^r elements (r <= 4 layers) between shared
+// memory and registers per chunk, so a pass costs one shared-memory round trip per
+// four layers. Every butterfly is the reference's exact M31 butterfly with the
+// reference's twiddle, so outputs are bit-identical.
+#include "circle.cuh"
+
+namespace zs {
+
+// ---------------------------------------------------------------------------
+// Twiddle tables
+// ---------------------------------------------------------------------------
+
+// Tree levels t = 0 .. lg-2: level t holds x(D^t(P_r)) for r < 2^(lg-2-t) in
+// bit-reversed order, P_r = offset + r*step of the half coset (circle.zig:69-82).
+__global__ void k_tw_tree(unsigned lg, cpoint offset, cpoint step, uint32_t* TW) {
+  const uint32_t half = 1u << (lg - 1);
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= (1u << (lg - 2))) return;
+  cpoint pt = padd(offset, pmul(step, r));
+  for (unsigned t = 0; t + 2 <= lg; ++t) {
+    if (r >= (1u << (lg - 2 - t))) break;
+    const uint32_t off = half - (1u << (lg - 1 - t));
+    TW[half + off + bitrev(r, lg - 2 - t)] = pt.x;
+    pt = pdbl(pt);
+  }
+  if (r == 0) TW[2 * half - 1] = 1;  // the reference's padding slot
+}
+
+// Circle layer from the first tree level: (f0, f1) -> [f1, -f1, -f0, f0] (circle.zig:96-106).
+__global__ void k_tw_circle_layer(unsigned lg, uint32_t* TW) {
+  const uint32_t half = 1u << (lg - 1);
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= (half >> 2)) return;
+  const uint32_t f0 = TW[half + 2 * k], f1 = TW[half + 2 * k + 1];
+  TW[4 * k] = f1;
+  TW[4 * k + 1] = mneg(f1);
+  TW[4 * k + 2] = mneg(f0);
+  TW[4 * k + 3] = f0;
+}
+
+// lg = 1, 2: the reference's closed forms (circle.zig:210-220, 290-319) written as
+// the same flat table: layer 0 = [y] or [y, -y], layer 1 = [x].
+__global__ void k_tw_small(unsigned lg, cpoint p0, uint32_t* TW) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (lg == 1) {
+    TW[0] = p0.y;
+    TW[1] = 1;
+  } else {
+    TW[0] = p0.y;
+    TW[1] = mneg(p0.y);
+    TW[2] = p0.x;
+    TW[3] = 1;
+  }
+}
+
+__global__ void k_invert(const uint32_t* in, uint32_t* out, uint32_t n) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = minv(in[k]);
+}
+
+// canonicHalf(lg) (src/m31/circle/coset.zig:59-65): B = generator().neg(),
+// offset = B * 2^(30-lg), step = B * 2^(32-lg).
+void canonic_half(unsigned lg, cpoint* offset, cpoint* step) {
+  const cpoint gen_neg = {1268011823u, mneg(2)};
+  *offset = pmul(gen_neg, (uint64_t)1 << (30 - lg));
+  *step = pmul(gen_neg, (uint64_t)1 << (32 - lg));
+}
+
+CircleDomain::CircleDomain(unsigned lg_, cudaStream_t st) : lg(lg_) {
+  if (lg < 1 || lg > 28) throw Error(ZS_EMALFORMED, "circle domain log size must be in [1, 28]");
+  cpoint offset, step;
+  canonic_half(lg, &offset, &step);
+  init(offset, step, st);
+}
+
+CircleDomain::CircleDomain(unsigned lg_, cpoint offset, cpoint step, cudaStream_t st) : lg(lg_) {
+  if (lg < 1 || lg > 28) throw Error(ZS_EMALFORMED, "circle domain log size must be in [1, 28]");
+  init(offset, step, st);
+}
+
+void CircleDomain::init(cpoint offset, cpoint step, cudaStream_t st) {
+  const uint32_t n = 1u << lg;
+  ZS_CUDA(cudaMallocAsync(&tw, n * sizeof(uint32_t), st));
+  ZS_CUDA(cudaMallocAsync(&itw, n * sizeof(uint32_t), st));
+  if (lg <= 2) {
+    k_tw_small<<<1, 32, 0, st>>>(lg, offset, tw);
+  } else {
+    const uint32_t r = 1u << (lg - 2);
+    k_tw_tree<<<(r + 255) / 256, 256, 0, st>>>(lg, offset, step, tw);
+    const uint32_t k = 1u << (lg - 3);
+    k_tw_circle_layer<<<(k + 255) / 256, 256, 0, st>>>(lg, tw);
+  }
+  k_invert<<<(n + 255) / 256, 256, 0, st>>>(tw, itw, n);
+  ZS_CUDA(cudaGetLastError());
+}
+
+CircleDomain::~CircleDomain() {
+  cudaFree(tw);
+  cudaFree(itw);
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory group transforms
+// ---------------------------------------------------------------------------
+
+// One padding word per 32 keeps strided chunk accesses on distinct banks.
+__device__ __forceinline__ uint32_t padx(uint32_t e) { return e + (e >> 5); }
+__host__ __device__ inline uint32_t group_stride(unsigned M) {
+  const uint32_t g = 1u << M;
+  return g + (g >> 5) + 1;
+}
+
+// Applies layers [b0, b0 + R) (group-local numbering; global layer = local + shift)
+// to every group held in `s`. Element e of group gi sits at virtual position
+// vb[gi] + e, so the twiddle of a butterfly at global layer i whose lower element
+// has virtual position V is T_i[V >> (local layer + 1)].
+template <int R, bool INV>
+__device__ __forceinline__ void chunk(uint32_t* s, uint32_t gstride, unsigned G, unsigned M, unsigned b0,
+                                      unsigned shift, const uint32_t* __restrict__ TW, uint32_t n_dom,
+                                      const uint32_t* vb) {
+  const unsigned sl = M - R;
+  const uint32_t total = G << sl;
+  for (uint32_t slot = threadIdx.x; slot < total; slot += blockDim.x) {
+    const uint32_t gi = slot >> sl;
+    const uint32_t rest = slot & ((1u << sl) - 1);
+    const uint32_t e0 = ((rest >> b0) << (b0 + R)) | (rest & ((1u << b0) - 1));
+    uint32_t* base = s + gi * gstride;
+    uint32_t v[1 << R];
+#pragma unroll
+    for (int m = 0; m < (1 << R); ++m) v[m] = base[padx(e0 | ((uint32_t)m << b0))];
+    const uint32_t Vh = (vb[gi] + e0) >> (b0 + R);
+    if (!INV) {
+#pragma unroll
+      for (int l = R - 1; l >= 0; --l) {
+        const unsigned i = b0 + l + shift;
+        const uint32_t* T = TW + (n_dom - (n_dom >> i)) + (Vh << (R - l - 1));
+#pragma unroll
+        for (int hb = 0; hb < (1 << (R - 1 - l)); ++hb) {
+          const uint32_t t = __ldg(T + hb);
+#pragma unroll
+          for (int lm = 0; lm < (1 << l); ++lm) {
+            const int m0 = (hb << (l + 1)) | lm, m1 = m0 | (1 << l);
+            const uint32_t x1 = mmul(v[m1], t), x0 = v[m0];
+            v[m1] = msub(x0, x1);
+            v[m0] = madd(x0, x1);
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int l = 0; l < R; ++l) {
+        const unsigned i = b0 + l + shift;
+        const uint32_t* T = TW + (n_dom - (n_dom >> i)) + (Vh << (R - l - 1));
+#pragma unroll
+        for (int hb = 0; hb < (1 << (R - 1 - l)); ++hb) {
+          const uint32_t t = __ldg(T + hb);
+#pragma unroll
+          for (int lm = 0; lm < (1 << l); ++lm) {
+            const int m0 = (hb << (l + 1)) | lm, m1 = m0 | (1 << l);
+            const uint32_t x0 = v[m0], x1 = v[m1];
+            v[m0] = madd(x0, x1);
+            v[m1] = mmul(msub(x0, x1), t);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < (1 << R); ++m) base[padx(e0 | ((uint32_t)m << b0))] = v[m];
+  }
+}
+
+template <bool INV>
+__device__ __forceinline__ void chunk_dispatch(unsigned r, uint32_t* s, uint32_t gstride, unsigned G, unsigned M,
+                                               unsigned b0, unsigned shift, const uint32_t* TW, uint32_t n_dom,
+                                               const uint32_t* vb) {
+  switch (r) {
+    case 1: chunk<1, INV>(s, gstride, G, M, b0, shift, TW, n_dom, vb); break;
+    case 2: chunk<2, INV>(s, gstride, G, M, b0, shift, TW, n_dom, vb); break;
+    case 3: chunk<3, INV>(s, gstride, G, M, b0, shift, TW, n_dom, vb); break;
+    default: chunk<4, INV>(s, gstride, G, M, b0, shift, TW, n_dom, vb); break;
+  }
+}
+
+// All M local layers: DIF top-down for the forward transform, DIT bottom-up for
+// the inverse, in chunks of at most four layers.
+template <bool INV>
+__device__ __forceinline__ void run_layers(uint32_t* s, uint32_t gstride, unsigned G, unsigned M, unsigned shift,
+                           const uint32_t* TW, uint32_t n_dom, const uint32_t* vb) {
+  if (M == 0) return;
+  const unsigned nch = (M + 3) / 4, base = M / nch, extra = M % nch;
+  if (!INV) {
+    unsigned top = M;
+    for (unsigned c = 0; c < nch; ++c) {
+      const unsigned r = base + (c < extra ? 1 : 0);
+      chunk_dispatch<false>(r, s, gstride, G, M, top - r, shift, TW, n_dom, vb);
+      top -= r;
+      __syncthreads();
+    }
+  } else {
+    unsigned bot = 0;
+    for (unsigned c = 0; c < nch; ++c) {
+      const unsigned r = base + (c < extra ? 1 : 0);
+      chunk_dispatch<true>(r, s, gstride, G, M, bot, shift, TW, n_dom, vb);
+      bot += r;
+      __syncthreads();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass kernels. blockIdx.y = column; columns are `col_stride` words apart.
+// ---------------------------------------------------------------------------
+
+// Inverse layers [0, K) of a size-2^L transform. Reads natural-order evaluations
+// (the reference bit-reverses them first), writes position order to `tmp`.
+__global__ void __launch_bounds__(512) k_ifft_low(const uint32_t* __restrict__ in, size_t in_stride,
+                                                  uint32_t* __restrict__ tmp, unsigned L, unsigned K, unsigned G,
+                                                  const uint32_t* __restrict__ ITW) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t n = 1u << L, gsz = 1u << K, gstride = group_stride(K);
+  const unsigned hb = L - K;
+  uint32_t* vb = sm + G * gstride;
+  const uint32_t gp0 = blockIdx.x * G;
+  const uint32_t* col = in + (size_t)blockIdx.y * in_stride;
+  uint32_t* out = tmp + (size_t)blockIdx.y * n;
+  if (threadIdx.x < G) vb[threadIdx.x] = bitrev(gp0 + threadIdx.x, hb) << K;
+  const unsigned lg_g = 31 - __clz(G);
+  for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+    const uint32_t t = idx & (G - 1), v = idx >> lg_g;
+    sm[t * gstride + padx(bitrev(v, K))] = __ldg(col + ((size_t)v << hb) + gp0 + t);
+  }
+  __syncthreads();
+  run_layers<true>(sm, gstride, G, K, 0, ITW, n, vb);
+  for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+    const uint32_t t = idx >> K, e = idx & (gsz - 1);
+    out[vb[t] + e] = sm[t * gstride + padx(e)];
+  }
+}
+
+// Middle pass over groups that share the low K position bits (M = L - K layers).
+//   mode LDE:       inverse layers [K, L), scale 1/n, then for each of the 2^B
+//                   quarters the forward layers [K, L) of the size-2^(L+B) transform
+//                   (its top B layers only copy: the padded half is zero).
+//   mode IFFT_ONLY: inverse layers [K, L), scale 1/n, store de-interleaved (A then B).
+//   mode FFT_ONLY:  load A-then-B coefficients interleaved, forward layers [K, L).
+enum MidMode : int { MID_LDE = 0, MID_IFFT_ONLY = 1, MID_FFT_ONLY = 2 };
+
+__global__ void __launch_bounds__(512) k_mid(const uint32_t* __restrict__ in, size_t in_stride,
+                                             uint32_t* __restrict__ out, size_t out_stride, unsigned L, unsigned K,
+                                             unsigned B, unsigned G, const uint32_t* __restrict__ ITW_small,
+                                             const uint32_t* __restrict__ TW_big, int mode) {
+  extern __shared__ uint32_t sm[];
+  const unsigned M = L - K;
+  const uint32_t n = 1u << L, gsz = 1u << M, gstride = group_stride(M);
+  uint32_t* s_in = sm;
+  uint32_t* s_w = sm + G * gstride;
+  uint32_t* vb = s_w + G * gstride;
+  const uint32_t lo0 = blockIdx.x * G;
+  const uint32_t* src = in + (size_t)blockIdx.y * in_stride;
+  uint32_t* dst = out + (size_t)blockIdx.y * out_stride;
+  const unsigned lg_g = 31 - __clz(G);
+  if (threadIdx.x < G) vb[threadIdx.x] = 0;
+  if (mode == MID_FFT_ONLY) {
+    // interleaved position p holds A[p/2] (even p) or B[p/2] (odd p)
+    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
+      const uint32_t p = (hi << K) | (lo0 + t);
+      s_in[t * gstride + padx(hi)] = __ldg(src + ((p & 1) ? (n >> 1) + (p >> 1) : (p >> 1)));
+    }
+    __syncthreads();
+    run_layers<false>(s_in, gstride, G, M, K, TW_big, n << B, vb);
+    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
+      dst[((size_t)hi << K) + lo0 + t] = s_in[t * gstride + padx(hi)];
+    }
+    return;
+  }
+  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+    const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
+    s_in[t * gstride + padx(hi)] = __ldg(src + ((size_t)hi << K) + lo0 + t);
+  }
+  __syncthreads();
+  run_layers<true>(s_in, gstride, G, M, K, ITW_small, n, vb);
+  // 1/n = 2^(31 - L) mod p: scaling is a rotation of the 31-bit word.
+  const unsigned inv_n_shift = (31 - L) % 31;
+  if (mode == MID_IFFT_ONLY) {
+    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
+      const uint32_t p = (hi << K) | (lo0 + t);
+      const uint32_t v = mshl(s_in[t * gstride + padx(hi)], inv_n_shift);
+      dst[(p & 1) ? (n >> 1) + (p >> 1) : (p >> 1)] = v;
+    }
+    return;
+  }
+  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+    const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
+    const uint32_t a = t * gstride + padx(hi);
+    s_in[a] = mshl(s_in[a], inv_n_shift);
+  }
+  __syncthreads();
+  for (uint32_t q = 0; q < (1u << B); ++q) {
+    for (uint32_t idx = threadIdx.x; idx < G * gstride; idx += blockDim.x) s_w[idx] = s_in[idx];
+    if (threadIdx.x < G) vb[threadIdx.x] = q << M;
+    __syncthreads();
+    run_layers<false>(s_w, gstride, G, M, K, TW_big, n << B, vb);
+    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
+      dst[(size_t)q * n + ((size_t)hi << K) + lo0 + t] = s_w[t * gstride + padx(hi)];
+    }
+    __syncthreads();
+  }
+}
+
+// Forward layers [0, K) of a size-2^LB transform over contiguous groups, then the
+// reference's final bit reversal on the store (natural-order evaluations).
+__global__ void __launch_bounds__(512) k_fft_low(const uint32_t* __restrict__ mid, size_t mid_stride,
+                                                 uint32_t* __restrict__ out, size_t out_stride, unsigned LB,
+                                                 unsigned K, unsigned G, const uint32_t* __restrict__ TW) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t N = 1u << LB, gsz = 1u << K, gstride = group_stride(K);
+  const unsigned hb = LB - K;
+  uint32_t* vb = sm + G * gstride;
+  const uint32_t q0 = blockIdx.x * G;
+  const uint32_t* src = mid + (size_t)blockIdx.y * mid_stride;
+  uint32_t* dst = out + (size_t)blockIdx.y * out_stride;
+  if (threadIdx.x < G) vb[threadIdx.x] = bitrev(q0 + threadIdx.x, hb) << K;
+  __syncthreads();
+  for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+    const uint32_t t = idx >> K, e = idx & (gsz - 1);
+    sm[t * gstride + padx(e)] = __ldg(src + vb[t] + e);
+  }
+  __syncthreads();
+  run_layers<false>(sm, gstride, G, K, 0, TW, N, vb);
+  const unsigned lg_g = 31 - __clz(G);
+  for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+    const uint32_t t = idx & (G - 1), v = idx >> lg_g;
+    dst[((size_t)v << hb) + q0 + t] = sm[t * gstride + padx(bitrev(v, K))];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host launch helpers
+// ---------------------------------------------------------------------------
+
+namespace {
+constexpr unsigned kThreads = 512;
+constexpr uint32_t kGroupWords = 16384;  // words of group data per shared buffer
+
+unsigned pick_split(unsigned L) {
+  unsigned k = L <= 20 ? (L < 10 ? L : 10) : (L + 1) / 2;
+  return k;
+}
+unsigned pick_groups(unsigned M, uint32_t n_groups) {
+  uint32_t g = kGroupWords >> M;
+  if (g == 0) g = 1;
+  if (g > 16) g = 16;
+  if (g > n_groups) g = n_groups;
+  return g;
+}
+size_t smem_bytes(unsigned M, unsigned G, unsigned buffers) {
+  return ((size_t)buffers * G * group_stride(M) + G) * sizeof(uint32_t);
+}
+void set_smem(const void* fn, size_t bytes) {
+  ZS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+}  // namespace
+
+size_t lde_scratch_words(unsigned L, unsigned B, uint32_t C) {
+  // tmp (C * 2^L) + mid (C * 2^(L+B))
+  return (size_t)C * (((size_t)1 << L) + ((size_t)1 << (L + B)));
+}
+
+void circle_lde(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, size_t out_stride, uint32_t C,
+                unsigned L, unsigned B, const CircleDomain& small, const CircleDomain& big, uint32_t* scratch,
+                cudaStream_t st) {
+  if (small.lg != L || big.lg != L + B) throw Error(ZS_EGENERIC, "circle_lde: domain mismatch");
+  const unsigned K = pick_split(L);
+  const uint32_t n = 1u << L;
+  uint32_t* tmp = scratch;
+  uint32_t* mid = scratch + (size_t)C * n;
+  {
+    const uint32_t ngroups = 1u << (L - K);
+    const unsigned G = pick_groups(K, ngroups);
+    const size_t sb = smem_bytes(K, G, 1);
+    set_smem((const void*)k_ifft_low, sb);
+    k_ifft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_in, in_stride, tmp, L, K, G, small.itw);
+  }
+  {
+    const unsigned M = L - K;
+    const uint32_t ngroups = 1u << K;
+    const unsigned G = pick_groups(M, ngroups);
+    const size_t sb = smem_bytes(M, G, 2);
+    set_smem((const void*)k_mid, sb);
+    k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(tmp, n, mid, (size_t)n << B, L, K, B, G, small.itw, big.tw,
+                                                      MID_LDE);
+  }
+  {
+    const unsigned LB = L + B;
+    const uint32_t ngroups = 1u << (LB - K);
+    const unsigned G = pick_groups(K, ngroups);
+    const size_t sb = smem_bytes(K, G, 1);
+    set_smem((const void*)k_fft_low, sb);
+    k_fft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(mid, (size_t)n << B, d_out, out_stride, LB, K, G, big.tw);
+  }
+  ZS_CUDA(cudaGetLastError());
+}
+
+void circle_fft(const uint32_t* d_coeffs, uint32_t* d_evals, uint32_t C, const CircleDomain& dom, uint32_t* scratch,
+                cudaStream_t st) {
+  const unsigned L = dom.lg, K = pick_split(L), M = L - K;
+  const uint32_t n = 1u << L;
+  {
+    const uint32_t ngroups = 1u << K;
+    const unsigned G = pick_groups(M, ngroups);
+    const size_t sb = smem_bytes(M, G, 2);
+    set_smem((const void*)k_mid, sb);
+    k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_coeffs, n, scratch, n, L, K, 0, G, dom.itw, dom.tw,
+                                                      MID_FFT_ONLY);
+  }
+  {
+    const uint32_t ngroups = 1u << (L - K);
+    const unsigned G = pick_groups(K, ngroups);
+    const size_t sb = smem_bytes(K, G, 1);
+    set_smem((const void*)k_fft_low, sb);
+    k_fft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(scratch, n, d_evals, n, L, K, G, dom.tw);
+  }
+  ZS_CUDA(cudaGetLastError());
+}
+
+void circle_ifft(const uint32_t* d_evals, uint32_t* d_coeffs, uint32_t C, const CircleDomain& dom, uint32_t* scratch,
+                 cudaStream_t st) {
+  const unsigned L = dom.lg, K = pick_split(L), M = L - K;
+  const uint32_t n = 1u << L;
+  {
+    const uint32_t ngroups = 1u << (L - K);
+    const unsigned G = pick_groups(K, ngroups);
+    const size_t sb = smem_bytes(K, G, 1);
+    set_smem((const void*)k_ifft_low, sb);
+    k_ifft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_evals, n, scratch, L, K, G, dom.itw);
+  }
+  {
+    const uint32_t ngroups = 1u << K;
+    const unsigned G = pick_groups(M, ngroups);
+    const size_t sb = smem_bytes(M, G, 2);
+    set_smem((const void*)k_mid, sb);
+    k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(scratch, n, d_coeffs, n, L, K, 0, G, dom.itw, dom.tw,
+                                                      MID_IFFT_ONLY);
+  }
+  ZS_CUDA(cudaGetLastError());
+}
+
+}  // namespace zs

@@ -1,0 +1,114 @@
+// FRI fold over QM31 fused with the commitment of the folded layer.
+//
+// fri.zig:209-219 folds y0 = L[j], y1 = L[j + n/2] at x = D_i[j] into
+//   (y0 + y1) * inv2 + alpha * ((y0 - y1) * x^-1 * inv2).
+// x^-1 is rebuilt from tables instead of a per-point inversion: D_i[j] is a unit of
+// the QM31 ring, so its inverse is unique and equals
+// (FRI_OFFSET^(2^i))^-1 * w_0^-(j * 2^i), w_0 = primitiveRootOfUnity(dlog). inv2 = 2^30.
+#include "blake3.cuh"
+#include "fri.cuh"
+
+namespace zs {
+
+__global__ void k_fold_tables(qm31 w0inv, qm31* tabs) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 3 * 2048) return;
+  const uint32_t which = k / 2048, e = k % 2048;
+  // w0inv^(e * 2^(11 * which))
+  qm31 base = w0inv;
+  for (uint32_t s = 0; s < 11 * which; ++s) base = qmul(base, base);
+  tabs[k] = qpow(base, e);
+}
+
+FoldTables::FoldTables(unsigned d, cudaStream_t st) : dlog(d) {
+  if (dlog > 32) throw Error(ZS_EMALFORMED, "FRI domain log size above 32");
+  ZS_CUDA(cudaMallocAsync(&tables, 3 * 2048 * sizeof(qm31), st));
+  const qm31 w0 = q_root_of_unity(dlog);
+  k_fold_tables<<<(3 * 2048 + 255) / 256, 256, 0, st>>>(qinv(w0), tables);
+  ZS_CUDA(cudaGetLastError());
+}
+FoldTables::~FoldTables() { cudaFree(tables); }
+
+qm31 FoldTables::offset_inv(unsigned layer) const { return qinv(qpow(q_fri_offset(), (uint64_t)1 << layer)); }
+
+namespace {
+constexpr unsigned kRun = 256;
+constexpr unsigned kSPad = kRun + 1;
+}  // namespace
+
+__device__ __forceinline__ qm31 ld_q(const qm31* p) {
+  const uint4 r = __ldg(reinterpret_cast<const uint4*>(p));
+  return qmake(r.x, r.y, r.z, r.w);
+}
+
+__global__ void __launch_bounds__(kRun) k_fold(const qm31* __restrict__ in, qm31* __restrict__ out, uint32_t half,
+                                               qm31 alpha, qm31 off_inv, unsigned layer,
+                                               const qm31* __restrict__ tabs, uint32_t* tree_words,
+                                               unsigned log_next) {
+  __shared__ uint32_t d[8 * kSPad];
+  const uint64_t first = (uint64_t)blockIdx.x * blockDim.x;
+  const uint32_t j = (uint32_t)(first + threadIdx.x);
+  const qm31 y0 = ld_q(in + j), y1 = ld_q(in + j + half);
+  const uint64_t k = (uint64_t)j << layer;
+  qm31 xinv = qmul(ld_q(tabs + (k & 2047)), ld_q(tabs + 2048 + ((k >> 11) & 2047)));
+  if (k >> 22) xinv = qmul(xinv, ld_q(tabs + 4096 + ((k >> 22) & 2047)));
+  xinv = qmul(xinv, off_inv);
+  constexpr uint32_t inv2 = 1u << 30;
+  const qm31 hs = qmul_m(qadd(y0, y1), inv2);
+  const qm31 hd = qmul_m(qmul(qsub(y0, y1), xinv), inv2);
+  const qm31 r = qadd(hs, qmul(alpha, hd));
+  reinterpret_cast<uint4*>(out)[j] = make_uint4(r.a.a, r.a.b, r.b.a, r.b.b);
+  if (!tree_words) return;
+  uint32_t o[8];
+  b3::hash_qm31(r, o);
+  {
+    uint4* dst = reinterpret_cast<uint4*>(tree_words + 8 * (size_t)j);
+    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+  }
+#pragma unroll
+  for (int w = 0; w < 8; ++w) d[w * kSPad + threadIdx.x] = o[w];
+  __syncthreads();
+  // climb the run's subtree (same scheme as the Merkle leaf kernels)
+  const size_t N2 = (size_t)2 << log_next;
+  unsigned lvl = 0;
+  for (unsigned cnt = blockDim.x >> 1; cnt >= 1; cnt >>= 1) {
+    ++lvl;
+    const unsigned t = threadIdx.x;
+    uint32_t oo[8];
+    const bool act = t < cnt;
+    if (act) {
+      uint32_t l[8], rr[8];
+#pragma unroll
+      for (int w = 0; w < 8; ++w) {
+        l[w] = d[w * kSPad + 2 * t];
+        rr[w] = d[w * kSPad + 2 * t + 1];
+      }
+      b3::hash2(l, rr, oo);
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int w = 0; w < 8; ++w) d[w * kSPad + t] = oo[w];
+      const uint64_t idx = (first >> lvl) + t;
+      uint4* dst = reinterpret_cast<uint4*>(tree_words + 8 * (N2 - (N2 >> lvl) + idx));
+      dst[0] = make_uint4(oo[0], oo[1], oo[2], oo[3]);
+      dst[1] = make_uint4(oo[4], oo[5], oo[6], oo[7]);
+    }
+    __syncthreads();
+  }
+}
+
+void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31& alpha, unsigned layer,
+              const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st) {
+  const unsigned threads = half >= kRun ? kRun : half;
+  unsigned run_log = 0;
+  while ((1u << run_log) < threads) ++run_log;
+  k_fold<<<half / threads, threads, 0, st>>>(d_in, d_out, half, alpha, tabs.offset_inv(layer), layer, tabs.tables,
+                                             next_tree ? next_tree->words : nullptr,
+                                             next_tree ? next_tree->log_n : 0);
+  ZS_CUDA(cudaGetLastError());
+  if (next_tree) tree_finish(*next_tree, run_log, st);
+}
+
+}  // namespace zs

@@ -1,0 +1,27 @@
+// FRI folding over QM31 on the device (src/m31/fri.zig).
+#pragma once
+#include "merkle.cuh"
+
+namespace zs {
+
+// Inverse domain points of the FRI layers of a size-2^dlog domain
+// (D_i[j] = FRI_OFFSET^(2^i) * w_{dlog-i}^j, fri.zig:96-117): w_0^-k is the
+// product of three 2^11-entry tables, so any k < 2^33 costs two QM31 products.
+struct FoldTables {
+  unsigned dlog = 0;
+  qm31* tables = nullptr;  // 3 * 2048 entries
+  explicit FoldTables(unsigned dlog, cudaStream_t st);
+  ~FoldTables();
+  FoldTables(const FoldTables&) = delete;
+  FoldTables& operator=(const FoldTables&) = delete;
+  // (FRI_OFFSET^(2^layer))^-1, host-side.
+  qm31 offset_inv(unsigned layer) const;
+};
+
+// One fold (fri.zig:209-219): out[j] = (y0 + y1)/2 + alpha * (y0 - y1) / (2 D_layer[j]),
+// y0 = in[j], y1 = in[j + half], for j < half. When `next_tree` is given, also
+// writes the leaves hashQM31(out[j]) and the whole tree of the folded layer.
+void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31& alpha, unsigned layer,
+              const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st);
+
+}  // namespace zs

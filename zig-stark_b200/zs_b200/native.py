@@ -1,0 +1,222 @@
+"""ctypes binding of ``libzs_b200.so`` (the C ABI in include/zs_m31.h).
+
+The GPU library is the only implementation behind these calls: there is no CPU
+fallback, and loading fails loudly when the library has not been built.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzs_b200.so")
+_lib = None
+
+u8p = ctypes.POINTER(ctypes.c_uint8)
+u32p = ctypes.POINTER(ctypes.c_uint32)
+
+ERRORS = {-1: "generic error", -2: "malformed input", -3: "out of memory", -4: "protocol error",
+          -5: "device error"}
+
+
+class ZsError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"{what} failed: {code} ({ERRORS.get(code, 'unknown')})")
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `make -C zig-stark_b200` "
+                              "(or __graft_entry__.build()) first")
+        L = ctypes.CDLL(LIB_PATH)
+        L.zs_version.restype = ctypes.c_char_p
+        L.zs_m31_circle_fft.argtypes = [u32p, ctypes.c_uint32] + [ctypes.c_uint32] * 5 + [u32p]
+        L.zs_m31_circle_ifft.argtypes = [u32p, ctypes.c_uint32] + [ctypes.c_uint32] * 5 + [u32p]
+        L.zs_m31_commit_plan_create.argtypes = [ctypes.c_uint32] * 4 + [ctypes.POINTER(ctypes.c_void_p)]
+        L.zs_m31_commit_plan_destroy.argtypes = [ctypes.c_void_p]
+        L.zs_m31_commit_plan_destroy.restype = None
+        L.zs_m31_commit_plan_set_challenges.argtypes = [ctypes.c_void_p, u32p, u32p]
+        L.zs_m31_commit_plan_trace_buffer.argtypes = [ctypes.c_void_p]
+        L.zs_m31_commit_plan_trace_buffer.restype = ctypes.c_void_p
+        L.zs_m31_commit_plan_upload.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.zs_m31_commit_plan_run_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.zs_m31_commit_plan_run_phase.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                                    ctypes.c_void_p]
+        L.zs_m31_commit_plan_results.argtypes = [ctypes.c_void_p, ctypes.c_void_p, u8p, u8p, u32p]
+        L.zs_m31_commit_plan_copy_lde.argtypes = [ctypes.c_void_p, u32p]
+        L.zs_m31_commit_plan_copy_layer.argtypes = [ctypes.c_void_p, ctypes.c_uint32, u32p]
+        L.zs_m31_commit_plan_launches.argtypes = [ctypes.c_void_p]
+        L.zs_m31_commit_plan_launches.restype = ctypes.c_uint32
+        L.zs_m31_circle_commit.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u32p, u32p,
+                                           ctypes.c_uint32, u8p, u8p, u32p]
+        _lib = L
+    return _lib
+
+
+def check(rc, what):
+    if rc != 0:
+        raise ZsError(rc, what)
+
+
+def _u32(a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return a, a.ctypes.data_as(u32p)
+
+
+def version():
+    return lib().zs_version().decode()
+
+
+# ---------------------------------------------------------------------------
+# circle FFT (src/cuda/circlefft_gpu.zig:46-175)
+# ---------------------------------------------------------------------------
+
+P = 2147483647
+
+
+def _pt_add(a, b):
+    return ((a[0] * b[0] - a[1] * b[1]) % P, (a[0] * b[1] + a[1] * b[0]) % P)
+
+
+def _pt_mul(pt, k):
+    r = (1, 0)
+    while k:
+        if k & 1:
+            r = _pt_add(r, pt)
+        pt = _pt_add(pt, pt)
+        k >>= 1
+    return r
+
+
+def canonic_half_coset(log_size):
+    """CircleCoset.canonicHalf(log_size) (coset.zig:59-65) as (offset, step, log_half)."""
+    gen_neg = (1268011823, P - 2)
+    return _pt_mul(gen_neg, 1 << (30 - log_size)), _pt_mul(gen_neg, 1 << (32 - log_size)), log_size - 1
+
+
+def circle_fft(coeffs, half_coset=None):
+    """circleFFT: A-then-B coefficients -> natural-order evaluations on
+    half_coset ++ conjugate. `coeffs` is (n,) or (columns, n); `half_coset` =
+    (offset, step, log_half), default canonicHalf(log2 n)."""
+    return _circle(coeffs, half_coset, inverse=False)
+
+
+def circle_ifft(evals, half_coset=None):
+    """circleIFFT: natural-order evaluations -> A-then-B coefficients."""
+    return _circle(evals, half_coset, inverse=True)
+
+
+def _circle(x, half_coset, inverse):
+    x, p = _u32(x)
+    n = x.shape[-1]
+    cols = x.size // n
+    log_n = n.bit_length() - 1
+    if (1 << log_n) != n or n < 2:
+        raise ValueError("transform length must be a power of two >= 2")
+    if half_coset is None:
+        half_coset = canonic_half_coset(log_n)
+    (ox, oy), (sx, sy), log_half = half_coset
+    if log_half + 1 != log_n:
+        raise ValueError("half coset size does not match the transform length")
+    out = np.empty_like(x)
+    fn = lib().zs_m31_circle_ifft if inverse else lib().zs_m31_circle_fft
+    check(fn(p, cols, ox, oy, sx, sy, log_half, out.ctypes.data_as(u32p)),
+          "zs_m31_circle_ifft" if inverse else "zs_m31_circle_fft")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# circle commit workload
+# ---------------------------------------------------------------------------
+
+class CommitPlan:
+    """Device-resident plan of the circle commit workload (zs_m31_commit_plan_*)."""
+
+    def __init__(self, n_columns, log_rows, log_blowup, n_folds):
+        self.n_columns, self.log_rows, self.log_blowup, self.n_folds = n_columns, log_rows, log_blowup, n_folds
+        h = ctypes.c_void_p()
+        check(lib().zs_m31_commit_plan_create(n_columns, log_rows, log_blowup, n_folds, ctypes.byref(h)),
+              "zs_m31_commit_plan_create")
+        self._h = h
+
+    def close(self):
+        if self._h:
+            lib().zs_m31_commit_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_challenges(self, gammas, alphas):
+        g, pg = _u32(gammas)
+        a, pa = _u32(alphas if self.n_folds else np.zeros(4, np.uint32))
+        check(lib().zs_m31_commit_plan_set_challenges(self._h, pg, pa), "zs_m31_commit_plan_set_challenges")
+
+    def trace_ptr(self):
+        return lib().zs_m31_commit_plan_trace_buffer(self._h)
+
+    def upload(self, trace, stream=None):
+        """trace: host array (n_columns, 2^log_rows); pinned memory makes the copy asynchronous."""
+        if isinstance(trace, np.ndarray):
+            trace = np.ascontiguousarray(trace, dtype=np.uint32)
+            ptr = trace.ctypes.data
+        else:
+            ptr = int(trace)
+        check(lib().zs_m31_commit_plan_upload(self._h, ctypes.c_void_p(ptr), ctypes.c_void_p(stream or 0)),
+              "zs_m31_commit_plan_upload")
+
+    def run(self, d_trace=None, stream=None):
+        check(lib().zs_m31_commit_plan_run_device(self._h, ctypes.c_void_p(d_trace or 0),
+                                                  ctypes.c_void_p(stream or 0)), "zs_m31_commit_plan_run_device")
+
+    PHASES = ("lde", "row_tree", "folds")
+
+    def run_phase(self, phase, d_trace=None, stream=None):
+        check(lib().zs_m31_commit_plan_run_phase(self._h, phase, ctypes.c_void_p(d_trace or 0),
+                                                 ctypes.c_void_p(stream or 0)), "zs_m31_commit_plan_run_phase")
+
+    def results(self, stream=None):
+        root = (ctypes.c_uint8 * 32)()
+        layer_roots = np.zeros((self.n_folds, 32), dtype=np.uint8)
+        final = np.zeros((1 << (self.log_rows + self.log_blowup - self.n_folds), 4), dtype=np.uint32)
+        check(lib().zs_m31_commit_plan_results(self._h, ctypes.c_void_p(stream or 0), root,
+                                               layer_roots.ctypes.data_as(u8p), final.ctypes.data_as(u32p)),
+              "zs_m31_commit_plan_results")
+        return {"lde_root": bytes(root), "layer_roots": layer_roots, "final_layer": final}
+
+    def lde(self):
+        out = np.zeros((self.n_columns, 1 << (self.log_rows + self.log_blowup)), dtype=np.uint32)
+        check(lib().zs_m31_commit_plan_copy_lde(self._h, out.ctypes.data_as(u32p)), "zs_m31_commit_plan_copy_lde")
+        return out
+
+    def layer(self, i):
+        out = np.zeros((1 << (self.log_rows + self.log_blowup - i), 4), dtype=np.uint32)
+        check(lib().zs_m31_commit_plan_copy_layer(self._h, i, out.ctypes.data_as(u32p)),
+              "zs_m31_commit_plan_copy_layer")
+        return out
+
+    def launches(self):
+        return int(lib().zs_m31_commit_plan_launches(self._h))
+
+
+def circle_commit(trace, log_blowup, gammas, alphas):
+    """One-shot host-buffer call (zs_m31_circle_commit)."""
+    trace, pt = _u32(trace)
+    n_cols, n = trace.shape
+    log_rows = n.bit_length() - 1
+    g, pg = _u32(gammas)
+    a, pa = _u32(alphas)
+    n_folds = a.size // 4
+    root = (ctypes.c_uint8 * 32)()
+    layer_roots = np.zeros((max(n_folds, 1), 32), dtype=np.uint8)
+    final = np.zeros((1 << (log_rows + log_blowup - n_folds), 4), dtype=np.uint32)
+    check(lib().zs_m31_circle_commit(pt, n_cols, log_rows, log_blowup, pg, pa, n_folds, root,
+                                     layer_roots.ctypes.data_as(u8p), final.ctypes.data_as(u32p)),
+          "zs_m31_circle_commit")
+    return {"lde_root": bytes(root), "layer_roots": layer_roots[:n_folds], "final_layer": final}
