@@ -36,6 +36,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--log-rows", type=int, default=LOG_ROWS, help="smaller cases for profiling")
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
@@ -165,8 +167,9 @@ def main():
     from zs_b200 import workload as wl
 
     torch.cuda.set_device(local)
-    trace, gammas, alphas = wl.commit_inputs(N_COLS, LOG_ROWS, N_FOLDS)
-    plan = native.CommitPlan(N_COLS, LOG_ROWS, LOG_BLOWUP, N_FOLDS)
+    log_rows = args.log_rows
+    trace, gammas, alphas = wl.commit_inputs(N_COLS, log_rows, N_FOLDS)
+    plan = native.CommitPlan(N_COLS, log_rows, LOG_BLOWUP, N_FOLDS)
     plan.set_challenges(gammas, alphas)
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
@@ -217,22 +220,24 @@ def main():
 
     # end to end through the C ABI: H2D of the trace from pinned memory, run, read back
     h2d = trace.nbytes
-    d2h = 32 + 32 * N_FOLDS + (1 << (LOG_ROWS + LOG_BLOWUP - N_FOLDS)) * 16
-    for _ in range(args.warmup):
-        plan.upload(pinned.data_ptr(), sp)
-        plan.run(None, sp)
-        plan.results(sp)
-    barrier(world)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        plan.upload(pinned.data_ptr(), sp)
-        plan.run(None, sp)
-        r = plan.results(sp)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world) / args.steps
-    assert r["lde_root"] == ref_root, "e2e run changed the LDE root"
+    d2h = 32 + 32 * N_FOLDS + (1 << (log_rows + LOG_BLOWUP - N_FOLDS)) * 16
+    e2e_s = float("nan")
+    if not args.no_e2e:
+        for _ in range(args.warmup):
+            plan.upload(pinned.data_ptr(), sp)
+            plan.run(None, sp)
+            plan.results(sp)
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            plan.upload(pinned.data_ptr(), sp)
+            plan.run(None, sp)
+            r = plan.results(sp)
+        e2e_s = max_over_ranks(time.perf_counter() - t0, world) / args.steps
+        assert r["lde_root"] == ref_root, "e2e run changed the LDE root"
 
-    rows = (1 << LOG_ROWS) * world
+    rows = (1 << log_rows) * world
     value = rows / (ms_step / 1e3)
     peaks = {}
     try:
@@ -241,7 +246,7 @@ def main():
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     # dominant phase and its algorithmic bytes (inputs and outputs it must touch)
-    n, N = 1 << LOG_ROWS, 1 << (LOG_ROWS + LOG_BLOWUP)
+    n, N = 1 << log_rows, 1 << (log_rows + LOG_BLOWUP)
     alg = {
         "lde": N_COLS * (n + N) * 4,                      # read trace, write LDE
         "row_tree": N_COLS * N * 4 + (2 * N - 1) * 32 * 2 + N * 16,  # read LDE, write 2 trees + g
@@ -255,7 +260,7 @@ def main():
         "vs_baseline": None, "dtype": "u32 (M31 / QM31 exact)", "data": "synthetic (SplitMix64 seeded)",
         "config": {"workload": "circle commit: 64 cols x 2^20 M31, blowup 4, row-leaf Blake3 Merkle, "
                                "16-fold QM31 FRI chain with per-layer commits",
-                   "columns": N_COLS, "log_rows": LOG_ROWS, "log_blowup": LOG_BLOWUP, "folds": N_FOLDS,
+                   "columns": N_COLS, "log_rows": log_rows, "log_blowup": LOG_BLOWUP, "folds": N_FOLDS,
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)"},
         "phases_ms": phase_ms,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
@@ -268,7 +273,7 @@ def main():
         "gpu_launches": plan.launches() * args.steps,
         "clocks": clocks.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and log_rows == LOG_ROWS:
         line["cpu_baseline"] = cpu_baseline_sample(os.cpu_count() or 1)
     if rank == 0:
         print(json.dumps(line), flush=True)
