@@ -112,6 +112,22 @@ int32_t zs_m31_circle_commit(const uint32_t *trace, uint32_t n_columns, uint32_t
                              const uint32_t *gammas, const uint32_t *alphas, uint32_t n_folds, uint8_t *lde_root,
                              uint8_t *layer_roots, uint32_t *final_layer);
 
+/* ---- allocation-free circle LDE --------------------------------------------
+ * No counterpart in the reference. For callers that cannot call cudaMalloc (a plugin
+ * whose host process reserves all device memory up front in its own arena, or a
+ * latency-bound loop where an allocation may synchronize the device): the circle
+ * low-degree extension of zs_m31_commit_plan's first phase, with the caller's device
+ * buffers for input (n_columns x 2^log_rows words, column-major, natural order on
+ * canonicHalf(log_rows)) and output (n_columns x 2^(log_rows+log_blowup) words), and
+ * every other word it needs in one fixed 16 MiB device array inside the library.
+ * It allocates nothing. Limit: 2*2^L + 2*2^(L+B) + n_columns*(2^L + 2^(L+B)) words
+ * <= 2^22 (L = log_rows, B = log_blowup); larger requests return -2. All calls share
+ * the array, so calls whose GPU work overlaps race; the first call on a device looks
+ * up the array's address and should come before any stream capture. Asynchronous on
+ * `stream` (a cudaStream_t; NULL = default stream). */
+int32_t zs_m31_circle_lde_noalloc(const uint32_t *d_in, uint32_t *d_out, uint32_t n_columns, uint32_t log_rows,
+                                  uint32_t log_blowup, void *stream);
+
 /* Release a buffer returned by the ABI (zig-capi.h:73-74). */
 void zs_free(zs_host_allocator host, uint8_t *ptr, size_t len);
 

@@ -469,4 +469,60 @@ void circle_ifft(const uint32_t* d_evals, uint32_t* d_coeffs, uint32_t C, const 
   ZS_CUDA(cudaGetLastError());
 }
 
+// ---------------------------------------------------------------------------
+// Table-parameterised variants for callers that own every buffer (the
+// allocation-free entry point in noalloc.cu): the canonic domain's tables are
+// written into caller memory, and the LDE takes the tables directly.
+// ---------------------------------------------------------------------------
+
+void circle_twiddles_into(unsigned lg, uint32_t* tw, uint32_t* itw, cudaStream_t st) {
+  cpoint offset, step;
+  canonic_half(lg, &offset, &step);
+  const uint32_t n = 1u << lg;
+  if (lg <= 2) {
+    k_tw_small<<<1, 32, 0, st>>>(lg, offset, tw);
+  } else {
+    const uint32_t r = 1u << (lg - 2);
+    k_tw_tree<<<(r + 255) / 256, 256, 0, st>>>(lg, offset, step, tw);
+    const uint32_t k = 1u << (lg - 3);
+    k_tw_circle_layer<<<(k + 255) / 256, 256, 0, st>>>(lg, tw);
+  }
+  k_invert<<<(n + 255) / 256, 256, 0, st>>>(tw, itw, n);
+  ZS_CUDA(cudaGetLastError());
+}
+
+void circle_lde_tables(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, size_t out_stride, uint32_t C,
+                       unsigned L, unsigned B, const uint32_t* itw_small, const uint32_t* tw_big, uint32_t* scratch,
+                       cudaStream_t st) {
+  const unsigned K = pick_split(L);
+  const uint32_t n = 1u << L;
+  uint32_t* tmp = scratch;
+  uint32_t* mid = scratch + (size_t)C * n;
+  {
+    const uint32_t ngroups = 1u << (L - K);
+    const unsigned G = pick_groups(K, ngroups);
+    const size_t sb = smem_bytes(K, G, 1);
+    set_smem((const void*)k_ifft_low, sb);
+    k_ifft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_in, in_stride, tmp, L, K, G, itw_small);
+  }
+  {
+    const unsigned M = L - K;
+    const uint32_t ngroups = 1u << K;
+    const unsigned G = pick_groups(M, ngroups);
+    const size_t sb = smem_bytes(M, G, 2);
+    set_smem((const void*)k_mid, sb);
+    k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(tmp, n, mid, (size_t)n << B, L, K, B, G, itw_small, tw_big,
+                                                      MID_LDE);
+  }
+  {
+    const unsigned LB = L + B;
+    const uint32_t ngroups = 1u << (LB - K);
+    const unsigned G = pick_groups(K, ngroups);
+    const size_t sb = smem_bytes(K, G, 1);
+    set_smem((const void*)k_fft_low, sb);
+    k_fft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(mid, (size_t)n << B, d_out, out_stride, LB, K, G, tw_big);
+  }
+  ZS_CUDA(cudaGetLastError());
+}
+
 }  // namespace zs

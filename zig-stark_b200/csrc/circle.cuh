@@ -42,4 +42,13 @@ void circle_fft(const uint32_t* d_coeffs, uint32_t* d_evals, uint32_t C, const C
 void circle_ifft(const uint32_t* d_evals, uint32_t* d_coeffs, uint32_t C, const CircleDomain& dom, uint32_t* scratch,
                  cudaStream_t st);
 
+// Forward and inverse tables of the canonic domain of size 2^lg written into caller
+// memory (2^lg words each), and circle_lde with the tables passed directly
+// (itw_small: inverse table of the 2^L domain, tw_big: forward table of the 2^(L+B)
+// domain; scratch: lde_scratch_words(L, B, C) words).
+void circle_twiddles_into(unsigned lg, uint32_t* tw, uint32_t* itw, cudaStream_t st);
+void circle_lde_tables(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, size_t out_stride, uint32_t C,
+                       unsigned L, unsigned B, const uint32_t* itw_small, const uint32_t* tw_big, uint32_t* scratch,
+                       cudaStream_t st);
+
 }  // namespace zs

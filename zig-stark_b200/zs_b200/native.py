@@ -52,6 +52,8 @@ def lib():
         L.zs_m31_commit_plan_launches.restype = ctypes.c_uint32
         L.zs_m31_circle_commit.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u32p, u32p,
                                            ctypes.c_uint32, u8p, u8p, u32p]
+        L.zs_m31_circle_lde_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -220,3 +222,10 @@ def circle_commit(trace, log_blowup, gammas, alphas):
                                      layer_roots.ctypes.data_as(u8p), final.ctypes.data_as(u32p)),
           "zs_m31_circle_commit")
     return {"lde_root": bytes(root), "layer_roots": layer_roots[:n_folds], "final_layer": final}
+
+
+def circle_lde_noalloc(d_in, d_out, n_columns, log_rows, log_blowup, stream=None):
+    """zs_m31_circle_lde_noalloc on caller-owned device buffers (device pointers as
+    ints); returns the C ABI status code."""
+    return int(lib().zs_m31_circle_lde_noalloc(ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), n_columns, log_rows,
+                                               log_blowup, ctypes.c_void_p(stream or 0)))
