@@ -51,6 +51,24 @@ enum {
     ZS_AIR_LINEAR_EXAMPLE = 6
 };
 
+/* ---- prover ------------------------------------------------------------------
+ * Replaces GenericStark(Air).proveWithPreprocessed (src/m31/stark.zig:327-658) and
+ * prove (stark.zig:303-311); the conventions are zs_binius_prove's (zig-capi.h:41-51).
+ *   params         wire StarkParams {u8 trace_log, u8 log_blowup, usize num_queries,
+ *                  u8 remainder_log} (stark.zig:75-90)
+ *   public_inputs  wire Air.PublicInputs of `air_id`
+ *   preprocessed   wire []const []const QM31 (empty buffer or a zero-length slice when
+ *                  the AIR has none), trace: wire []const []const QM31
+ *   channel_sep    the domain separator passed to Channel.init (channel.zig:16-21)
+ * On success *out_proof / *out_len hold the serialized GenericStark(Air).Proof
+ * (stark.zig:107-122), allocated with `host` and released with zs_free. The proof is
+ * byte-identical to the reference prover's for the same inputs. Parameters the
+ * reference asserts on (stark.zig:230-232, fri.zig:228) return -4. */
+int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t *params, size_t params_len,
+                     const uint8_t *public_inputs, size_t public_inputs_len, const uint8_t *preprocessed,
+                     size_t preprocessed_len, const uint8_t *trace, size_t trace_len, const uint8_t *channel_sep,
+                     size_t channel_sep_len, uint8_t **out_proof, size_t *out_len);
+
 /* ---- circle FFT -------------------------------------------------------------
  * Replaces src/cuda/circlefft_gpu.zig:46-108 circleFFT(allocator, coeffs, half_coset,
  * evals) and :111-175 circleIFFT(...), themselves GPU versions of

@@ -1,0 +1,85 @@
+"""GPU prover (zs_m31_prove) byte-identical to the oracle's GenericStark proofs, and
+accepted by the oracle verifier, for every compiled-in AIR."""
+import numpy as np
+import pytest
+
+from zs_b200 import wire
+from zs_b200 import workload as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(orc, air, params, pi, trace, pre=(), sep=b"s", valid=True):
+    from zs_b200 import native
+    pre_b = wire.columns(list(pre)) if len(pre) else b""
+    got = native.prove(air, params, pi, trace, pre_b, sep)
+    want = orc.prove(air, params.encode(), pi, pre_b, wire.columns(trace), sep, mode=1)
+    assert got == want
+    assert orc.verify(air, params.encode(), pi, got, sep) == valid
+    return got
+
+
+@pytest.mark.parametrize("trace_log,log_blowup,nq,rem", [(4, 3, 12, 3), (8, 3, 16, 3), (1, 2, 4, 2), (2, 1, 8, 2),
+                                                         (6, 2, 16, 3), (10, 1, 20, 4), (12, 2, 16, 3)])
+def test_fib(orc, trace_log, log_blowup, nq, rem):
+    tr = wl.fib_trace(1 << trace_log)
+    _check(orc, wl.AIR_FIB, wire.StarkParams(trace_log, log_blowup, nq, rem), wl.fib_public(tr), tr,
+           sep=b"zig-stark:stark:fib")
+
+
+def test_fib_wrong_claim_still_proves(orc):
+    # the prover does not check the statement; the verifier rejects (stark.zig:1282-1299)
+    tr = wl.fib_trace(16)
+    bad = wire.qm31(((int(tr[0][-1][0]) + 1) % wl.P, 0, 0, 0))
+    _check(orc, wl.AIR_FIB, wire.StarkParams(4, 3, 12, 3), bad, tr, sep=b"zig-stark:stark:fib", valid=False)
+
+
+def test_seeded_fib_config(orc):
+    """The 2^12-row Fibonacci workload: a_0 = 1, seeded a_1, blowup 4, 16 queries."""
+    tr, pi = wl.seeded_fib(12)
+    _check(orc, wl.AIR_SEEDED_FIB, wire.StarkParams(12, 2, 16, 3), pi, tr, sep=b"zig-stark:fibonacci:example")
+
+
+@pytest.mark.parametrize("air,gen", [(wl.AIR_RANGE_CHECK, wl.range_check_trace), (wl.AIR_AND_TABLE, wl.and_table_trace),
+                                     (wl.AIR_MULTIPLICITY, wl.multiplicity_trace)])
+@pytest.mark.parametrize("trace_log,log_blowup", [(4, 3), (6, 2), (11, 2)])
+def test_lookup_airs(orc, air, gen, trace_log, log_blowup):
+    tr, table = gen(1 << trace_log)
+    valid = air != wl.AIR_MULTIPLICITY or trace_log == 4
+    _check(orc, air, wire.StarkParams(trace_log, log_blowup, 16, 3), b"", tr, table, sep=b"zig-stark:stark:lookup",
+           valid=valid)
+
+
+def test_rescue_example(orc):
+    tr, pi = wl.rescue_example()
+    _check(orc, wl.AIR_RESCUE_EXAMPLE, wire.StarkParams(3, 3, 16, 3), pi, tr, sep=b"zig-stark:rescue:example")
+
+
+def test_linear_example(orc):
+    tr, pi = wl.linear_example()
+    _check(orc, wl.AIR_LINEAR_EXAMPLE, wire.StarkParams(3, 3, 16, 3), pi, tr, sep=b"zig-stark:ml_linear:example")
+
+
+def test_random_qm31_trace(orc):
+    # non-embedded QM31 trace values (the prover does not assume M31 inputs)
+    rng = np.random.default_rng(9)
+    tr = [rng.integers(0, wl.P, (64, 4), dtype=np.uint32) for _ in range(2)]
+    _check(orc, wl.AIR_FIB, wire.StarkParams(6, 2, 16, 3), wire.qm31((5, 6, 7, 8)), tr, valid=False)
+
+
+def test_malformed_inputs(orc):
+    from zs_b200 import native
+    tr = wl.fib_trace(16)
+    params = wire.StarkParams(4, 3, 12, 3)
+    with pytest.raises(native.ZsError) as e:
+        native.prove(wl.AIR_FIB, params, b"\x00" * 15, tr)
+    assert e.value.code == -2
+    with pytest.raises(native.ZsError) as e:
+        native.prove(wl.AIR_FIB, params, wl.fib_public(tr), tr[:1])
+    assert e.value.code == -2
+    with pytest.raises(native.ZsError) as e:
+        native.prove(wl.AIR_FIB, wire.StarkParams(4, 3, 12, 7), wl.fib_public(tr), tr)
+    assert e.value.code == -4
+    with pytest.raises(native.ZsError) as e:
+        native.prove(99, params, b"", tr)
+    assert e.value.code == -1

@@ -6,6 +6,7 @@
 #include "../../include/zs_m31.h"
 #include "circle.cuh"
 #include "commit.cuh"
+#include "stark.cuh"
 
 using namespace zs;
 
@@ -175,6 +176,36 @@ int32_t zs_m31_circle_commit(const uint32_t* trace, uint32_t n_columns, uint32_t
   if (rc == 0) rc = zs_m31_commit_plan_results(plan, nullptr, lde_root, layer_roots, final_layer);
   zs_m31_commit_plan_destroy(plan);
   return rc;
+}
+
+int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t* params, size_t params_len,
+                     const uint8_t* public_inputs, size_t public_inputs_len, const uint8_t* preprocessed,
+                     size_t preprocessed_len, const uint8_t* trace, size_t trace_len, const uint8_t* channel_sep,
+                     size_t channel_sep_len, uint8_t** out_proof, size_t* out_len) {
+  return guarded([&] {
+    if (!out_proof || !out_len || !host.alloc) throw Error(ZS_EMALFORMED, "null output or allocator");
+    if ((!params && params_len) || (!public_inputs && public_inputs_len) || (!preprocessed && preprocessed_len) ||
+        (!trace && trace_len) || (!channel_sep && channel_sep_len))
+      throw Error(ZS_EMALFORMED, "null input buffer with a non-zero length");
+    ensure_device();
+    cudaStream_t st = nullptr;
+    ZS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    std::vector<uint8_t> bytes;
+    try {
+      bytes = stark_prove(air_id, params, params_len, public_inputs, public_inputs_len, preprocessed,
+                          preprocessed_len, trace, trace_len, channel_sep, channel_sep_len, st);
+    } catch (...) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+      throw;
+    }
+    cudaStreamDestroy(st);
+    uint8_t* buf = (uint8_t*)host.alloc(host.ctx, bytes.size() ? bytes.size() : 1);
+    if (!buf) throw Error(ZS_ENOMEM, "host allocator returned null");
+    std::memcpy(buf, bytes.data(), bytes.size());
+    *out_proof = buf;
+    *out_len = bytes.size();
+  });
 }
 
 void zs_free(zs_host_allocator host, uint8_t* ptr, size_t len) {

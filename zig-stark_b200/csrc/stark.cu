@@ -1,0 +1,643 @@
+// GenericStark(Air).proveWithPreprocessed (src/m31/stark.zig:327-658) on the device.
+//
+// The transcript (Channel) stays on the host and sees exactly the bytes the
+// reference absorbs, in the same order; everything proportional to the trace or the
+// domain runs on the GPU:
+//   LDE of every column (QM31 NTT: interpolation on H, evaluation on D),
+//   one Merkle tree per committed column (hashQM31 leaves),
+//   the LogUp accumulator (row contributions + a parallel prefix sum),
+//   the quotient Hc(x)/Z_H(x) on D,
+//   the DEEP evaluations f_j(z), f_j(w z) (parallel Horner sums),
+//   the DEEP codeword, the FRI layers (fold fused with the next layer's commitment),
+//   and the gather of every revealed value and Merkle path.
+// All device arithmetic is exact, so every root, layer and proof byte equals the
+// reference's.
+#include <memory>
+#include <vector>
+
+#include "airs.cuh"
+#include "fri.cuh"
+#include "host.cuh"
+#include "merkle.cuh"
+#include "ntt.cuh"
+#include "stark.cuh"
+
+namespace zs {
+
+namespace {
+
+constexpr unsigned kT = 256;
+
+__device__ __forceinline__ qm31 ldq(const qm31* p) {
+  const uint4 r = *reinterpret_cast<const uint4*>(p);
+  return qmake(r.x, r.y, r.z, r.w);
+}
+__device__ __forceinline__ void stq(qm31* p, const qm31& v) {
+  *reinterpret_cast<uint4*>(p) = make_uint4(v.a.a, v.a.b, v.b.a, v.b.b);
+}
+
+// Everything the quotient and DEEP kernels need beyond the codewords.
+struct QuotConsts {
+  AirConsts air;
+  uint32_t m, m_total, n_pre, num_trans, n_rel, total_bound, shift;
+  unsigned log_N, log_blowup;
+  qm31 last_point;  // w^(n-1)
+  qm31 offset;      // FRI_OFFSET
+  qm31 alphas[kMaxTrans + 2 * kMaxRel];
+  qm31 betas[kMaxBound];
+  uint32_t b_col[kMaxBound];
+  qm31 b_val[kMaxBound];
+  qm31 b_pt[kMaxBound];  // p_k = w^step_k
+  qm31 zh[8], zh_inv[8];  // Z_H(d_i) depends on i mod 2^log_blowup
+  qm31 ac[kMaxKey], ar[kMaxRel];
+  uint32_t sel[kMaxRel], mult[kMaxRel], n_keys[kMaxRel], keys[kMaxRel][kMaxKey], tabs[kMaxRel][kMaxKey];
+};
+
+__device__ __forceinline__ qm31 domain_point(const QuotConsts& k, const qm31* __restrict__ wpow, uint32_t i) {
+  // d_i = FRI_OFFSET * w_N^i, w_N^(N/2) = -1, wpow[k] = w_N^k for k < N/2
+  const uint32_t half = 1u << (k.log_N - 1);
+  qm31 w = i < half ? ldq(wpow + i) : qneg(ldq(wpow + (i - half)));
+  return qmul(k.offset, w);
+}
+
+__device__ __host__ __forceinline__ qm31 combined_key(const qm31* ac, uint32_t nk, const uint32_t* cols,
+                                                      const qm31* row) {
+  qm31 key = qzero();
+  for (uint32_t j = 0; j < nk; ++j) key = qadd(key, qmul(ac[j], row[cols[j]]));
+  return key;
+}
+
+// stark.zig:259-276 (denominator-cleared LogUp constraint).
+__device__ __host__ __forceinline__ qm31 lookup_constraint(const QuotConsts& k, uint32_t r, const qm31* cur,
+                                                           const qm31* pre, const qm31& acc, const qm31& accn) {
+  const qm31 sel = cur[k.sel[r]], mult = cur[k.mult[r]];
+  const qm31 key = combined_key(k.ac, k.n_keys[r], k.keys[r], cur);
+  const qm31 tkey = combined_key(k.ac, k.n_keys[r], k.tabs[r], pre);
+  const qm31 dacc = qsub(accn, acc);
+  const qm31 lb = qsub(qmul(dacc, qsub(k.ar[r], key)), mult);
+  const qm31 tb = qadd(qmul(dacc, qsub(k.ar[r], tkey)), qone());
+  return qadd(qmul(sel, lb), qmul(qsub(qone(), sel), tb));
+}
+
+// Hc(x) (stark.zig:505-533): transitions x (x - w^(n-1)), cyclic LogUp and
+// selector-binarity constraints, boundary terms with Z_H(x) / (x - p_k).
+__device__ __host__ inline qm31 composition(const QuotConsts& k, const qm31& x, const qm31* cur, const qm31* next,
+                                            const qm31* pre, const qm31& zh) {
+  qm31 res[kMaxTrans];
+  air_eval(k.air, x, cur, next, res);
+  qm31 h = qzero();
+  const qm31 xl = qsub(x, k.last_point);
+  for (uint32_t t = 0; t < k.num_trans; ++t) h = qadd(h, qmul(k.alphas[t], qmul(res[t], xl)));
+  for (uint32_t r = 0; r < k.n_rel; ++r)
+    h = qadd(h, qmul(k.alphas[k.num_trans + r], lookup_constraint(k, r, cur, pre, cur[k.m + r], next[k.m + r])));
+  for (uint32_t r = 0; r < k.n_rel; ++r) {
+    const qm31 sel = cur[k.sel[r]];
+    h = qadd(h, qmul(k.alphas[k.num_trans + k.n_rel + r], qmul(sel, qsub(qone(), sel))));
+  }
+  for (uint32_t b = 0; b < k.total_bound; ++b) {
+    const qm31 term = qmul(qmul(qsub(cur[k.b_col[b]], k.b_val[b]), zh), qinv(qsub(x, k.b_pt[b])));
+    h = qadd(h, qmul(k.betas[b], term));
+  }
+  return h;
+}
+
+// cw: codewords of all columns ([pre | main | acc]), N each.
+__global__ void __launch_bounds__(kT) k_quotient(const qm31* __restrict__ cw, qm31* __restrict__ q,
+                                                 const qm31* __restrict__ wpow, const QuotConsts* __restrict__ kp) {
+  const QuotConsts& k = *kp;
+  const uint32_t N = 1u << k.log_N;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t in = (i + k.shift) & (N - 1);
+  qm31 cur[kMaxCols], next[kMaxCols], pre[kMaxPre];
+  for (uint32_t j = 0; j < k.n_pre; ++j) pre[j] = ldq(cw + (size_t)j * N + i);
+  for (uint32_t j = 0; j < k.m_total; ++j) {
+    const qm31* c = cw + (size_t)(k.n_pre + j) * N;
+    cur[j] = ldq(c + i);
+    next[j] = ldq(c + in);
+  }
+  const qm31 x = domain_point(k, wpow, i);
+  const uint32_t zi = i & ((1u << k.log_blowup) - 1);
+  const qm31 h = composition(k, x, cur, next, pre, k.zh[zi]);
+  stq(q + i, qmul(h, k.zh_inv[zi]));
+}
+
+// LogUp row contributions (stark.zig:283-297) on H: out[i] = contribution of row i.
+__global__ void k_logup_rows(const qm31* __restrict__ vals, uint32_t n, const QuotConsts* __restrict__ kp,
+                             uint32_t r, qm31* __restrict__ out) {
+  const QuotConsts& k = *kp;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  qm31 row[kMaxCols], pre[kMaxPre];
+  for (uint32_t j = 0; j < k.n_pre; ++j) pre[j] = ldq(vals + (size_t)j * n + i);
+  for (uint32_t j = 0; j < k.m; ++j) row[j] = ldq(vals + (size_t)(k.n_pre + j) * n + i);
+  const qm31 sel = row[k.sel[r]], mult = row[k.mult[r]];
+  const qm31 key = combined_key(k.ac, k.n_keys[r], k.keys[r], row);
+  const qm31 tkey = combined_key(k.ac, k.n_keys[r], k.tabs[r], pre);
+  const qm31 lt = qmul(sel, qmul(mult, qinv(qsub(k.ar[r], key))));
+  const qm31 tt = qmul(qsub(qone(), sel), qinv(qsub(k.ar[r], tkey)));
+  stq(out + i, qsub(lt, tt));
+}
+
+// Exclusive prefix sum of QM31 values in blocks of 1024 (exact, so any association
+// order gives the reference's acc[i] = sum_{k<i} c_k).
+__global__ void __launch_bounds__(1024) k_scan_block(const qm31* in, qm31* out, uint32_t n, qm31* block_sums) {
+  __shared__ qm31 s[1024];
+  const uint32_t i = blockIdx.x * 1024 + threadIdx.x;
+  s[threadIdx.x] = i < n ? ldq(in + i) : qzero();
+  __syncthreads();
+  for (uint32_t d = 1; d < 1024; d <<= 1) {
+    qm31 v = threadIdx.x >= d ? s[threadIdx.x - d] : qzero();
+    __syncthreads();
+    s[threadIdx.x] = qadd(s[threadIdx.x], v);
+    __syncthreads();
+  }
+  // inclusive in s; exclusive output
+  if (i < n) stq(out + i, threadIdx.x == 0 ? qzero() : s[threadIdx.x - 1]);
+  if (threadIdx.x == 1023 && block_sums) stq(block_sums + blockIdx.x, s[1023]);
+}
+
+__global__ void k_scan_add(qm31* out, uint32_t n, const qm31* block_prefix) {
+  const uint32_t i = blockIdx.x * 1024 + threadIdx.x;
+  if (i < n && blockIdx.x > 0) stq(out + i, qadd(ldq(out + i), ldq(block_prefix + blockIdx.x)));
+}
+
+// partial[pt][col][blk] = sum over the block's k of coeffs[col][k] * zpow[pt][k].
+__global__ void __launch_bounds__(kT) k_eval_partial(const qm31* __restrict__ coeffs, uint32_t n,
+                                                     const qm31* __restrict__ zpow, uint32_t npt, qm31* partial) {
+  __shared__ qm31 s[kT];
+  const uint32_t col = blockIdx.y, pt = blockIdx.z;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  qm31 v = qzero();
+  if (k < n) v = qmul(ldq(coeffs + (size_t)col * n + k), ldq(zpow + (size_t)pt * n + k));
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (uint32_t d = blockDim.x / 2; d > 0; d >>= 1) {
+    if (threadIdx.x < d) s[threadIdx.x] = qadd(s[threadIdx.x], s[threadIdx.x + d]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) stq(partial + ((size_t)pt * gridDim.y + col) * gridDim.x + blockIdx.x, s[0]);
+}
+
+// Sums `nblk` partials per (pt, col) sequentially (nblk is small).
+__global__ void k_eval_sum(const qm31* partial, uint32_t nblk, uint32_t count, qm31* out) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= count) return;
+  qm31 acc = qzero();
+  for (uint32_t b = 0; b < nblk; ++b) acc = qadd(acc, ldq(partial + (size_t)idx * nblk + b));
+  stq(out + idx, acc);
+}
+
+// DEEP codeword (stark.zig:577-588), with 1/(d_i - z) factored out of the sum.
+struct DeepConsts {
+  uint32_t m_total, n_pre, shift;
+  unsigned log_N;
+  qm31 offset, z, qz;
+  qm31 gammas[2 * kMaxCols + 1];
+  qm31 evals[2 * kMaxCols];
+};
+
+__global__ void __launch_bounds__(kT) k_deep(const qm31* __restrict__ cw, const qm31* __restrict__ q,
+                                             const qm31* __restrict__ wpow, const DeepConsts* __restrict__ kp,
+                                             qm31* __restrict__ g) {
+  const DeepConsts& k = *kp;
+  const uint32_t N = 1u << k.log_N;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t in = (i + k.shift) & (N - 1);
+  const uint32_t half = N >> 1;
+  const qm31 w = i < half ? ldq(wpow + i) : qneg(ldq(wpow + (i - half)));
+  const qm31 x = qmul(k.offset, w);
+  const qm31 inv_dz = qinv(qsub(x, k.z));
+  qm31 acc = qzero();
+  for (uint32_t j = 0; j < k.m_total; ++j) {
+    const qm31* c = cw + (size_t)(k.n_pre + j) * N;
+    acc = qadd(acc, qmul(k.gammas[j], qsub(ldq(c + i), k.evals[j])));
+    acc = qadd(acc, qmul(k.gammas[k.m_total + j], qsub(ldq(c + in), k.evals[k.m_total + j])));
+  }
+  acc = qadd(acc, qmul(k.gammas[2 * k.m_total], qsub(ldq(q + i), k.qz)));
+  stq(g + i, qmul(acc, inv_dz));
+}
+
+// Gather: out[r] = words [idx * w, (idx + 1) * w) of src[r] (requests prepared on the host).
+struct GatherReq {
+  const uint32_t* src;
+  uint64_t index;
+  uint32_t words;
+  uint32_t out_off;
+};
+__global__ void k_gather(const GatherReq* __restrict__ reqs, uint32_t count, uint32_t* __restrict__ out) {
+  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= count) return;
+  const GatherReq q = reqs[r];
+  for (uint32_t w = 0; w < q.words; ++w) out[q.out_off + w] = q.src[q.index * q.words + w];
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(size_t count, cudaStream_t s) : n(count), st(s) {
+    ZS_CUDA(cudaMallocAsync((void**)&p, (count ? count : 1) * sizeof(T), s));
+  }
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+
+Digest root_of(const DeviceTree& t, cudaStream_t st) {
+  Digest d;
+  ZS_CUDA(cudaMemcpyAsync(d.data(), t.root(), 32, cudaMemcpyDeviceToHost, st));
+  ZS_CUDA(cudaStreamSynchronize(st));
+  return d;
+}
+
+struct OwnedTree {
+  DeviceTree t;
+  cudaStream_t st;
+  OwnedTree(unsigned log_n, cudaStream_t s) : st(s) {
+    t.log_n = log_n;
+    ZS_CUDA(cudaMallocAsync((void**)&t.words, DeviceTree::words_for(log_n) * sizeof(uint32_t), s));
+  }
+  ~OwnedTree() { cudaFreeAsync(t.words, st); }
+};
+
+std::vector<std::vector<qm31>> read_columns(const uint8_t* d, size_t n) {
+  std::vector<std::vector<qm31>> cols;
+  if (n == 0) return cols;
+  WireReader r(d, n);
+  const uint64_t m = r.len(8);
+  for (uint64_t j = 0; j < m; ++j) {
+    const uint64_t len = r.len(16);
+    std::vector<qm31> c(len);
+    for (auto& v : c) v = r.q();
+    cols.push_back(std::move(c));
+  }
+  r.end();
+  return cols;
+}
+
+}  // namespace
+
+std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_t params_len, const uint8_t* pi,
+                                 size_t pi_len, const uint8_t* pre_b, size_t pre_len, const uint8_t* trace_b,
+                                 size_t trace_len, const uint8_t* sep, size_t sep_len, cudaStream_t st) {
+  // ---- inputs -------------------------------------------------------------
+  StarkParamsH sp;
+  {
+    WireReader r(params_b, params_len);
+    sp.trace_log = r.u8();
+    sp.log_blowup = r.u8();
+    sp.num_queries = r.u64();
+    sp.remainder_log = r.u8();
+    r.end();
+  }
+  const AirInfo air = make_air(air_id, pi, pi_len);
+  const auto pre = read_columns(pre_b, pre_len);
+  const auto trace = read_columns(trace_b, trace_len);
+  const unsigned tl = sp.trace_log, lb = sp.log_blowup, lN = tl + lb;
+  if (lN > 26 || lb > 3) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 26 or log_blowup above 3");
+  const uint32_t n = 1u << tl, N = 1u << lN, shift = 1u << lb;
+  if (air.fixed_n && n != air.fixed_n) throw Error(ZS_EMALFORMED, "the AIR is defined for a fixed trace length");
+  if (trace.size() != air.m || pre.size() != air.n_pre) throw Error(ZS_EMALFORMED, "column count mismatch");
+  for (auto& c : trace)
+    if (c.size() != n) throw Error(ZS_EMALFORMED, "column length mismatch");
+  for (auto& c : pre)
+    if (c.size() != n) throw Error(ZS_EMALFORMED, "column length mismatch");
+  const uint32_t m = air.m, n_pre = air.n_pre, n_rel = air.n_rel, m_total = m + n_rel;
+  const uint32_t n_trans_total = air.num_trans + 2 * n_rel, total_bound = air.num_bound + n_rel;
+  const uint32_t n_deep = 2 * m_total + 1, reveal_len = 2 * m_total + 1 + n_pre;
+  if (m_total > kMaxCols || air.num_trans > kMaxTrans || total_bound > kMaxBound || n_pre > kMaxPre)
+    throw Error(ZS_EGENERIC, "AIR exceeds the compiled-in limits");
+  // FRI parameters (stark.zig:197-239)
+  FriParamsH fp;
+  {
+    const uint64_t dc = air.max_constraint_degree(n);
+    const uint64_t sat = dc > n ? dc - n : 0;
+    const uint64_t degree_g = (n - 1) > sat ? (n - 1) : sat;
+    unsigned log = 0;
+    uint64_t bound = 1;
+    while (bound <= degree_g) ++log, bound <<= 1;
+    if (log > lN || sp.remainder_log >= lN || sp.remainder_log < lN - log)
+      throw Error(ZS_EPROTOCOL, "parameters violate the FRI sizing assertions");
+    fp.log_size = (uint8_t)log;
+    fp.log_blowup = (uint8_t)(lN - log);
+    fp.num_queries = sp.num_queries;
+    fp.remainder_log = sp.remainder_log;
+    if (fp.remainder_log < fp.log_blowup) throw Error(ZS_EPROTOCOL, "remainder_log below the FRI blowup");
+  }
+  const unsigned L = fp.folds();
+  const qm31 w = q_root_of_unity(tl), offset = q_fri_offset();
+
+  // ---- LDE of preprocessed and main columns ------------------------------------
+  const uint32_t ncol = n_pre + m_total;  // [pre | main | acc]
+  NttTables small(tl, st), big(lN, st);
+  DevBuf<qm31> offset_pows(n, st);
+  qm31_powers(offset, offset_pows.p, n, st);
+  DevBuf<qm31> vals((size_t)ncol * n, st), coeffs((size_t)ncol * n, st), cw((size_t)ncol * N, st);
+  {
+    std::vector<qm31> host((size_t)(n_pre + m) * n);
+    for (uint32_t j = 0; j < n_pre; ++j) std::copy(pre[j].begin(), pre[j].end(), host.begin() + (size_t)j * n);
+    for (uint32_t j = 0; j < m; ++j) std::copy(trace[j].begin(), trace[j].end(), host.begin() + (size_t)(n_pre + j) * n);
+    ZS_CUDA(cudaMemcpyAsync(vals.p, host.data(), host.size() * sizeof(qm31), cudaMemcpyHostToDevice, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+  }
+  lde_qm31(vals.p, n, coeffs.p, n, cw.p, N, n_pre + m, small, big, offset_pows.p, st);
+
+  std::vector<std::unique_ptr<OwnedTree>> trees;
+  for (uint32_t j = 0; j < ncol; ++j) trees.push_back(std::make_unique<OwnedTree>(lN, st));
+  for (uint32_t j = 0; j < n_pre + m; ++j) build_qm31_tree(cw.p + (size_t)j * N, trees[j]->t, st);
+
+  Channel ch(sep, sep_len);
+  WireWriter proof;
+  proof.u8(sp.trace_log);
+  proof.u8(sp.log_blowup);
+  proof.u64(sp.num_queries);
+  proof.u8(sp.remainder_log);
+  std::vector<Digest> pre_roots, trace_roots, acc_roots;
+  for (uint32_t j = 0; j < n_pre; ++j) {
+    pre_roots.push_back(root_of(trees[j]->t, st));
+    ch.absorb(pre_roots.back());
+  }
+  for (uint32_t j = 0; j < m; ++j) {
+    trace_roots.push_back(root_of(trees[n_pre + j]->t, st));
+    ch.absorb(trace_roots.back());
+  }
+
+  // ---- LogUp challenges and accumulators ---------------------------------------
+  QuotConsts kc{};
+  kc.air = air.consts;
+  kc.m = m, kc.m_total = m_total, kc.n_pre = n_pre, kc.num_trans = air.num_trans, kc.n_rel = n_rel;
+  kc.total_bound = total_bound, kc.shift = shift, kc.log_N = lN, kc.log_blowup = lb;
+  kc.offset = offset;
+  kc.last_point = qpow(w, n - 1);
+  for (uint32_t j = 0; j < air.n_lc; ++j) kc.ac[j] = ch.sample_q();
+  for (uint32_t r = 0; r < n_rel; ++r) kc.ar[r] = ch.sample_q();
+  for (uint32_t r = 0; r < n_rel; ++r) {
+    kc.sel[r] = air.sel[r], kc.mult[r] = air.mult[r], kc.n_keys[r] = air.n_keys[r];
+    for (uint32_t j = 0; j < air.n_keys[r]; ++j) kc.keys[r][j] = air.keys[r][j], kc.tabs[r][j] = air.tabs[r][j];
+  }
+  DevBuf<QuotConsts> d_kc(1, st);
+  ZS_CUDA(cudaMemcpyAsync(d_kc.p, &kc, sizeof(kc), cudaMemcpyHostToDevice, st));
+  if (n_rel > 0) {
+    DevBuf<qm31> contrib(n, st);
+    const uint32_t nb = (n + 1023) / 1024;
+    DevBuf<qm31> sums(nb, st), sums_scan(nb, st);
+    for (uint32_t r = 0; r < n_rel; ++r) {
+      qm31* acc_vals = vals.p + (size_t)(n_pre + m + r) * n;
+      k_logup_rows<<<(n + kT - 1) / kT, kT, 0, st>>>(vals.p, n, d_kc.p, r, contrib.p);
+      // acc[i] = sum_{k < i} contrib[k] (stark.zig:438-446)
+      k_scan_block<<<nb, 1024, 0, st>>>(contrib.p, acc_vals, n, sums.p);
+      if (nb > 1) {
+        if (nb > 1024) throw Error(ZS_EGENERIC, "trace too long for the accumulator scan");
+        k_scan_block<<<1, 1024, 0, st>>>(sums.p, sums_scan.p, nb, nullptr);
+        k_scan_add<<<nb, 1024, 0, st>>>(acc_vals, n, sums_scan.p);
+      }
+    }
+    ZS_CUDA(cudaGetLastError());
+    lde_qm31(vals.p + (size_t)(n_pre + m) * n, n, coeffs.p + (size_t)(n_pre + m) * n, n,
+             cw.p + (size_t)(n_pre + m) * N, N, n_rel, small, big, offset_pows.p, st);
+    for (uint32_t r = 0; r < n_rel; ++r) {
+      build_qm31_tree(cw.p + (size_t)(n_pre + m + r) * N, trees[n_pre + m + r]->t, st);
+      acc_roots.push_back(root_of(trees[n_pre + m + r]->t, st));
+      ch.absorb(acc_roots.back());
+    }
+  }
+  proof.digests(trace_roots);
+  if (n_pre > 0) {
+    proof.u8(1);
+    proof.digests(pre_roots);
+  } else {
+    proof.u8(0);
+  }
+  if (n_rel > 0) {
+    proof.u8(1);
+    proof.digests(acc_roots);
+  } else {
+    proof.u8(0);
+  }
+
+  // ---- constraint weights and the quotient -------------------------------------
+  for (uint32_t t = 0; t < n_trans_total; ++t) kc.alphas[t] = ch.sample_q();
+  std::vector<Boundary> bnd;
+  air.boundary(n, bnd);
+  for (uint32_t r = 0; r < n_rel; ++r) bnd.push_back({m + r, 0, qzero()});
+  for (uint32_t b = 0; b < total_bound; ++b) {
+    kc.betas[b] = ch.sample_q();
+    kc.b_col[b] = bnd[b].column;
+    kc.b_val[b] = bnd[b].value;
+    kc.b_pt[b] = qpow(w, bnd[b].step);
+  }
+  {
+    // Z_H(d_i) = offset^n * (w_N^n)^(i mod 2^lb) - 1
+    const qm31 on = qpow(offset, n), wb = q_root_of_unity(lb);
+    qm31 acc = on;
+    for (uint32_t t = 0; t < shift; ++t) {
+      kc.zh[t] = qsub(acc, qone());
+      kc.zh_inv[t] = qinv(kc.zh[t]);
+      acc = qmul(acc, wb);
+    }
+  }
+  ZS_CUDA(cudaMemcpyAsync(d_kc.p, &kc, sizeof(kc), cudaMemcpyHostToDevice, st));
+  DevBuf<qm31> q(N, st);
+  k_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_kc.p);
+  ZS_CUDA(cudaGetLastError());
+  OwnedTree qtree(lN, st);
+  build_qm31_tree(q.p, qtree.t, st);
+  const Digest qroot = root_of(qtree.t, st);
+  ch.absorb(qroot);
+  proof.digest(qroot);
+
+  // ---- DEEP evaluations (stark.zig:547-570) ------------------------------------
+  const qm31 z = ch.sample_q();
+  const qm31 wz = qmul(z, w);
+  std::vector<qm31> deep(n_deep);
+  std::vector<qm31> pre_z(n_pre);
+  {
+    DevBuf<qm31> zpow((size_t)2 * n, st);
+    qm31_powers(z, zpow.p, n, st);
+    qm31_powers(wz, zpow.p + n, n, st);
+    const uint32_t nblk = (n + kT - 1) / kT;
+    DevBuf<qm31> partial((size_t)2 * ncol * nblk, st), sums((size_t)2 * ncol, st);
+    k_eval_partial<<<dim3(nblk, ncol, 2), kT, 0, st>>>(coeffs.p, n, zpow.p, 2, partial.p);
+    k_eval_sum<<<(2 * ncol + 63) / 64, 64, 0, st>>>(partial.p, nblk, 2 * ncol, sums.p);
+    ZS_CUDA(cudaGetLastError());
+    std::vector<qm31> hs(2 * ncol);
+    ZS_CUDA(cudaMemcpyAsync(hs.data(), sums.p, hs.size() * sizeof(qm31), cudaMemcpyDeviceToHost, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t j = 0; j < m_total; ++j) {
+      deep[j] = hs[n_pre + j];                  // f_j(z)
+      deep[m_total + j] = hs[ncol + n_pre + j];  // f_j(w z)
+    }
+    for (uint32_t j = 0; j < n_pre; ++j) pre_z[j] = hs[j];
+    // computeQuotientAt (stark.zig:794-849)
+    const qm31 zh = qsub(qpow(z, n), qone());
+    const qm31 h = composition(kc, z, deep.data(), deep.data() + m_total, pre_z.data(), zh);
+    deep[2 * m_total] = qmul(h, qinv(zh));
+  }
+  for (auto& v : deep) ch.absorb(v);
+  proof.qs(deep);
+
+  // ---- DEEP codeword and FRI ---------------------------------------------------
+  DeepConsts dc{};
+  dc.m_total = m_total, dc.n_pre = n_pre, dc.shift = shift, dc.log_N = lN;
+  dc.offset = offset, dc.z = z, dc.qz = deep[2 * m_total];
+  for (uint32_t j = 0; j < n_deep; ++j) dc.gammas[j] = ch.sample_q();
+  for (uint32_t j = 0; j < 2 * m_total; ++j) dc.evals[j] = deep[j];
+  DevBuf<DeepConsts> d_dc(1, st);
+  ZS_CUDA(cudaMemcpyAsync(d_dc.p, &dc, sizeof(dc), cudaMemcpyHostToDevice, st));
+  std::vector<std::unique_ptr<DevBuf<qm31>>> layers;
+  layers.push_back(std::make_unique<DevBuf<qm31>>(N, st));
+  k_deep<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_dc.p, layers[0]->p);
+  ZS_CUDA(cudaGetLastError());
+
+  FoldTables ftabs(lN, st);
+  std::vector<std::unique_ptr<OwnedTree>> ftrees;
+  for (unsigned i = 0; i < L; ++i) ftrees.push_back(std::make_unique<OwnedTree>(lN - i, st));
+  if (L > 0) build_qm31_tree(layers[0]->p, ftrees[0]->t, st);
+  std::vector<Digest> froots;
+  for (unsigned i = 0; i < L; ++i) {
+    froots.push_back(root_of(ftrees[i]->t, st));
+    ch.absorb(froots.back());
+    const qm31 alpha = ch.sample_q();
+    const uint32_t half = N >> (i + 1);
+    layers.push_back(std::make_unique<DevBuf<qm31>>(half, st));
+    fri_fold(layers[i]->p, layers[i + 1]->p, half, alpha, i, ftabs, i + 1 < L ? &ftrees[i + 1]->t : nullptr, st);
+  }
+  // remainder (fri.zig:228-233): interpolate the first 2^(remainder_log - log_blowup)
+  // points of layer L on the host (at most a few dozen values).
+  const uint32_t rem = 1u << (fp.remainder_log - fp.log_blowup);
+  std::vector<qm31> last(rem);
+  ZS_CUDA(cudaMemcpyAsync(last.data(), layers[L]->p, rem * sizeof(qm31), cudaMemcpyDeviceToHost, st));
+  ZS_CUDA(cudaStreamSynchronize(st));
+  std::vector<qm31> xs(rem);
+  {
+    const qm31 wl = q_root_of_unity(lN - L);
+    qm31 acc = qpow(offset, (uint64_t)1 << L);
+    for (uint32_t j = 0; j < rem; ++j) {
+      xs[j] = acc;
+      acc = qmul(acc, wl);
+    }
+  }
+  const std::vector<qm31> remainder = interpolate_small(xs, last);
+  for (auto& v : remainder) ch.absorb(v);
+
+  // ---- queries (fri.zig:236-256, stark.zig:595-625) -----------------------------
+  std::vector<uint64_t> p0s(sp.num_queries);
+  for (auto& p : p0s) p = ch.sample_index(N);
+  std::vector<GatherReq> reqs;
+  uint32_t off = 0;
+  auto want_value = [&](const qm31* base, uint64_t idx) {
+    reqs.push_back({reinterpret_cast<const uint32_t*>(base), idx, 4, off});
+    off += 4;
+  };
+  auto want_path = [&](const DeviceTree& t, uint64_t idx) {
+    for (unsigned lvl = 0; lvl < t.log_n; ++lvl) {
+      reqs.push_back({t.level(lvl), (idx >> lvl) ^ 1, 8, off});
+      off += 8;
+    }
+  };
+  // FRI pairs
+  for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
+    uint64_t p = p0s[qi];
+    for (unsigned i = 0; i < L; ++i) {
+      const uint64_t nn = (uint64_t)N >> (i + 1), pn = p % nn;
+      want_value(layers[i]->p, pn);
+      want_value(layers[i]->p, pn + nn);
+      want_path(ftrees[i]->t, pn);
+      want_path(ftrees[i]->t, pn + nn);
+      p = pn;
+    }
+  }
+  // STARK reveals
+  for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
+    const uint64_t p0 = p0s[qi], pn = (p0 + shift) % N;
+    for (uint32_t j = 0; j < m_total; ++j) {
+      const qm31* c = cw.p + (size_t)(n_pre + j) * N;
+      want_value(c, p0);
+      want_path(trees[n_pre + j]->t, p0);
+      want_value(c, pn);
+      want_path(trees[n_pre + j]->t, pn);
+    }
+    want_value(q.p, p0);
+    want_path(qtree.t, p0);
+    for (uint32_t j = 0; j < n_pre; ++j) {
+      want_value(cw.p + (size_t)j * N, p0);
+      want_path(trees[j]->t, p0);
+    }
+  }
+  std::vector<uint32_t> gathered(off);
+  if (!reqs.empty()) {
+    DevBuf<GatherReq> d_reqs(reqs.size(), st);
+    DevBuf<uint32_t> d_out(off, st);
+    ZS_CUDA(cudaMemcpyAsync(d_reqs.p, reqs.data(), reqs.size() * sizeof(GatherReq), cudaMemcpyHostToDevice, st));
+    k_gather<<<((uint32_t)reqs.size() + kT - 1) / kT, kT, 0, st>>>(d_reqs.p, (uint32_t)reqs.size(), d_out.p);
+    ZS_CUDA(cudaGetLastError());
+    ZS_CUDA(cudaMemcpyAsync(gathered.data(), d_out.p, off * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+  }
+  size_t cursor = 0;
+  auto next_value = [&]() {
+    const uint32_t* w4 = gathered.data() + cursor;
+    cursor += 4;
+    return qmake(w4[0], w4[1], w4[2], w4[3]);
+  };
+  auto next_path = [&](unsigned log_n) {
+    std::vector<Digest> path(log_n);
+    for (auto& d : path) {
+      std::memcpy(d.data(), gathered.data() + cursor, 32);
+      cursor += 8;
+    }
+    return path;
+  };
+
+  // ---- serialization (stark.zig:107-122, fri.zig:72-79) --------------------------
+  proof.u8(fp.log_size);  // Fri.Proof.params
+  proof.u8(fp.log_blowup);
+  proof.u64(fp.num_queries);
+  proof.u8(fp.remainder_log);
+  proof.digests(froots);
+  proof.qs(remainder);
+  proof.u64(sp.num_queries);
+  for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
+    proof.u64(p0s[qi]);
+    proof.u64(L);
+    for (unsigned i = 0; i < L; ++i) {
+      const qm31 v0 = next_value(), v1 = next_value();
+      const auto path0 = next_path(lN - i), path1 = next_path(lN - i);
+      proof.q(v0);
+      proof.q(v1);
+      proof.digests(path0);
+      proof.digests(path1);
+    }
+  }
+  proof.u64(sp.num_queries);
+  for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
+    std::vector<qm31> values(reveal_len);
+    std::vector<std::vector<Digest>> paths(reveal_len);
+    for (uint32_t j = 0; j < m_total; ++j) {
+      values[j] = next_value();
+      paths[j] = next_path(lN);
+      values[m_total + j] = next_value();
+      paths[m_total + j] = next_path(lN);
+    }
+    values[2 * m_total] = next_value();
+    paths[2 * m_total] = next_path(lN);
+    for (uint32_t j = 0; j < n_pre; ++j) {
+      values[2 * m_total + 1 + j] = next_value();
+      paths[2 * m_total + 1 + j] = next_path(lN);
+    }
+    proof.u64(p0s[qi]);
+    proof.qs(values);
+    proof.u64(reveal_len);
+    for (auto& p : paths) proof.digests(p);
+  }
+  ZS_CUDA(cudaStreamSynchronize(st));
+  return proof.out;
+}
+
+}  // namespace zs

@@ -1,0 +1,16 @@
+// GenericStark(Air) prover on the device (see stark.cu).
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+
+namespace zs {
+
+// Proves `trace` (and `preprocessed`) for the compiled-in AIR `air_id` with the
+// transcript separator `sep`; every argument is in the reference's wire format.
+// Returns the serialized GenericStark(Air).Proof (stark.zig:107-122).
+std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params, size_t params_len, const uint8_t* pi,
+                                 size_t pi_len, const uint8_t* pre, size_t pre_len, const uint8_t* trace,
+                                 size_t trace_len, const uint8_t* sep, size_t sep_len, cudaStream_t st);
+
+}  // namespace zs

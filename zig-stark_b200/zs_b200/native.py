@@ -229,3 +229,60 @@ def circle_lde_noalloc(d_in, d_out, n_columns, log_rows, log_blowup, stream=None
     ints); returns the C ABI status code."""
     return int(lib().zs_m31_circle_lde_noalloc(ctypes.c_void_p(d_in), ctypes.c_void_p(d_out), n_columns, log_rows,
                                                log_blowup, ctypes.c_void_p(stream or 0)))
+
+
+# ---------------------------------------------------------------------------
+# prover (zs_m31_prove)
+# ---------------------------------------------------------------------------
+
+_libc = ctypes.CDLL(None)
+_libc.malloc.restype = ctypes.c_void_p
+_libc.malloc.argtypes = [ctypes.c_size_t]
+_libc.free.restype = None
+_libc.free.argtypes = [ctypes.c_void_p]
+_ALLOC_T = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
+_FREE_T = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t)
+
+
+class HostAllocator(ctypes.Structure):
+    """zs_host_allocator (zig-capi.h:35-39) backed by the C library's malloc/free."""
+    _fields_ = [("ctx", ctypes.c_void_p), ("alloc", _ALLOC_T), ("free", _FREE_T)]
+
+
+_ALLOC = _ALLOC_T(lambda ctx, size: _libc.malloc(size))
+_FREE = _FREE_T(lambda ctx, ptr, size: _libc.free(ptr))
+HOST = HostAllocator(None, _ALLOC, _FREE)
+
+
+def _bind_prove():
+    L = lib()
+    if not getattr(L, "_prove_bound", False):
+        L.zs_m31_prove.argtypes = [HostAllocator, ctypes.c_uint32] + [ctypes.c_char_p, ctypes.c_size_t] * 5 + \
+            [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]
+        L.zs_free.argtypes = [HostAllocator, ctypes.c_void_p, ctypes.c_size_t]
+        L.zs_free.restype = None
+        L._prove_bound = True
+    return L
+
+
+def prove(air_id, params, public_inputs, trace, preprocessed=b"", channel_sep=b""):
+    """GenericStark(Air).proveWithPreprocessed on the GPU; returns the serialized proof.
+
+    params: wire StarkParams bytes (or wire.StarkParams); trace / preprocessed: wire
+    []const []const QM31 bytes (or lists of (n, 4) uint32 arrays)."""
+    from . import wire
+    if not isinstance(params, (bytes, bytearray)):
+        params = params.encode()
+    if not isinstance(trace, (bytes, bytearray)):
+        trace = wire.columns(trace)
+    if not isinstance(preprocessed, (bytes, bytearray)):
+        preprocessed = wire.columns(preprocessed)
+    L = _bind_prove()
+    out = ctypes.c_void_p()
+    n = ctypes.c_size_t()
+    check(L.zs_m31_prove(HOST, air_id, params, len(params), public_inputs, len(public_inputs), preprocessed,
+                         len(preprocessed), trace, len(trace), channel_sep, len(channel_sep), ctypes.byref(out),
+                         ctypes.byref(n)), "zs_m31_prove")
+    data = ctypes.string_at(out.value, n.value)
+    L.zs_free(HOST, out, n.value)
+    return data
