@@ -154,16 +154,18 @@ __device__ __forceinline__ void chunk(uint32_t* s, uint32_t gstride, unsigned G,
       for (int l = R - 1; l >= 0; --l) {
         const unsigned i = b0 + l + shift;
         const uint32_t* T = TW + (n_dom - (n_dom >> i)) + (Vh << (R - l - 1));
+        uint32_t tws[1 << (R - 1)];
 #pragma unroll
-        for (int hb = 0; hb < (1 << (R - 1 - l)); ++hb) {
-          const uint32_t t = __ldg(T + hb);
+        for (int hb = 0; hb < (1 << (R - 1)); ++hb)
+          if (hb < (1 << (R - 1 - l))) tws[hb] = __ldg(T + hb);
 #pragma unroll
-          for (int lm = 0; lm < (1 << l); ++lm) {
-            const int m0 = (hb << (l + 1)) | lm, m1 = m0 | (1 << l);
-            const uint32_t x1 = mmul(v[m1], t), x0 = v[m0];
-            v[m1] = msub(x0, x1);
-            v[m0] = madd(x0, x1);
-          }
+        for (int m0 = 0; m0 < (1 << R); ++m0) {
+          if (m0 & (1 << l)) continue;
+          const int m1 = m0 | (1 << l);
+          const uint32_t t = tws[m0 >> (l + 1)];
+          const uint32_t x1 = mmul(v[m1], t), x0 = v[m0];
+          v[m1] = msub(x0, x1);
+          v[m0] = madd(x0, x1);
         }
       }
     } else {
@@ -171,16 +173,18 @@ __device__ __forceinline__ void chunk(uint32_t* s, uint32_t gstride, unsigned G,
       for (int l = 0; l < R; ++l) {
         const unsigned i = b0 + l + shift;
         const uint32_t* T = TW + (n_dom - (n_dom >> i)) + (Vh << (R - l - 1));
+        uint32_t tws[1 << (R - 1)];
 #pragma unroll
-        for (int hb = 0; hb < (1 << (R - 1 - l)); ++hb) {
-          const uint32_t t = __ldg(T + hb);
+        for (int hb = 0; hb < (1 << (R - 1)); ++hb)
+          if (hb < (1 << (R - 1 - l))) tws[hb] = __ldg(T + hb);
 #pragma unroll
-          for (int lm = 0; lm < (1 << l); ++lm) {
-            const int m0 = (hb << (l + 1)) | lm, m1 = m0 | (1 << l);
-            const uint32_t x0 = v[m0], x1 = v[m1];
-            v[m0] = madd(x0, x1);
-            v[m1] = mmul(msub(x0, x1), t);
-          }
+        for (int m0 = 0; m0 < (1 << R); ++m0) {
+          if (m0 & (1 << l)) continue;
+          const int m1 = m0 | (1 << l);
+          const uint32_t t = tws[m0 >> (l + 1)];
+          const uint32_t x0 = v[m0], x1 = v[m1];
+          v[m0] = madd(x0, x1);
+          v[m1] = mmul(msub(x0, x1), t);
         }
       }
     }
@@ -370,8 +374,9 @@ unsigned pick_split(unsigned L) {
   unsigned k = L <= 20 ? (L < 10 ? L : 10) : (L + 1) / 2;
   return k;
 }
-unsigned pick_groups(unsigned M, uint32_t n_groups) {
-  uint32_t g = kGroupWords >> M;
+// Groups per CTA: up to `budget` words of group data per shared buffer, at most 16.
+unsigned pick_groups(unsigned M, uint32_t n_groups, uint32_t budget = kGroupWords) {
+  uint32_t g = budget >> M;
   if (g == 0) g = 1;
   if (g > 16) g = 16;
   if (g > n_groups) g = n_groups;
@@ -408,7 +413,7 @@ void circle_lde(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, size_t 
   {
     const unsigned M = L - K;
     const uint32_t ngroups = 1u << K;
-    const unsigned G = pick_groups(M, ngroups);
+    const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
     const size_t sb = smem_bytes(M, G, 2);
     set_smem((const void*)k_mid, sb);
     k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(tmp, n, mid, (size_t)n << B, L, K, B, G, small.itw, big.tw,
@@ -431,7 +436,7 @@ void circle_fft(const uint32_t* d_coeffs, uint32_t* d_evals, uint32_t C, const C
   const uint32_t n = 1u << L;
   {
     const uint32_t ngroups = 1u << K;
-    const unsigned G = pick_groups(M, ngroups);
+    const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
     const size_t sb = smem_bytes(M, G, 2);
     set_smem((const void*)k_mid, sb);
     k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_coeffs, n, scratch, n, L, K, 0, G, dom.itw, dom.tw,
@@ -460,7 +465,7 @@ void circle_ifft(const uint32_t* d_evals, uint32_t* d_coeffs, uint32_t C, const 
   }
   {
     const uint32_t ngroups = 1u << K;
-    const unsigned G = pick_groups(M, ngroups);
+    const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
     const size_t sb = smem_bytes(M, G, 2);
     set_smem((const void*)k_mid, sb);
     k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(scratch, n, d_coeffs, n, L, K, 0, G, dom.itw, dom.tw,
@@ -508,7 +513,7 @@ void circle_lde_tables(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, 
   {
     const unsigned M = L - K;
     const uint32_t ngroups = 1u << K;
-    const unsigned G = pick_groups(M, ngroups);
+    const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
     const size_t sb = smem_bytes(M, G, 2);
     set_smem((const void*)k_mid, sb);
     k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(tmp, n, mid, (size_t)n << B, L, K, B, G, itw_small, tw_big,

@@ -1,6 +1,7 @@
 // The circle commit workload as one device-resident plan: circle LDE of all
 // columns, row-leaf Merkle tree fused with the gamma combination and the layer-0
 // FRI commitment, then the fold chain with one fused fold+commit launch per layer.
+#include <cstdlib>
 #include <memory>
 #include <vector>
 
@@ -15,6 +16,9 @@ CommitPlan::CommitPlan(uint32_t C_, unsigned L_, unsigned B_, unsigned F_) : C(C
   if (L < 1 || L + B > 28) throw Error(ZS_EMALFORMED, "log_rows + log_blowup must be in [1, 28]");
   if (F > L + B) throw Error(ZS_EMALFORMED, "more folds than domain bits");
   ZS_CUDA(cudaStreamCreateWithFlags(&setup, cudaStreamNonBlocking));
+  for (auto& s : sides) ZS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  events.resize(F + 2 + kSides);
+  for (auto& e : events) ZS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   const size_t n = (size_t)1 << L, N = (size_t)1 << (L + B);
   small = std::make_unique<CircleDomain>(L, setup);
   big = std::make_unique<CircleDomain>(L + B, setup);
@@ -34,11 +38,14 @@ CommitPlan::CommitPlan(uint32_t C_, unsigned L_, unsigned B_, unsigned F_) : C(C
     alloc((void**)&layer_trees[i].words, DeviceTree::words_for(L + B - i) * sizeof(uint32_t));
   }
   alphas.assign(F, qzero());
+  const char* env = std::getenv("ZS_NO_GRAPH");
+  use_graph = !(env && env[0] == '1');
   ZS_CUDA(cudaStreamSynchronize(setup));
 }
 
 CommitPlan::~CommitPlan() {
   cudaDeviceSynchronize();
+  drop_graph();
   cudaFree(trace);
   cudaFree(lde);
   cudaFree(scratch);
@@ -49,6 +56,8 @@ CommitPlan::~CommitPlan() {
   small.reset();
   big.reset();
   tabs.reset();
+  for (auto& e : events) cudaEventDestroy(e);
+  for (auto& s : sides) cudaStreamDestroy(s);
   cudaStreamDestroy(setup);
 }
 
@@ -58,6 +67,7 @@ void CommitPlan::set_challenges(const uint32_t* h_gammas, const uint32_t* h_alph
   for (unsigned i = 0; i < F; ++i)
     alphas[i] = qmake(h_alphas[4 * i], h_alphas[4 * i + 1], h_alphas[4 * i + 2], h_alphas[4 * i + 3]);
   ZS_CUDA(cudaMemcpy(gammas, g.data(), C * sizeof(qm31), cudaMemcpyHostToDevice));
+  drop_graph();  // fold challenges are baked into the captured launches
 }
 
 void CommitPlan::run_phase(int phase, const uint32_t* d_trace, cudaStream_t st) {
@@ -81,41 +91,82 @@ void CommitPlan::run_phase(int phase, const uint32_t* d_trace, cudaStream_t st) 
   }
 }
 
+// The step as a DAG: the LDE, the row leaves and the fold chain run on `st`; each
+// tree above its leaves (the row tree, the g tree, every committed fold layer's
+// tree) is finished on a side stream as soon as its leaves exist, so the narrow
+// tops of the trees overlap with each other and with the folds.
+void CommitPlan::run_direct(const uint32_t* d_trace, cudaStream_t st) {
+  const size_t n = (size_t)1 << L, N = (size_t)1 << (L + B);
+  if (!d_trace) d_trace = trace;
+  circle_lde(d_trace, n, lde, N, C, L, B, *small, *big, scratch, st);
+  build_row_leaves(lde, N, C, row_tree, gammas, layers[0], F > 0 ? &layer_trees[0] : nullptr, st);
+  unsigned side = 0;
+  bool used[kSides] = {};
+  auto branch = [&](DeviceTree& t) {
+    cudaEvent_t e = events[ev_used++];
+    ZS_CUDA(cudaEventRecord(e, st));
+    used[side % kSides] = true;
+    cudaStream_t s = sides[side++ % kSides];
+    ZS_CUDA(cudaStreamWaitEvent(s, e, 0));
+    tree_finish(t, 0, s);
+  };
+  ev_used = 0;
+  branch(row_tree);
+  if (F > 0) branch(layer_trees[0]);
+  for (unsigned i = 0; i < F; ++i) {
+    const uint32_t half = (uint32_t)(N >> (i + 1));
+    const bool commit = i + 1 < F;
+    fri_fold(layers[i], layers[i + 1], half, alphas[i], i, *tabs, commit ? &layer_trees[i + 1] : nullptr, st,
+             /*finish_tree=*/false);
+    if (commit) branch(layer_trees[i + 1]);
+  }
+  for (unsigned k = 0; k < kSides; ++k) {
+    if (!used[k]) continue;  // only streams forked from `st` may join it (graph capture)
+    cudaEvent_t e = events[ev_used++];
+    ZS_CUDA(cudaEventRecord(e, sides[k]));
+    ZS_CUDA(cudaStreamWaitEvent(st, e, 0));
+  }
+}
+
+void CommitPlan::drop_graph() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  graph_exec = nullptr;
+  graph_trace = nullptr;
+}
+
+// The whole step is one CUDA graph (about a hundred launches, most of them small
+// tree and fold kernels), captured on the plan's own stream and replayed on the
+// caller's; it is recaptured when the trace pointer or the challenges change.
 void CommitPlan::run(const uint32_t* d_trace, cudaStream_t st) {
-  run_phase(PHASE_LDE, d_trace, st);
-  run_phase(PHASE_ROW_TREE, d_trace, st);
-  run_phase(PHASE_FOLDS, d_trace, st);
+  if (!d_trace) d_trace = trace;
+  if (!use_graph) return run_direct(d_trace, st);
+  if (!graph_exec || graph_trace != d_trace) {
+    drop_graph();
+    cudaGraph_t g = nullptr;
+    ZS_CUDA(cudaStreamBeginCapture(setup, cudaStreamCaptureModeThreadLocal));
+    try {
+      run_direct(d_trace, setup);
+    } catch (...) {
+      cudaStreamEndCapture(setup, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    ZS_CUDA(cudaStreamEndCapture(setup, &g));
+    const cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    ZS_CUDA(e);
+    graph_trace = d_trace;
+  }
+  ZS_CUDA(cudaGraphLaunch(graph_exec, st));
 }
 
 uint32_t CommitPlan::launches() const {
-  // circle_lde: 3; row tree: leaf kernel + tree_up launches (+ those of the g tree);
-  // each fold: 1 + tree_up launches of the next layer's tree.
-  auto up = [](unsigned log_n, unsigned from) {
-    uint32_t k = 0;
-    unsigned lvl = from;
-    while (lvl < log_n) {
-      const uint64_t count = (uint64_t)1 << (log_n - lvl);
-      const uint64_t per = count >= 512 ? 512 : count;
-      unsigned g = 0;
-      while (((uint64_t)1 << g) < per) ++g;
-      lvl += g;
-      ++k;
-    }
-    return k;
-  };
-  auto run_log = [](uint64_t count) {
-    const uint64_t threads = count >= 256 ? 256 : count;
-    unsigned g = 0;
-    while (((uint64_t)1 << g) < threads) ++g;
-    return g;
-  };
+  // circle_lde: 3; row leaves: 1 + the row tree's and the g tree's tree_finish;
+  // each fold: 1 + the folded layer's tree_finish when it is committed.
   const unsigned LB = L + B;
-  uint32_t k = 3 + 1 + up(LB, run_log((uint64_t)1 << LB));
-  if (F > 0) k += up(LB, run_log((uint64_t)1 << LB));
-  for (unsigned i = 0; i < F; ++i) {
-    k += 1;
-    if (i + 1 < F) k += up(LB - i - 1, run_log((uint64_t)1 << (LB - i - 1)));
-  }
+  uint32_t k = 3 + 1 + tree_finish_launches(LB, 0);
+  if (F > 0) k += tree_finish_launches(LB, 0);
+  for (unsigned i = 0; i < F; ++i) k += 1 + (i + 1 < F ? tree_finish_launches(LB - i - 1, 0) : 0);
   return k;
 }
 

@@ -31,11 +31,23 @@ struct CommitPlan {
   CommitPlan(const CommitPlan&) = delete;
   CommitPlan& operator=(const CommitPlan&) = delete;
   void set_challenges(const uint32_t* h_gammas, const uint32_t* h_alphas);
+  // Replays the captured graph of the whole step (set ZS_NO_GRAPH=1 for direct launches).
   void run(const uint32_t* d_trace, cudaStream_t st);
+  void run_direct(const uint32_t* d_trace, cudaStream_t st);
   // One of the three phases of run(): the circle LDE (3 launches); the row-leaf
   // tree fused with the gamma combination and the layer-0 tree; the fold chain.
   void run_phase(int phase, const uint32_t* d_trace, cudaStream_t st);
   uint32_t launches() const;
+
+ private:
+  static constexpr unsigned kSides = 3;
+  cudaStream_t sides[kSides] = {};
+  std::vector<cudaEvent_t> events;
+  unsigned ev_used = 0;
+  bool use_graph = true;
+  cudaGraphExec_t graph_exec = nullptr;
+  const uint32_t* graph_trace = nullptr;
+  void drop_graph();
 };
 
 }  // namespace zs

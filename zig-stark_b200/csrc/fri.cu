@@ -32,8 +32,7 @@ FoldTables::~FoldTables() { cudaFree(tables); }
 qm31 FoldTables::offset_inv(unsigned layer) const { return qinv(qpow(q_fri_offset(), (uint64_t)1 << layer)); }
 
 namespace {
-constexpr unsigned kRun = 256;
-constexpr unsigned kSPad = kRun + 1;
+constexpr unsigned kThreads = 256;
 }  // namespace
 
 __device__ __forceinline__ qm31 ld_q(const qm31* p) {
@@ -41,13 +40,12 @@ __device__ __forceinline__ qm31 ld_q(const qm31* p) {
   return qmake(r.x, r.y, r.z, r.w);
 }
 
-__global__ void __launch_bounds__(kRun) k_fold(const qm31* __restrict__ in, qm31* __restrict__ out, uint32_t half,
-                                               qm31 alpha, qm31 off_inv, unsigned layer,
-                                               const qm31* __restrict__ tabs, uint32_t* tree_words,
-                                               unsigned log_next) {
-  __shared__ uint32_t d[8 * kSPad];
-  const uint64_t first = (uint64_t)blockIdx.x * blockDim.x;
-  const uint32_t j = (uint32_t)(first + threadIdx.x);
+// One fold output per thread, plus its hashQM31 leaf when the folded layer is committed.
+__global__ void __launch_bounds__(kThreads) k_fold(const qm31* __restrict__ in, qm31* __restrict__ out, uint32_t half,
+                                                   qm31 alpha, qm31 off_inv, unsigned layer,
+                                                   const qm31* __restrict__ tabs, uint32_t* leaf_words) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= half) return;
   const qm31 y0 = ld_q(in + j), y1 = ld_q(in + j + half);
   const uint64_t k = (uint64_t)j << layer;
   qm31 xinv = qmul(ld_q(tabs + (k & 2047)), ld_q(tabs + 2048 + ((k >> 11) & 2047)));
@@ -58,57 +56,20 @@ __global__ void __launch_bounds__(kRun) k_fold(const qm31* __restrict__ in, qm31
   const qm31 hd = qmul_m(qmul(qsub(y0, y1), xinv), inv2);
   const qm31 r = qadd(hs, qmul(alpha, hd));
   reinterpret_cast<uint4*>(out)[j] = make_uint4(r.a.a, r.a.b, r.b.a, r.b.b);
-  if (!tree_words) return;
+  if (!leaf_words) return;
   uint32_t o[8];
   b3::hash_qm31(r, o);
-  {
-    uint4* dst = reinterpret_cast<uint4*>(tree_words + 8 * (size_t)j);
-    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
-  }
-#pragma unroll
-  for (int w = 0; w < 8; ++w) d[w * kSPad + threadIdx.x] = o[w];
-  __syncthreads();
-  // climb the run's subtree (same scheme as the Merkle leaf kernels)
-  const size_t N2 = (size_t)2 << log_next;
-  unsigned lvl = 0;
-  for (unsigned cnt = blockDim.x >> 1; cnt >= 1; cnt >>= 1) {
-    ++lvl;
-    const unsigned t = threadIdx.x;
-    uint32_t oo[8];
-    const bool act = t < cnt;
-    if (act) {
-      uint32_t l[8], rr[8];
-#pragma unroll
-      for (int w = 0; w < 8; ++w) {
-        l[w] = d[w * kSPad + 2 * t];
-        rr[w] = d[w * kSPad + 2 * t + 1];
-      }
-      b3::hash2(l, rr, oo);
-    }
-    __syncthreads();
-    if (act) {
-#pragma unroll
-      for (int w = 0; w < 8; ++w) d[w * kSPad + t] = oo[w];
-      const uint64_t idx = (first >> lvl) + t;
-      uint4* dst = reinterpret_cast<uint4*>(tree_words + 8 * (N2 - (N2 >> lvl) + idx));
-      dst[0] = make_uint4(oo[0], oo[1], oo[2], oo[3]);
-      dst[1] = make_uint4(oo[4], oo[5], oo[6], oo[7]);
-    }
-    __syncthreads();
-  }
+  uint4* dst = reinterpret_cast<uint4*>(leaf_words + 8 * (size_t)j);
+  dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+  dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
 }
 
 void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31& alpha, unsigned layer,
-              const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st) {
-  const unsigned threads = half >= kRun ? kRun : half;
-  unsigned run_log = 0;
-  while ((1u << run_log) < threads) ++run_log;
-  k_fold<<<half / threads, threads, 0, st>>>(d_in, d_out, half, alpha, tabs.offset_inv(layer), layer, tabs.tables,
-                                             next_tree ? next_tree->words : nullptr,
-                                             next_tree ? next_tree->log_n : 0);
+              const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st, bool finish_tree) {
+  k_fold<<<(half + kThreads - 1) / kThreads, kThreads, 0, st>>>(d_in, d_out, half, alpha, tabs.offset_inv(layer), layer,
+                                                                tabs.tables, next_tree ? next_tree->words : nullptr);
   ZS_CUDA(cudaGetLastError());
-  if (next_tree) tree_finish(*next_tree, run_log, st);
+  if (next_tree && finish_tree) tree_finish(*next_tree, 0, st);
 }
 
 }  // namespace zs

@@ -20,8 +20,9 @@ struct FoldTables {
 
 // One fold (fri.zig:209-219): out[j] = (y0 + y1)/2 + alpha * (y0 - y1) / (2 D_layer[j]),
 // y0 = in[j], y1 = in[j + half], for j < half. When `next_tree` is given, also
-// writes the leaves hashQM31(out[j]) and the whole tree of the folded layer.
+// writes the leaves hashQM31(out[j]) and, unless `finish_tree` is false (the caller
+// finishes it elsewhere), the rest of the folded layer's tree.
 void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31& alpha, unsigned layer,
-              const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st);
+              const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st, bool finish_tree = true);
 
 }  // namespace zs

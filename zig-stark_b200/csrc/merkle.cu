@@ -1,94 +1,92 @@
 // Merkle trees on the device (src/core/merkle/merkle.zig:17-68).
 //
-// Leaves and the first levels are built by one CTA per run of up to 256 leaves:
-// each thread hashes its leaf with one Blake3 compression chain in registers, the
-// CTA keeps the run's digests in shared memory and climbs its subtree (hash2 =
-// Blake3("zig-stark:pair" || L || R), two compressions), writing every level
-// because openings need them. Levels above the runs are finished by k_tree_up
-// in the same way, 512 nodes per CTA.
+// Two kinds of kernels, both without block-wide barriers so every lane stays busy:
+//   leaf kernels: one thread per leaf, one Blake3 compression chain in registers
+//     (hashQM31 = 1 compression, hashM31s of a 64-value row = 4);
+//   k_tree_up: one thread per 2^s consecutive digests of a level (s <= 3) folds them
+//     into its own s-level subtree with hash2 (= Blake3("zig-stark:pair" || L || R),
+//     two compressions), writing every node, because openings need all levels.
+// A tree over 2^22 leaves therefore takes one leaf launch and eight tree launches.
 #include "blake3.cuh"
 #include "merkle.cuh"
 
 namespace zs {
 
 namespace {
-constexpr unsigned kRun = 256;      // leaves per CTA in the leaf kernels
-constexpr unsigned kSPad = kRun + 1;  // word-major digest rows in shared memory
-
-// Climbs the subtree of `count` digests held word-major in d[w * kSPad + i],
-// writing levels level0+1 .. level0+log2(count) of `tree`. `first` is the index
-// (at level0) of the CTA's first digest.
-__device__ void climb(uint32_t* d, unsigned count, uint32_t* tree_words, unsigned log_n, unsigned level0,
-                      uint64_t first) {
-  const size_t N2 = (size_t)2 << log_n;
-  unsigned lvl = level0;
-  for (unsigned cnt = count >> 1; cnt >= 1; cnt >>= 1) {
-    ++lvl;
-    const unsigned t = threadIdx.x;
-    uint32_t o[8];
-    const bool act = t < cnt;
-    if (act) {
-      uint32_t l[8], r[8];
-#pragma unroll
-      for (int w = 0; w < 8; ++w) {
-        l[w] = d[w * kSPad + 2 * t];
-        r[w] = d[w * kSPad + 2 * t + 1];
-      }
-      b3::hash2(l, r, o);
-    }
-    __syncthreads();
-    if (act) {
-#pragma unroll
-      for (int w = 0; w < 8; ++w) d[w * kSPad + t] = o[w];
-      const uint64_t idx = (first >> (lvl - level0)) + t;
-      uint4* dst = reinterpret_cast<uint4*>(tree_words + 8 * (N2 - (N2 >> lvl) + idx));
-      dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-      dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
-    }
-    __syncthreads();
-  }
-}
+constexpr unsigned kThreads = 256;
 
 __device__ __forceinline__ void put_digest(uint32_t* tree_words, size_t digest_index, const uint32_t o[8]) {
   uint4* dst = reinterpret_cast<uint4*>(tree_words + 8 * digest_index);
   dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
   dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
 }
+__device__ __forceinline__ void get_digest(const uint32_t* tree_words, size_t digest_index, uint32_t o[8]) {
+  const uint4* src = reinterpret_cast<const uint4*>(tree_words + 8 * digest_index);
+  const uint4 a = src[0], b = src[1];
+  o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+  o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+
+// The subtree over CNT (2, 4 or 8) consecutive digests of `level0` starting at index
+// `first` (a multiple of CNT): digests arrive in order from `next(k, d)`, a stack of
+// pending left siblings merges them, and every new node is written.
+template <int CNT, typename Next>
+__device__ __forceinline__ void thread_subtree(Next&& next, uint32_t* tree_words, unsigned log_n, unsigned level0,
+                                               uint64_t first) {
+  const size_t N2 = (size_t)2 << log_n;
+  uint32_t stk[3][8];
+#pragma unroll
+  for (int k = 0; k < CNT; ++k) {
+    uint32_t cur[8];
+    next(k, cur);
+    int depth = __popc(k) ;  // pending left siblings before merging leaf k (k's set bits)
+#pragma unroll
+    for (int b = 0; (1 << (b + 1)) <= CNT; ++b) {
+      if (((k >> b) & 1) == 0) break;
+      --depth;
+      uint32_t o[8];
+      b3::hash2(stk[depth], cur, o);
+#pragma unroll
+      for (int w = 0; w < 8; ++w) cur[w] = o[w];
+      const unsigned lvl = level0 + b + 1;
+      put_digest(tree_words, (N2 - (N2 >> lvl)) + ((first + k) >> (b + 1)), cur);
+    }
+    if (k + 1 < CNT) {
+#pragma unroll
+      for (int w = 0; w < 8; ++w) stk[depth][w] = cur[w];
+    }
+  }
+}
 }  // namespace
 
-// hashQM31 leaves + subtree per CTA.
-__global__ void __launch_bounds__(kRun) k_qm31_leaves(const qm31* __restrict__ vals, uint32_t* tree_words,
-                                                      unsigned log_n) {
-  __shared__ uint32_t d[8 * kSPad];
-  const uint64_t first = (uint64_t)blockIdx.x * blockDim.x;
-  const uint64_t i = first + threadIdx.x;
+// hashQM31 leaves (src/m31/hash.zig:33-37).
+__global__ void __launch_bounds__(kThreads) k_qm31_leaves(const qm31* __restrict__ vals, uint32_t* tree_words,
+                                                          uint64_t n) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
   const uint4 raw = __ldg(reinterpret_cast<const uint4*>(vals) + i);
   uint32_t o[8];
   b3::hash_qm31(qmake(raw.x, raw.y, raw.z, raw.w), o);
   put_digest(tree_words, i, o);
-#pragma unroll
-  for (int w = 0; w < 8; ++w) d[w * kSPad + threadIdx.x] = o[w];
-  __syncthreads();
-  climb(d, blockDim.x, tree_words, log_n, 0, first);
 }
 
-// Row leaves over C columns (+ optional gamma combination and its QM31 tree).
-__global__ void __launch_bounds__(kRun) k_row_leaves(const uint32_t* __restrict__ cols, size_t col_stride,
-                                                     uint32_t C, uint32_t* tree_words, unsigned log_n,
-                                                     const qm31* __restrict__ gammas, qm31* g_out,
-                                                     uint32_t* g_tree_words) {
-  __shared__ uint32_t d[8 * kSPad];
+// Row leaves hashM31s(col_0[r], ..., col_{C-1}[r]) (src/m31/hash.zig:15-25), and
+// optionally g[r] = sum_c gammas[c] * col_c[r] with its hashQM31 leaf.
+__global__ void __launch_bounds__(kThreads) k_row_leaves(const uint32_t* __restrict__ cols, size_t col_stride,
+                                                         uint32_t C, uint32_t* tree_words, uint64_t n,
+                                                         const qm31* __restrict__ gammas, qm31* g_out,
+                                                         uint32_t* g_tree_words) {
   __shared__ qm31 sg[256];
   const bool comb = gammas != nullptr;
   if (comb)
     for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) sg[c] = gammas[c];
   __syncthreads();
-  const uint64_t first = (uint64_t)blockIdx.x * blockDim.x;
-  const uint64_t r = first + threadIdx.x;
+  const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
   qm31 acc = qzero();
   uint32_t cv[8];
   b3::iv(cv);
-  const uint32_t nblocks = (C * 4 + 63) / 64 == 0 ? 1 : (C * 4 + 63) / 64;
+  const uint32_t nblocks = C * 4 <= 64 ? 1 : (C * 4 + 63) / 64;
   for (uint32_t blk = 0; blk < nblocks; ++blk) {
     uint32_t m[16];
 #pragma unroll
@@ -107,48 +105,25 @@ __global__ void __launch_bounds__(kRun) k_row_leaves(const uint32_t* __restrict_
     b3::compress_cv(cv, m, len, flags);
   }
   put_digest(tree_words, r, cv);
-#pragma unroll
-  for (int w = 0; w < 8; ++w) d[w * kSPad + threadIdx.x] = cv[w];
-  __syncthreads();
-  climb(d, blockDim.x, tree_words, log_n, 0, first);
   if (!comb) return;
   if (g_out) reinterpret_cast<uint4*>(g_out)[r] = make_uint4(acc.a.a, acc.a.b, acc.b.a, acc.b.b);
   if (g_tree_words) {
     uint32_t o[8];
     b3::hash_qm31(acc, o);
     put_digest(g_tree_words, r, o);
-#pragma unroll
-    for (int w = 0; w < 8; ++w) d[w * kSPad + threadIdx.x] = o[w];
-    __syncthreads();
-    climb(d, blockDim.x, g_tree_words, log_n, 0, first);
   }
 }
 
-// Levels above `level0`: each CTA climbs from up to 2 * blockDim.x digests.
-__global__ void __launch_bounds__(kRun) k_tree_up(uint32_t* tree_words, unsigned log_n, unsigned level0) {
-  __shared__ uint32_t d[8 * kSPad];
+// Levels level0+1 .. level0+log2(CNT): thread t folds digests [t*CNT, (t+1)*CNT) of level0.
+template <int CNT>
+__global__ void __launch_bounds__(kThreads) k_tree_up(uint32_t* tree_words, unsigned log_n, unsigned level0) {
+  const uint64_t count = ((uint64_t)1 << (log_n - level0)) / CNT;
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
   const size_t N2 = (size_t)2 << log_n;
-  const uint64_t count_in = (uint64_t)1 << (log_n - level0);
-  const unsigned per = 2 * blockDim.x < count_in ? 2 * blockDim.x : (unsigned)count_in;
-  const uint64_t first = (uint64_t)blockIdx.x * per;
   const uint32_t* src = tree_words + 8 * (N2 - (N2 >> level0));
-  // first level: pairs from global
-  const unsigned t = threadIdx.x;
-  const unsigned cnt = per >> 1;
-  uint32_t o[8];
-  if (t < cnt) {
-    uint32_t l[8], r[8];
-    const uint4* a = reinterpret_cast<const uint4*>(src + 8 * (first + 2 * t));
-    uint4 a0 = a[0], a1 = a[1], b0 = a[2], b1 = a[3];
-    l[0] = a0.x; l[1] = a0.y; l[2] = a0.z; l[3] = a0.w; l[4] = a1.x; l[5] = a1.y; l[6] = a1.z; l[7] = a1.w;
-    r[0] = b0.x; r[1] = b0.y; r[2] = b0.z; r[3] = b0.w; r[4] = b1.x; r[5] = b1.y; r[6] = b1.z; r[7] = b1.w;
-    b3::hash2(l, r, o);
-    put_digest(tree_words, (N2 - (N2 >> (level0 + 1))) + (first >> 1) + t, o);
-#pragma unroll
-    for (int w = 0; w < 8; ++w) d[w * kSPad + t] = o[w];
-  }
-  __syncthreads();
-  climb(d, cnt, tree_words, log_n, level0 + 1, first >> 1);
+  const uint64_t first = t * CNT;
+  thread_subtree<CNT>([&](int k, uint32_t d[8]) { get_digest(src, first + k, d); }, tree_words, log_n, level0, first);
 }
 
 static unsigned log2u(uint64_t x) {
@@ -157,36 +132,72 @@ static unsigned log2u(uint64_t x) {
   return l;
 }
 
+static void launch_up(DeviceTree& tree, unsigned lvl, unsigned s, cudaStream_t st) {
+  const uint64_t threads_total = ((uint64_t)1 << (tree.log_n - lvl)) >> s;
+  const unsigned blocks = (unsigned)((threads_total + kThreads - 1) / kThreads);
+  switch (s) {
+    case 1: k_tree_up<2><<<blocks, kThreads, 0, st>>>(tree.words, tree.log_n, lvl); break;
+    case 2: k_tree_up<4><<<blocks, kThreads, 0, st>>>(tree.words, tree.log_n, lvl); break;
+    default: k_tree_up<8><<<blocks, kThreads, 0, st>>>(tree.words, tree.log_n, lvl); break;
+  }
+}
+
+// Three levels per launch while a level still gives every SM plenty of threads
+// (one thread chains 7 nodes = 14 compressions); above that one level per launch,
+// so the narrow top of the tree costs one hash2 of latency per level.
+static unsigned levels_per_launch(unsigned log_n, unsigned lvl) {
+  const unsigned remaining = log_n - lvl;
+  if (remaining >= 3 && remaining >= 3 + 15) return 3;  // >= 2^15 threads of 8-node subtrees
+  return 1;
+}
+
 void tree_finish(DeviceTree& tree, unsigned from_level, cudaStream_t st) {
   unsigned lvl = from_level;
   while (lvl < tree.log_n) {
-    const uint64_t count = (uint64_t)1 << (tree.log_n - lvl);  // digests at lvl
-    const unsigned threads = count >= 2 * kRun ? kRun : (unsigned)(count / 2);
-    const uint64_t per = 2 * (uint64_t)threads;
-    k_tree_up<<<(unsigned)(count / per), threads, 0, st>>>(tree.words, tree.log_n, lvl);
-    lvl += log2u(per);
+    const unsigned s = levels_per_launch(tree.log_n, lvl);
+    launch_up(tree, lvl, s, st);
+    lvl += s;
   }
   ZS_CUDA(cudaGetLastError());
 }
 
+uint32_t tree_finish_launches(unsigned log_n, unsigned from_level) {
+  uint32_t k = 0;
+  for (unsigned lvl = from_level; lvl < log_n; lvl += levels_per_launch(log_n, lvl)) ++k;
+  return k;
+}
+
 void build_qm31_tree(const qm31* d_values, DeviceTree& tree, cudaStream_t st) {
   const uint64_t n = (uint64_t)1 << tree.log_n;
-  const unsigned threads = n >= kRun ? kRun : (unsigned)n;
-  k_qm31_leaves<<<(unsigned)(n / threads), threads, 0, st>>>(d_values, tree.words, tree.log_n);
+  k_qm31_leaves<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(d_values, tree.words, n);
   ZS_CUDA(cudaGetLastError());
-  tree_finish(tree, log2u(threads), st);
+  tree_finish(tree, 0, st);
+}
+
+void build_qm31_leaves(const qm31* d_values, DeviceTree& tree, cudaStream_t st) {
+  const uint64_t n = (uint64_t)1 << tree.log_n;
+  k_qm31_leaves<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(d_values, tree.words, n);
+  ZS_CUDA(cudaGetLastError());
+}
+
+void build_row_leaves(const uint32_t* d_cols, size_t col_stride, uint32_t C, DeviceTree& tree, const qm31* d_gammas,
+                      qm31* g_out, DeviceTree* g_tree, cudaStream_t st) {
+  if (C == 0 || C > 256) throw Error(ZS_EMALFORMED, "row leaves need 1..256 columns");
+  const uint64_t n = (uint64_t)1 << tree.log_n;
+  k_row_leaves<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+      d_cols, col_stride, C, tree.words, n, d_gammas, g_out, g_tree ? g_tree->words : nullptr);
+  ZS_CUDA(cudaGetLastError());
 }
 
 void build_row_tree(const uint32_t* d_cols, size_t col_stride, uint32_t C, DeviceTree& tree, const qm31* d_gammas,
                     qm31* g_out, DeviceTree* g_tree, cudaStream_t st) {
   if (C == 0 || C > 256) throw Error(ZS_EMALFORMED, "row leaves need 1..256 columns");
   const uint64_t n = (uint64_t)1 << tree.log_n;
-  const unsigned threads = n >= kRun ? kRun : (unsigned)n;
-  k_row_leaves<<<(unsigned)(n / threads), threads, 0, st>>>(d_cols, col_stride, C, tree.words, tree.log_n, d_gammas,
-                                                            g_out, g_tree ? g_tree->words : nullptr);
+  k_row_leaves<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(
+      d_cols, col_stride, C, tree.words, n, d_gammas, g_out, g_tree ? g_tree->words : nullptr);
   ZS_CUDA(cudaGetLastError());
-  tree_finish(tree, log2u(threads), st);
-  if (g_tree) tree_finish(*g_tree, log2u(threads), st);
+  tree_finish(tree, 0, st);
+  if (g_tree) tree_finish(*g_tree, 0, st);
 }
 
 // out[q * log_n * 8 ...] = siblings of indices[q], bottom-up.

@@ -25,8 +25,13 @@ struct DeviceTree {
 
 // Leaves hashQM31(values[i]) for 2^log_n QM31 values plus the whole tree.
 void build_qm31_tree(const qm31* d_values, DeviceTree& tree, cudaStream_t st);
-// Completes levels above `from_level` (levels <= from_level must be written).
+// Leaves only (level 0) of build_qm31_tree.
+void build_qm31_leaves(const qm31* d_values, DeviceTree& tree, cudaStream_t st);
+// Completes levels above `from_level` (levels <= from_level must be written), three
+// levels per launch.
 void tree_finish(DeviceTree& tree, unsigned from_level, cudaStream_t st);
+// Number of launches tree_finish makes.
+uint32_t tree_finish_launches(unsigned log_n, unsigned from_level);
 
 // Opening path of leaf `index` (siblings bottom-up, merkle.zig:57-68), read back to
 // the host from a device tree. `out` receives log_n digests of 32 bytes.
@@ -42,5 +47,8 @@ void tree_open_many(const DeviceTree& tree, const uint64_t* d_indices, uint32_t 
 // `g_tree` is not null, the tree over hashQM31(g[r]).
 void build_row_tree(const uint32_t* d_cols, size_t col_stride, uint32_t C, DeviceTree& tree, const qm31* d_gammas,
                     qm31* g_out, DeviceTree* g_tree, cudaStream_t st);
+// The leaf level only of build_row_tree (and of the g tree); finish with tree_finish.
+void build_row_leaves(const uint32_t* d_cols, size_t col_stride, uint32_t C, DeviceTree& tree, const qm31* d_gammas,
+                      qm31* g_out, DeviceTree* g_tree, cudaStream_t st);
 
 }  // namespace zs
