@@ -205,12 +205,83 @@ __device__ __forceinline__ void chunk_dispatch(unsigned r, uint32_t* s, uint32_t
   }
 }
 
+// Compile-time variant of `chunk` for a known group size 2^M and chunk offset B0.
+// The chunk's index bits never overlap the slot's, so element m sits at
+// padx(e0) + padx(m << B0): one runtime address per slot, immediate offsets after it.
+template <int R, bool INV, unsigned M, unsigned B0>
+__device__ __forceinline__ void chunk_ct(uint32_t* s, uint32_t gstride, unsigned G, unsigned shift,
+                                         const uint32_t* __restrict__ TW, uint32_t n_dom, const uint32_t* vb) {
+  constexpr unsigned SL = M - R;
+  const uint32_t total = G << SL;
+  for (uint32_t slot = threadIdx.x; slot < total; slot += blockDim.x) {
+    const uint32_t gi = slot >> SL;
+    const uint32_t rest = slot & ((1u << SL) - 1);
+    const uint32_t e0 = ((rest >> B0) << (B0 + R)) | (rest & ((1u << B0) - 1));
+    uint32_t* base = s + gi * gstride + padx(e0);
+    uint32_t v[1 << R];
+#pragma unroll
+    for (int m = 0; m < (1 << R); ++m) v[m] = base[(m << B0) + ((m << B0) >> 5)];
+    const uint32_t Vh = (vb[gi] + e0) >> (B0 + R);
+#pragma unroll
+    for (int ll = 0; ll < R; ++ll) {
+      const int l = INV ? ll : R - 1 - ll;
+      const unsigned i = B0 + l + shift;
+      const uint32_t* T = TW + (n_dom - (n_dom >> i)) + (Vh << (R - l - 1));
+      uint32_t tws[1 << (R - 1)];
+#pragma unroll
+      for (int hb = 0; hb < (1 << (R - 1)); ++hb)
+        if (hb < (1 << (R - 1 - l))) tws[hb] = __ldg(T + hb);
+#pragma unroll
+      for (int m0 = 0; m0 < (1 << R); ++m0) {
+        if (m0 & (1 << l)) continue;
+        const int m1 = m0 | (1 << l);
+        const uint32_t t = tws[m0 >> (l + 1)];
+        if (!INV) {
+          const uint32_t x1 = mmul(v[m1], t), x0 = v[m0];
+          v[m1] = msub(x0, x1);
+          v[m0] = madd(x0, x1);
+        } else {
+          const uint32_t x0 = v[m0], x1 = v[m1];
+          v[m0] = madd(x0, x1);
+          v[m1] = mmul(msub(x0, x1), t);
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < (1 << R); ++m) base[(m << B0) + ((m << B0) >> 5)] = v[m];
+  }
+}
+
+// All M layers with a compile-time chunk schedule (chunks of <= 4 layers, the
+// largest first), DONE layers already applied.
+template <bool INV, unsigned M, unsigned DONE>
+__device__ __forceinline__ void run_layers_ct(uint32_t* s, uint32_t gstride, unsigned G, unsigned shift,
+                                              const uint32_t* TW, uint32_t n_dom, const uint32_t* vb) {
+  if constexpr (DONE < M) {
+    constexpr unsigned REM = M - DONE;
+    constexpr unsigned NCH = (REM + 3) / 4;
+    constexpr unsigned R = (REM + NCH - 1) / NCH;
+    // forward: top-down, the chunk covers [M - DONE - R, M - DONE); inverse: bottom-up
+    constexpr unsigned B0 = INV ? DONE : M - DONE - R;
+    chunk_ct<R, INV, M, B0>(s, gstride, G, shift, TW, n_dom, vb);
+    __syncthreads();
+    run_layers_ct<INV, M, DONE + R>(s, gstride, G, shift, TW, n_dom, vb);
+  }
+}
+
 // All M local layers: DIF top-down for the forward transform, DIT bottom-up for
 // the inverse, in chunks of at most four layers.
 template <bool INV>
 __device__ __forceinline__ void run_layers(uint32_t* s, uint32_t gstride, unsigned G, unsigned M, unsigned shift,
                            const uint32_t* TW, uint32_t n_dom, const uint32_t* vb) {
   if (M == 0) return;
+  switch (M) {
+    case 8: return run_layers_ct<INV, 8, 0>(s, gstride, G, shift, TW, n_dom, vb);
+    case 9: return run_layers_ct<INV, 9, 0>(s, gstride, G, shift, TW, n_dom, vb);
+    case 10: return run_layers_ct<INV, 10, 0>(s, gstride, G, shift, TW, n_dom, vb);
+    case 11: return run_layers_ct<INV, 11, 0>(s, gstride, G, shift, TW, n_dom, vb);
+    default: break;
+  }
   const unsigned nch = (M + 3) / 4, base = M / nch, extra = M % nch;
   if (!INV) {
     unsigned top = M;
@@ -249,12 +320,14 @@ __global__ void __launch_bounds__(512) k_ifft_low(const uint32_t* __restrict__ i
   uint32_t* out = tmp + (size_t)blockIdx.y * n;
   if (threadIdx.x < G) vb[threadIdx.x] = bitrev(gp0 + threadIdx.x, hb) << K;
   const unsigned lg_g = 31 - __clz(G);
+  #pragma unroll 8
   for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
     const uint32_t t = idx & (G - 1), v = idx >> lg_g;
     sm[t * gstride + padx(bitrev(v, K))] = __ldg(col + ((size_t)v << hb) + gp0 + t);
   }
   __syncthreads();
   run_layers<true>(sm, gstride, G, K, 0, ITW, n, vb);
+  #pragma unroll 8
   for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
     const uint32_t t = idx >> K, e = idx & (gsz - 1);
     out[vb[t] + e] = sm[t * gstride + padx(e)];
@@ -269,7 +342,7 @@ __global__ void __launch_bounds__(512) k_ifft_low(const uint32_t* __restrict__ i
 //   mode FFT_ONLY:  load A-then-B coefficients interleaved, forward layers [K, L).
 enum MidMode : int { MID_LDE = 0, MID_IFFT_ONLY = 1, MID_FFT_ONLY = 2 };
 
-__global__ void __launch_bounds__(512) k_mid(const uint32_t* __restrict__ in, size_t in_stride,
+__global__ void __launch_bounds__(512, 2) k_mid(const uint32_t* __restrict__ in, size_t in_stride,
                                              uint32_t* __restrict__ out, size_t out_stride, unsigned L, unsigned K,
                                              unsigned B, unsigned G, const uint32_t* __restrict__ ITW_small,
                                              const uint32_t* __restrict__ TW_big, int mode) {
@@ -286,19 +359,22 @@ __global__ void __launch_bounds__(512) k_mid(const uint32_t* __restrict__ in, si
   if (threadIdx.x < G) vb[threadIdx.x] = 0;
   if (mode == MID_FFT_ONLY) {
     // interleaved position p holds A[p/2] (even p) or B[p/2] (odd p)
-    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+    #pragma unroll 8
+  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
       const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
       const uint32_t p = (hi << K) | (lo0 + t);
       s_in[t * gstride + padx(hi)] = __ldg(src + ((p & 1) ? (n >> 1) + (p >> 1) : (p >> 1)));
     }
     __syncthreads();
     run_layers<false>(s_in, gstride, G, M, K, TW_big, n << B, vb);
-    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+    #pragma unroll 8
+  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
       const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
       dst[((size_t)hi << K) + lo0 + t] = s_in[t * gstride + padx(hi)];
     }
     return;
   }
+  #pragma unroll 8
   for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
     const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
     s_in[t * gstride + padx(hi)] = __ldg(src + ((size_t)hi << K) + lo0 + t);
@@ -308,7 +384,8 @@ __global__ void __launch_bounds__(512) k_mid(const uint32_t* __restrict__ in, si
   // 1/n = 2^(31 - L) mod p: scaling is a rotation of the 31-bit word.
   const unsigned inv_n_shift = (31 - L) % 31;
   if (mode == MID_IFFT_ONLY) {
-    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+    #pragma unroll 8
+  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
       const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
       const uint32_t p = (hi << K) | (lo0 + t);
       const uint32_t v = mshl(s_in[t * gstride + padx(hi)], inv_n_shift);
@@ -316,6 +393,7 @@ __global__ void __launch_bounds__(512) k_mid(const uint32_t* __restrict__ in, si
     }
     return;
   }
+  #pragma unroll 8
   for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
     const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
     const uint32_t a = t * gstride + padx(hi);
@@ -327,7 +405,8 @@ __global__ void __launch_bounds__(512) k_mid(const uint32_t* __restrict__ in, si
     if (threadIdx.x < G) vb[threadIdx.x] = q << M;
     __syncthreads();
     run_layers<false>(s_w, gstride, G, M, K, TW_big, n << B, vb);
-    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+    #pragma unroll 8
+  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
       const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
       dst[(size_t)q * n + ((size_t)hi << K) + lo0 + t] = s_w[t * gstride + padx(hi)];
     }
@@ -349,6 +428,7 @@ __global__ void __launch_bounds__(512) k_fft_low(const uint32_t* __restrict__ mi
   uint32_t* dst = out + (size_t)blockIdx.y * out_stride;
   if (threadIdx.x < G) vb[threadIdx.x] = bitrev(q0 + threadIdx.x, hb) << K;
   __syncthreads();
+  #pragma unroll 8
   for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
     const uint32_t t = idx >> K, e = idx & (gsz - 1);
     sm[t * gstride + padx(e)] = __ldg(src + vb[t] + e);
@@ -356,6 +436,7 @@ __global__ void __launch_bounds__(512) k_fft_low(const uint32_t* __restrict__ mi
   __syncthreads();
   run_layers<false>(sm, gstride, G, K, 0, TW, N, vb);
   const unsigned lg_g = 31 - __clz(G);
+  #pragma unroll 8
   for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
     const uint32_t t = idx & (G - 1), v = idx >> lg_g;
     dst[((size_t)v << hb) + q0 + t] = sm[t * gstride + padx(bitrev(v, K))];

@@ -71,33 +71,67 @@ __global__ void __launch_bounds__(kThreads) k_qm31_leaves(const qm31* __restrict
 }
 
 // Row leaves hashM31s(col_0[r], ..., col_{C-1}[r]) (src/m31/hash.zig:15-25), and
-// optionally g[r] = sum_c gammas[c] * col_c[r] with its hashQM31 leaf.
+// optionally g[r] = sum_c gammas[c] * col_c[r] with its hashQM31 leaf. The four
+// coordinates of g accumulate unreduced 62-bit products in 64 bits (one wide
+// multiply-add each) with a Mersenne fold every four columns: after a fold the
+// accumulator is below 2^34, and four products below (p-1)^2 keep it below 2^64.
+__device__ __forceinline__ uint64_t fold64(uint64_t x) { return (x & P) + (x >> 31); }
+__device__ __forceinline__ uint32_t canon64(uint64_t x) {
+  x = fold64(fold64(x));  // < 2^31 + 8
+  const uint32_t s = (uint32_t)x;
+  return umin32(s, s - P);
+}
+
 __global__ void __launch_bounds__(kThreads) k_row_leaves(const uint32_t* __restrict__ cols, size_t col_stride,
                                                          uint32_t C, uint32_t* tree_words, uint64_t n,
                                                          const qm31* __restrict__ gammas, qm31* g_out,
                                                          uint32_t* g_tree_words) {
-  __shared__ qm31 sg[256];
+  __shared__ uint4 sg[256];
   const bool comb = gammas != nullptr;
   if (comb)
-    for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) sg[c] = gammas[c];
+    for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) sg[c] = reinterpret_cast<const uint4*>(gammas)[c];
   __syncthreads();
   const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
-  qm31 acc = qzero();
+  uint64_t acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
   uint32_t cv[8];
   b3::iv(cv);
   const uint32_t nblocks = C * 4 <= 64 ? 1 : (C * 4 + 63) / 64;
+  // The next block's 16 column loads are issued before the current block is
+  // compressed, so their latency hides behind ~700 integer instructions.
+  uint32_t nxt[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) nxt[k] = (uint32_t)k < C ? __ldg(cols + (size_t)k * col_stride + r) : 0u;
   for (uint32_t blk = 0; blk < nblocks; ++blk) {
     uint32_t m[16];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      const uint32_t w = blk * 16 + k;
-      uint32_t v = 0;
-      if (w < C) {
-        v = __ldg(cols + (size_t)w * col_stride + r);
-        if (comb) acc = qadd(acc, qmul_m(sg[w], v));
+    for (int k = 0; k < 16; ++k) m[k] = nxt[k];
+    if (blk + 1 < nblocks) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const uint32_t w = (blk + 1) * 16 + k;
+        nxt[k] = w < C ? __ldg(cols + (size_t)w * col_stride + r) : 0u;
       }
-      m[k] = v;
+    }
+    if (comb) {
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        const uint32_t w = blk * 16 + k;
+        if (w < C) {
+          const uint4 g = sg[w];
+          const uint32_t v = m[k];
+          acc0 += (uint64_t)g.x * v;
+          acc1 += (uint64_t)g.y * v;
+          acc2 += (uint64_t)g.z * v;
+          acc3 += (uint64_t)g.w * v;
+        }
+        if ((k & 3) == 3) {
+          acc0 = fold64(acc0);
+          acc1 = fold64(acc1);
+          acc2 = fold64(acc2);
+          acc3 = fold64(acc3);
+        }
+      }
     }
     const int rem = (int)(C * 4) - (int)(blk * 64);
     const uint32_t len = rem >= 64 ? 64u : (uint32_t)rem;
@@ -106,6 +140,7 @@ __global__ void __launch_bounds__(kThreads) k_row_leaves(const uint32_t* __restr
   }
   put_digest(tree_words, r, cv);
   if (!comb) return;
+  const qm31 acc = qmake(canon64(acc0), canon64(acc1), canon64(acc2), canon64(acc3));
   if (g_out) reinterpret_cast<uint4*>(g_out)[r] = make_uint4(acc.a.a, acc.a.b, acc.b.a, acc.b.b);
   if (g_tree_words) {
     uint32_t o[8];
