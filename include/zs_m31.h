@@ -69,6 +69,23 @@ int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t *par
                      size_t preprocessed_len, const uint8_t *trace, size_t trace_len, const uint8_t *channel_sep,
                      size_t channel_sep_len, uint8_t **out_proof, size_t *out_len);
 
+/* Replaces GenericStark(Air).verify (src/m31/stark.zig:660-784); conventions of
+ * zs_binius_verify (zig-capi.h:53-63). Sets *out_ok to 1 when the proof verifies and
+ * 0 otherwise; returns 0, or a negative code when the inputs cannot be parsed. Runs
+ * on the host (the reference's verifier is a few hundred hashes per query). */
+int32_t zs_m31_verify(zs_host_allocator host, uint32_t air_id, const uint8_t *params, size_t params_len,
+                      const uint8_t *public_inputs, size_t public_inputs_len, const uint8_t *proof, size_t proof_len,
+                      const uint8_t *channel_sep, size_t channel_sep_len, int *out_ok);
+
+/* The commitment path alone (stark.zig:397-414): each column (wire
+ * []const []const QM31, 2^trace_log values each) is interpolated on H, evaluated on
+ * D = FRI_OFFSET * <w_N> with N = 2^(trace_log + log_blowup) and committed as a
+ * Merkle tree of hashQM31 leaves. Output: the roots as wire []Digest (u64 count,
+ * then 32 bytes per column), allocated with `host`; the shape of zs_binius_commit
+ * (zig-capi.h:65-71). */
+int32_t zs_m31_commit_columns(zs_host_allocator host, uint8_t trace_log, uint8_t log_blowup, const uint8_t *columns,
+                              size_t columns_len, uint8_t **out_roots, size_t *out_len);
+
 /* ---- circle FFT -------------------------------------------------------------
  * Replaces src/cuda/circlefft_gpu.zig:46-108 circleFFT(allocator, coeffs, half_coset,
  * evals) and :111-175 circleIFFT(...), themselves GPU versions of

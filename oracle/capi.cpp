@@ -288,6 +288,25 @@ int orc_verify(uint32_t air_id, const uint8_t* params, size_t params_len, const 
   }
 }
 
+// Per-column commitment roots (stark.zig:397-414): NTT interpolation on H, coset
+// evaluation on D, MerkleTree over hashQM31 leaves. out: 32 bytes per column.
+int orc_commit_columns(const uint8_t* cols, size_t cols_len, unsigned trace_log, unsigned log_blowup, uint8_t* out) {
+  try {
+    auto c = readColumns(cols, cols_len);
+    for (size_t j = 0; j < c.size(); ++j) {
+      std::vector<QM31> coeffs = interpolateSubgroupNtt(c[j], trace_log);
+      std::vector<QM31> cw = evaluateCosetNtt(coeffs, friOffset(), trace_log + log_blowup);
+      MerkleTree t(hashCodeword(cw));
+      std::memcpy(out + 32 * j, t.root().data(), 32);
+    }
+    return 0;
+  } catch (const WireError& e) {
+    return e.code;
+  } catch (...) {
+    return -1;
+  }
+}
+
 // Re-serializes a proof after a round trip through the wire reader.
 int orc_proof_roundtrip(const uint8_t* proof, size_t proof_len, uint8_t** out, size_t* out_len) {
   try {

@@ -65,6 +65,7 @@ def lib():
                                  ctypes.c_size_t, ctypes.POINTER(ctypes.c_int)]
         L.orc_proof_roundtrip.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(u8p),
                                           ctypes.POINTER(ctypes.c_size_t)]
+        L.orc_commit_columns.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_uint, ctypes.c_uint, u8p]
         L.orc_circle_commit.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u32p, u32p,
                                         ctypes.c_uint32, ctypes.c_int, ctypes.c_int, u8p, u8p, u32p, u32p, u32p]
         _lib = L
@@ -297,3 +298,11 @@ def circle_commit(trace, log_blowup, gammas, alphas, faithful=False, threads=Non
         res["lde"] = lde
         res["g"] = g
     return res
+
+
+def commit_columns(columns: bytes, n_columns, trace_log, log_blowup):
+    out = (ctypes.c_uint8 * (32 * max(n_columns, 1)))()
+    rc = lib().orc_commit_columns(columns, len(columns), trace_log, log_blowup, out)
+    if rc != 0:
+        raise RuntimeError(f"orc_commit_columns failed: {rc}")
+    return [bytes(out)[32 * j:32 * j + 32] for j in range(n_columns)]

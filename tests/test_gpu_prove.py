@@ -83,3 +83,21 @@ def test_malformed_inputs(orc):
     with pytest.raises(native.ZsError) as e:
         native.prove(99, params, b"", tr)
     assert e.value.code == -1
+
+
+@pytest.mark.parametrize("trace_log,log_blowup,n_cols", [(0, 1, 1), (3, 2, 2), (10, 2, 5), (14, 1, 3), (16, 2, 2)])
+def test_commit_columns(orc, trace_log, log_blowup, n_cols):
+    """zs_m31_commit_columns = the per-column trees of stark.zig:397-414."""
+    from zs_b200 import native
+    rng = np.random.default_rng(trace_log * 7 + n_cols)
+    cols = [rng.integers(0, wl.P, (1 << trace_log, 4), dtype=np.uint32) for _ in range(n_cols)]
+    b = wire.columns(cols)
+    assert native.commit_columns(b, trace_log, log_blowup) == orc.commit_columns(b, n_cols, trace_log, log_blowup)
+
+
+def test_gpu_proofs_verify_with_library_verifier(orc):
+    from zs_b200 import native
+    tr, pi = wl.seeded_fib(10)
+    params = wire.StarkParams(10, 2, 16, 3)
+    proof = native.prove(wl.AIR_SEEDED_FIB, params, pi, tr, b"", b"lib")
+    assert native.verify(wl.AIR_SEEDED_FIB, params, pi, proof, b"lib")

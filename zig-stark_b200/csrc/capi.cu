@@ -7,6 +7,7 @@
 #include "circle.cuh"
 #include "commit.cuh"
 #include "stark.cuh"
+#include "verify.cuh"
 
 using namespace zs;
 
@@ -204,6 +205,48 @@ int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t* par
     if (!buf) throw Error(ZS_ENOMEM, "host allocator returned null");
     std::memcpy(buf, bytes.data(), bytes.size());
     *out_proof = buf;
+    *out_len = bytes.size();
+  });
+}
+
+int32_t zs_m31_verify(zs_host_allocator host, uint32_t air_id, const uint8_t* params, size_t params_len,
+                      const uint8_t* public_inputs, size_t public_inputs_len, const uint8_t* proof, size_t proof_len,
+                      const uint8_t* channel_sep, size_t channel_sep_len, int* out_ok) {
+  (void)host;
+  return guarded([&] {
+    if (!out_ok) throw Error(ZS_EMALFORMED, "null out_ok");
+    if ((!params && params_len) || (!public_inputs && public_inputs_len) || (!proof && proof_len) ||
+        (!channel_sep && channel_sep_len))
+      throw Error(ZS_EMALFORMED, "null input buffer with a non-zero length");
+    *out_ok = 0;
+    *out_ok = stark_verify(air_id, params, params_len, public_inputs, public_inputs_len, proof, proof_len,
+                           channel_sep, channel_sep_len)
+                  ? 1
+                  : 0;
+  });
+}
+
+int32_t zs_m31_commit_columns(zs_host_allocator host, uint8_t trace_log, uint8_t log_blowup, const uint8_t* columns,
+                              size_t columns_len, uint8_t** out_roots, size_t* out_len) {
+  return guarded([&] {
+    if (!out_roots || !out_len || !host.alloc) throw Error(ZS_EMALFORMED, "null output or allocator");
+    if (!columns && columns_len) throw Error(ZS_EMALFORMED, "null input buffer with a non-zero length");
+    ensure_device();
+    cudaStream_t st = nullptr;
+    ZS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    std::vector<uint8_t> bytes;
+    try {
+      bytes = commit_columns(columns, columns_len, trace_log, log_blowup, st);
+    } catch (...) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+      throw;
+    }
+    cudaStreamDestroy(st);
+    uint8_t* buf = (uint8_t*)host.alloc(host.ctx, bytes.size());
+    if (!buf) throw Error(ZS_ENOMEM, "host allocator returned null");
+    std::memcpy(buf, bytes.data(), bytes.size());
+    *out_roots = buf;
     *out_len = bytes.size();
   });
 }

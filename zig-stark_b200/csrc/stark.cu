@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "airs.cuh"
+#include "constraints.cuh"
 #include "fri.cuh"
 #include "host.cuh"
 #include "merkle.cuh"
@@ -36,69 +37,11 @@ __device__ __forceinline__ void stq(qm31* p, const qm31& v) {
   *reinterpret_cast<uint4*>(p) = make_uint4(v.a.a, v.a.b, v.b.a, v.b.b);
 }
 
-// Everything the quotient and DEEP kernels need beyond the codewords.
-struct QuotConsts {
-  AirConsts air;
-  uint32_t m, m_total, n_pre, num_trans, n_rel, total_bound, shift;
-  unsigned log_N, log_blowup;
-  qm31 last_point;  // w^(n-1)
-  qm31 offset;      // FRI_OFFSET
-  qm31 alphas[kMaxTrans + 2 * kMaxRel];
-  qm31 betas[kMaxBound];
-  uint32_t b_col[kMaxBound];
-  qm31 b_val[kMaxBound];
-  qm31 b_pt[kMaxBound];  // p_k = w^step_k
-  qm31 zh[8], zh_inv[8];  // Z_H(d_i) depends on i mod 2^log_blowup
-  qm31 ac[kMaxKey], ar[kMaxRel];
-  uint32_t sel[kMaxRel], mult[kMaxRel], n_keys[kMaxRel], keys[kMaxRel][kMaxKey], tabs[kMaxRel][kMaxKey];
-};
-
 __device__ __forceinline__ qm31 domain_point(const QuotConsts& k, const qm31* __restrict__ wpow, uint32_t i) {
   // d_i = FRI_OFFSET * w_N^i, w_N^(N/2) = -1, wpow[k] = w_N^k for k < N/2
   const uint32_t half = 1u << (k.log_N - 1);
   qm31 w = i < half ? ldq(wpow + i) : qneg(ldq(wpow + (i - half)));
   return qmul(k.offset, w);
-}
-
-__device__ __host__ __forceinline__ qm31 combined_key(const qm31* ac, uint32_t nk, const uint32_t* cols,
-                                                      const qm31* row) {
-  qm31 key = qzero();
-  for (uint32_t j = 0; j < nk; ++j) key = qadd(key, qmul(ac[j], row[cols[j]]));
-  return key;
-}
-
-// stark.zig:259-276 (denominator-cleared LogUp constraint).
-__device__ __host__ __forceinline__ qm31 lookup_constraint(const QuotConsts& k, uint32_t r, const qm31* cur,
-                                                           const qm31* pre, const qm31& acc, const qm31& accn) {
-  const qm31 sel = cur[k.sel[r]], mult = cur[k.mult[r]];
-  const qm31 key = combined_key(k.ac, k.n_keys[r], k.keys[r], cur);
-  const qm31 tkey = combined_key(k.ac, k.n_keys[r], k.tabs[r], pre);
-  const qm31 dacc = qsub(accn, acc);
-  const qm31 lb = qsub(qmul(dacc, qsub(k.ar[r], key)), mult);
-  const qm31 tb = qadd(qmul(dacc, qsub(k.ar[r], tkey)), qone());
-  return qadd(qmul(sel, lb), qmul(qsub(qone(), sel), tb));
-}
-
-// Hc(x) (stark.zig:505-533): transitions x (x - w^(n-1)), cyclic LogUp and
-// selector-binarity constraints, boundary terms with Z_H(x) / (x - p_k).
-__device__ __host__ inline qm31 composition(const QuotConsts& k, const qm31& x, const qm31* cur, const qm31* next,
-                                            const qm31* pre, const qm31& zh) {
-  qm31 res[kMaxTrans];
-  air_eval(k.air, x, cur, next, res);
-  qm31 h = qzero();
-  const qm31 xl = qsub(x, k.last_point);
-  for (uint32_t t = 0; t < k.num_trans; ++t) h = qadd(h, qmul(k.alphas[t], qmul(res[t], xl)));
-  for (uint32_t r = 0; r < k.n_rel; ++r)
-    h = qadd(h, qmul(k.alphas[k.num_trans + r], lookup_constraint(k, r, cur, pre, cur[k.m + r], next[k.m + r])));
-  for (uint32_t r = 0; r < k.n_rel; ++r) {
-    const qm31 sel = cur[k.sel[r]];
-    h = qadd(h, qmul(k.alphas[k.num_trans + k.n_rel + r], qmul(sel, qsub(qone(), sel))));
-  }
-  for (uint32_t b = 0; b < k.total_bound; ++b) {
-    const qm31 term = qmul(qmul(qsub(cur[k.b_col[b]], k.b_val[b]), zh), qinv(qsub(x, k.b_pt[b])));
-    h = qadd(h, qmul(k.betas[b], term));
-  }
-  return h;
 }
 
 // cw: codewords of all columns ([pre | main | acc]), N each.
@@ -638,6 +581,39 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   }
   ZS_CUDA(cudaStreamSynchronize(st));
   return proof.out;
+}
+
+// The commitment of columns alone (stark.zig:397-414): interpolate each column on
+// H, evaluate on D, one Merkle tree of hashQM31 leaves per column; returns the roots
+// as a wire []Digest (u64 count, then 32 bytes per column).
+std::vector<uint8_t> commit_columns(const uint8_t* cols_b, size_t cols_len, unsigned trace_log, unsigned log_blowup,
+                                    cudaStream_t st) {
+  const auto cols = read_columns(cols_b, cols_len);
+  const unsigned lN = trace_log + log_blowup;
+  if (lN > 26) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 26");
+  const uint32_t n = 1u << trace_log, N = 1u << lN, C = (uint32_t)cols.size();
+  for (auto& c : cols)
+    if (c.size() != n) throw Error(ZS_EMALFORMED, "column length is not 2^trace_log");
+  WireWriter out;
+  out.u64(C);
+  if (C == 0) return out.out;
+  NttTables small(trace_log, st), big(lN, st);
+  DevBuf<qm31> offset_pows(n, st);
+  qm31_powers(q_fri_offset(), offset_pows.p, n, st);
+  DevBuf<qm31> vals((size_t)C * n, st), coeffs((size_t)C * n, st), cw((size_t)C * N, st);
+  {
+    std::vector<qm31> host((size_t)C * n);
+    for (uint32_t j = 0; j < C; ++j) std::copy(cols[j].begin(), cols[j].end(), host.begin() + (size_t)j * n);
+    ZS_CUDA(cudaMemcpyAsync(vals.p, host.data(), host.size() * sizeof(qm31), cudaMemcpyHostToDevice, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+  }
+  lde_qm31(vals.p, n, coeffs.p, n, cw.p, N, C, small, big, offset_pows.p, st);
+  OwnedTree tree(lN, st);
+  for (uint32_t j = 0; j < C; ++j) {
+    build_qm31_tree(cw.p + (size_t)j * N, tree.t, st);
+    out.digest(root_of(tree.t, st));
+  }
+  return out.out;
 }
 
 }  // namespace zs

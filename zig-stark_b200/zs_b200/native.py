@@ -286,3 +286,42 @@ def prove(air_id, params, public_inputs, trace, preprocessed=b"", channel_sep=b"
     data = ctypes.string_at(out.value, n.value)
     L.zs_free(HOST, out, n.value)
     return data
+
+
+def verify(air_id, params, public_inputs, proof, channel_sep=b""):
+    """GenericStark(Air).verify (zs_m31_verify, host-side); returns True / False."""
+    if not isinstance(params, (bytes, bytearray)):
+        params = params.encode()
+    L = _bind_prove()
+    if not getattr(L, "_verify_bound", False):
+        L.zs_m31_verify.argtypes = [HostAllocator, ctypes.c_uint32] + [ctypes.c_char_p, ctypes.c_size_t] * 4 + \
+            [ctypes.POINTER(ctypes.c_int)]
+        L._verify_bound = True
+    ok = ctypes.c_int()
+    check(L.zs_m31_verify(HOST, air_id, params, len(params), public_inputs, len(public_inputs), proof, len(proof),
+                          channel_sep, len(channel_sep), ctypes.byref(ok)), "zs_m31_verify")
+    return bool(ok.value)
+
+
+def commit_columns(columns, trace_log, log_blowup):
+    """Per-column commitment roots (zs_m31_commit_columns); columns: wire bytes or a
+    list of (2^trace_log, 4) uint32 arrays. Returns a list of 32-byte roots."""
+    from . import wire
+    if not isinstance(columns, (bytes, bytearray)):
+        columns = wire.columns(columns)
+    L = _bind_prove()
+    if not getattr(L, "_commit_bound", False):
+        L.zs_m31_commit_columns.argtypes = [HostAllocator, ctypes.c_uint8, ctypes.c_uint8, ctypes.c_char_p,
+                                            ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p),
+                                            ctypes.POINTER(ctypes.c_size_t)]
+        L._commit_bound = True
+    out = ctypes.c_void_p()
+    n = ctypes.c_size_t()
+    check(L.zs_m31_commit_columns(HOST, trace_log, log_blowup, columns, len(columns), ctypes.byref(out),
+                                  ctypes.byref(n)), "zs_m31_commit_columns")
+    data = ctypes.string_at(out.value, n.value)
+    L.zs_free(HOST, out, n.value)
+    r = wire.Reader(data)
+    roots = r.digests()
+    r.end()
+    return roots
