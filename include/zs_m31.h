@@ -40,7 +40,10 @@ typedef struct {
  *   ZS_AIR_AND_TABLE       AndTableAir, stark.zig:1048-1131     PI {}
  *   ZS_AIR_MULTIPLICITY    MultiplicityAir, stark.zig:1139-1216 PI {}
  *   ZS_AIR_RESCUE_EXAMPLE  examples/rescue (8 rows)             PI {initial: [4]QM31, final: [4]QM31}
- *   ZS_AIR_LINEAR_EXAMPLE  examples/ml_linear (8 rows)          PI {x: []QM31, claimed_y: QM31} */
+ *   ZS_AIR_LINEAR_EXAMPLE  examples/ml_linear (8 rows)          PI {x: []QM31, claimed_y: QM31}
+ *   ZS_AIR_RESCUE_STACKED  the rescue example's permutation, 8 rows each, stacked to
+ *                          any 2^k >= 8 rows with square/cube helper columns (12
+ *                          columns, degree 2(n-1) + n/8)    PI {initial: [4]QM31, final: [4]QM31} */
 enum {
     ZS_AIR_FIB = 0,
     ZS_AIR_SEEDED_FIB = 1,
@@ -48,7 +51,8 @@ enum {
     ZS_AIR_AND_TABLE = 3,
     ZS_AIR_MULTIPLICITY = 4,
     ZS_AIR_RESCUE_EXAMPLE = 5,
-    ZS_AIR_LINEAR_EXAMPLE = 6
+    ZS_AIR_LINEAR_EXAMPLE = 6,
+    ZS_AIR_RESCUE_STACKED = 7
 };
 
 /* ---- prover ------------------------------------------------------------------

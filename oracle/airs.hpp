@@ -37,6 +37,7 @@ enum AirId : uint32_t {
   AIR_MULTIPLICITY = 4,
   AIR_RESCUE_EXAMPLE = 5,
   AIR_LINEAR_EXAMPLE = 6,
+  AIR_RESCUE_STACKED = 7,
 };
 
 struct Air {
@@ -210,6 +211,74 @@ struct LinearExampleAir : Air {
   }
 };
 
+// Independent Rescue permutations (the example's round: x^5 sbox, circulant MDS
+// (2,3,1,1), the example's LCG round constants) stacked 8 rows per permutation.
+// Columns s_0..s_3 (state), q_j = s_j^2 and t_j = q_j s_j, so s^5 = t q and every
+// constraint has degree 2 in the columns:
+//   C_j     = Z(x) * (next.s_j - sum_l MDS[j][l] * t_l * q_l - rc_j(x))   j < 4
+//   C_{4+j} = q_j - s_j^2,   C_{8+j} = t_j - q_j s_j
+// with y = x^(n/8) (so y = w8^(r mod 8) on row r), Z(x) = y - w8^7 switching the
+// round off on the last row of every permutation, and rc_j(x) = P_j(y), P_j the
+// degree-<8 interpolant of the round constants rc[t][j] (rc[7][j] = 0) on <w8>.
+// maxConstraintDegree = 2(n-1) + n/8, so at blowup 4 the FRI code keeps rate 1/2.
+// Boundaries: the first permutation's input and the last permutation's output.
+// PublicInputs {initial: [4]QM31, final: [4]QM31}.
+struct RescueStackedAir : Air {
+  QM31 initial[4], final_[4];
+  std::vector<QM31> P[4];  // P_j coefficients
+  QM31 w8_7;
+  mutable size_t trace_n = 8;
+  RescueStackedAir(const QM31* init, const QM31* fin) {
+    num_columns = 12;
+    num_transitions = 12;
+    num_boundary = 8;
+    for (size_t j = 0; j < 4; ++j) {
+      initial[j] = init[j];
+      final_[j] = fin[j];
+    }
+    QM31 rc[7][4];
+    RescueExampleAir::roundConstants(rc);
+    QM31 w8 = QM31::primitiveRootOfUnity(3);
+    std::vector<QM31> h(8);
+    QM31 acc = QM31::one();
+    for (size_t t = 0; t < 8; ++t) {
+      h[t] = acc;
+      acc = acc.mul(w8);
+    }
+    w8_7 = h[7];
+    for (size_t j = 0; j < 4; ++j) {
+      std::vector<QM31> ys(8);
+      for (size_t t = 0; t < 8; ++t) ys[t] = t < 7 ? rc[t][j] : QM31::zero();
+      P[j] = interpolateLagrange(h, ys);
+    }
+  }
+  void evalTransition(const QM31& x, const QM31* cur, const QM31* next, QM31* out) const override {
+    // y = x^(n/8); n is set by checkTraceLen before any evaluation
+    QM31 y = x.pow(trace_n / 8);
+    QM31 z = y.sub(w8_7);
+    for (size_t j = 0; j < 4; ++j) {
+      QM31 expect = QM31::zero();
+      for (size_t l = 0; l < 4; ++l)
+        expect = expect.add(cur[8 + l].mul(cur[4 + l]).mul(QM31::fromU32(RescueExampleAir::MDS[j][l])));
+      expect = expect.add(evalHorner(P[j], y));
+      out[j] = z.mul(next[j].sub(expect));
+      out[4 + j] = cur[4 + j].sub(cur[j].mul(cur[j]));
+      out[8 + j] = cur[8 + j].sub(cur[4 + j].mul(cur[j]));
+    }
+  }
+  size_t maxConstraintDegree(size_t n) const override { return 2 * (n - 1) + n / 8; }
+  void boundaryAssertions(size_t n, BoundaryAssertion* out) const override {
+    for (size_t j = 0; j < 4; ++j) {
+      out[j] = {j, 0, initial[j]};
+      out[4 + j] = {j, n - 1, final_[j]};
+    }
+  }
+  void checkTraceLen(size_t n) const override {
+    if (n < 8) throw WireError("stacked rescue AIR needs at least 8 rows", -2);
+    trace_n = n;
+  }
+};
+
 // Builds the AIR for `air_id` from the wire encoding of its PublicInputs.
 inline std::unique_ptr<Air> makeAir(uint32_t air_id, const uint8_t* pi, size_t pi_len) {
   Reader r(pi, pi_len);
@@ -245,6 +314,13 @@ inline std::unique_ptr<Air> makeAir(uint32_t air_id, const uint8_t* pi, size_t p
       std::vector<QM31> xs = r.qm31s();
       QM31 y = r.qm31();
       air = std::make_unique<LinearExampleAir>(std::move(xs), y);
+      break;
+    }
+    case AIR_RESCUE_STACKED: {
+      QM31 init[4], fin[4];
+      for (auto& v : init) v = r.qm31();
+      for (auto& v : fin) v = r.qm31();
+      air = std::make_unique<RescueStackedAir>(init, fin);
       break;
     }
     default:

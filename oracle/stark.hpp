@@ -219,10 +219,13 @@ struct Stark {
     std::vector<QM31> q(N);
     {
       QM31 last_point = h_points[n - 1];
-      std::vector<QM31> cur(m_total), nxt(m_total), rp(n_pre), inv_dp(total_bound);
       std::vector<QM31> pks(total_bound);
       for (size_t k = 0; k < total_bound; ++k) pks[k] = w.pow(bnd[k].step);
-      for (size_t i = 0; i < N; ++i) {
+      // every point is independent; the loop body is the reference's per point
+#pragma omp parallel for schedule(static)
+      for (long ii = 0; ii < (long)N; ++ii) {
+        const size_t i = (size_t)ii;
+        std::vector<QM31> cur(m_total), nxt(m_total), rp(n_pre), inv_dp(total_bound);
         QM31 zh = d_points[i].pow(n).sub(QM31::one());
         QM31 inv_zh = zh.inv();
         for (size_t j = 0; j < m_total; ++j) {
@@ -254,7 +257,9 @@ struct Stark {
 
     // stark.zig:577-588 DEEP codeword
     std::vector<QM31> g(N);
-    for (size_t i = 0; i < N; ++i) {
+#pragma omp parallel for schedule(static)
+    for (long ii = 0; ii < (long)N; ++ii) {
+      const size_t i = (size_t)ii;
       QM31 inv_dz = d_points[i].sub(z).inv();
       QM31 gv = QM31::zero();
       for (size_t j = 0; j < m_total; ++j) {
@@ -320,6 +325,7 @@ struct Stark {
   // stark.zig:660-784.
   bool verify(const StarkParams& params, const StarkProof& proof, Channel& ch) const {
     const size_t n = params.traceLen(), N = params.domainLen(), shift = params.shift();
+    air.checkTraceLen(n);
     if (proof.trace_roots.size() != m) return false;
     if (proof.deep_evals.size() != n_deep) return false;
     if (n_pre > 0 && (!proof.preprocessed_roots || proof.preprocessed_roots->size() != n_pre)) return false;

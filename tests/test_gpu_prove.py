@@ -101,3 +101,15 @@ def test_gpu_proofs_verify_with_library_verifier(orc):
     params = wire.StarkParams(10, 2, 16, 3)
     proof = native.prove(wl.AIR_SEEDED_FIB, params, pi, tr, b"", b"lib")
     assert native.verify(wl.AIR_SEEDED_FIB, params, pi, proof, b"lib")
+
+
+@pytest.mark.parametrize("trace_log", [3, 6, 10, 14])
+def test_rescue_stacked(orc, trace_log):
+    tr, pi = wl.rescue_stacked(trace_log)
+    _check(orc, wl.AIR_RESCUE_STACKED, wire.StarkParams(trace_log, 2, 16, 3), pi, tr, sep=b"zig-stark:rescue:example")
+
+
+def test_rescue_stacked_full_size(orc):
+    """2^18 rows of stacked Rescue permutations (2^15 of them) at blowup 4."""
+    tr, pi = wl.rescue_stacked(18)
+    _check(orc, wl.AIR_RESCUE_STACKED, wire.StarkParams(18, 2, 16, 3), pi, tr, sep=b"zig-stark:rescue:example")

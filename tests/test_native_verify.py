@@ -78,3 +78,13 @@ def test_malformed(orc):
     with pytest.raises(native.ZsError) as e:
         native.verify(wl.AIR_FIB, params, pi[:-1], proof, b"v")
     assert e.value.code == -2
+
+
+def test_rescue_stacked(orc):
+    tr, pi = wl.rescue_stacked(6)
+    params = wire.StarkParams(6, 2, 16, 3)
+    proof = _proof(orc, wl.AIR_RESCUE_STACKED, params, pi, tr)
+    assert native.verify(wl.AIR_RESCUE_STACKED, params, pi, proof, b"v")
+    bad = bytearray(pi)
+    bad[70] ^= 1
+    assert not native.verify(wl.AIR_RESCUE_STACKED, params, bytes(bad), proof, b"v")

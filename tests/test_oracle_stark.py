@@ -230,3 +230,44 @@ def test_malformed_inputs_rejected(orc):
     _, pi, proof = _fib(orc, 4, 3, 12, b"x", mode=1)
     assert not orc.verify(wl.AIR_FIB, params.encode(), pi, proof + b"\x00", b"x")
     assert not orc.verify(wl.AIR_FIB, params.encode(), pi, proof[:-1], b"x")
+
+
+@pytest.mark.parametrize("trace_log,log_blowup", [(3, 2), (5, 2), (6, 3), (7, 2)])
+def test_rescue_stacked_modes_and_verify(orc, trace_log, log_blowup):
+    """The stacked Rescue AIR: NTT mode equals the reference interpolation, the proof
+    verifies, and a forged final state is rejected."""
+    tr, pi = wl.rescue_stacked(trace_log)
+    # the example's per-permutation rounds hold in the generated trace
+    params = wire.StarkParams(trace_log, log_blowup, 16, 3)
+    a = orc.prove(wl.AIR_RESCUE_STACKED, params.encode(), pi, b"", wire.columns(tr), b"rs", mode=0)
+    b = orc.prove(wl.AIR_RESCUE_STACKED, params.encode(), pi, b"", wire.columns(tr), b"rs", mode=1)
+    assert a == b
+    assert orc.verify(wl.AIR_RESCUE_STACKED, params.encode(), pi, a, b"rs")
+    bad = bytearray(pi)
+    bad[64] = (bad[64] + 1) % 256
+    assert not orc.verify(wl.AIR_RESCUE_STACKED, params.encode(), bytes(bad), a, b"rs")
+
+
+def test_rescue_stacked_rejects_broken_round(orc):
+    tr, pi = wl.rescue_stacked(5)
+    tr[0] = tr[0].copy()
+    tr[0][3, 0] = (int(tr[0][3, 0]) + 1) % P  # row 3 is inside a permutation
+    params = wire.StarkParams(5, 2, 16, 3)
+    proof = orc.prove(wl.AIR_RESCUE_STACKED, params.encode(), pi, b"", wire.columns(tr), b"rs", mode=1)
+    assert not orc.verify(wl.AIR_RESCUE_STACKED, params.encode(), pi, proof, b"rs")
+
+
+def test_rescue_stacked_needs_blowup_4(orc):
+    # degree 2(n-1) + n/8 does not fit a domain without blowup: the FRI sizing check fails
+    tr, pi = wl.rescue_stacked(5)
+    with pytest.raises(RuntimeError, match="-4"):
+        orc.prove(wl.AIR_RESCUE_STACKED, wire.StarkParams(5, 0, 16, 3).encode(), pi, b"", wire.columns(tr), b"x")
+
+
+def test_rescue_stacked_first_permutation_matches_example():
+    """Rows 0..7 of the stacked trace are the example's permutation from that input."""
+    tr, _ = wl.rescue_stacked(4)
+    init = [tuple(int(x) for x in tr[j][0]) for j in range(4)]
+    ex, _ = wl.rescue_example(init)
+    for j in range(4):
+        assert np.array_equal(tr[j][:8], ex[j])

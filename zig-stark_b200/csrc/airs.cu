@@ -45,6 +45,7 @@ void AirInfo::boundary(uint64_t n, std::vector<Boundary>& out) const {
       out.push_back({0, n - 1, pi[2]});
       break;
     case AIR_RESCUE_EXAMPLE:  // main.zig:125-130
+    case AIR_RESCUE_STACKED:  // first permutation's input, last permutation's output
       for (uint32_t j = 0; j < 4; ++j) out.push_back({j, 0, pi[j]});
       for (uint32_t j = 0; j < 4; ++j) out.push_back({j, n - 1, pi[4 + j]});
       break;
@@ -87,6 +88,22 @@ AirInfo make_air(uint32_t air_id, const uint8_t* pi_bytes, size_t pi_len) {
       qm31 rc[7][4];
       rescue_round_constants(rc);
       const std::vector<qm31> h = subgroup_points(3);
+      a.consts.poly_len = 8;
+      for (int j = 0; j < 4; ++j) {
+        std::vector<qm31> ys(8);
+        for (int k = 0; k < 8; ++k) ys[k] = k < 7 ? rc[k][j] : qzero();
+        const std::vector<qm31> c = interpolate_small(h, ys);
+        for (int k = 0; k < 8; ++k) a.consts.poly[j][k] = c[k];
+      }
+      break;
+    }
+    case AIR_RESCUE_STACKED: {
+      a.m = 12, a.num_trans = 12, a.num_bound = 8, a.dc_mul = 2, a.dc_plus_n8 = true;
+      for (int i = 0; i < 8; ++i) a.pi.push_back(r.q());
+      qm31 rc[7][4];
+      rescue_round_constants(rc);
+      const std::vector<qm31> h = subgroup_points(3);
+      a.consts.w8_7 = h[7];
       a.consts.poly_len = 8;
       for (int j = 0; j < 4; ++j) {
         std::vector<qm31> ys(8);

@@ -22,7 +22,8 @@ enum AirIdInternal : uint32_t {
   AIR_MULTIPLICITY = 4,
   AIR_RESCUE_EXAMPLE = 5,
   AIR_LINEAR_EXAMPLE = 6,
-  AIR_COUNT = 7,
+  AIR_RESCUE_STACKED = 7,
+  AIR_COUNT = 8,
 };
 
 constexpr unsigned kMaxCols = 16;      // main + accumulator columns
@@ -36,7 +37,10 @@ constexpr unsigned kMaxKey = 4;
 struct AirConsts {
   uint32_t id;
   uint32_t poly_len;
-  qm31 poly[4][8];  // rescue: rc_poly[j] (main.zig:87-111); linear: inc (main.zig:59-81)
+  qm31 poly[4][8];  // rescue: rc_poly[j] (main.zig:87-111); linear: inc (main.zig:59-81);
+                    // stacked rescue: P_j, the periodic round constants on <w8>
+  qm31 w8_7;        // stacked rescue: w8^7, the row phase whose round is switched off
+  uint64_t n_div8;  // stacked rescue: n / 8
 };
 
 // Rescue example MDS matrix (examples/rescue/src/main.zig:19-25): circulant with first
@@ -72,6 +76,23 @@ ZS_HD void air_eval(const AirConsts& k, const qm31& x, const qm31* cur, const qm
         out[j] = qsub(next[j], expect);
       }
       break;
+    case AIR_RESCUE_STACKED: {
+      // Permutations of 8 rows; s_j = cur[j], q_j = cur[4 + j] = s_j^2 and
+      // t_j = cur[8 + j] = q_j s_j, so the round s^5 = t q has degree 2.
+      // y = x^(n/8) is w8^(r mod 8) on row r; the factor y - w8^7 switches the round
+      // off on each permutation's last row, and the round constants are P_j(y).
+      const qm31 y = qpow(x, k.n_div8);
+      const qm31 z = qsub(y, k.w8_7);
+      for (int j = 0; j < 4; ++j) {
+        qm31 expect = qzero();
+        for (int l = 0; l < 4; ++l) expect = qadd(expect, qmul_m(qmul(cur[8 + l], cur[4 + l]), rescue_mds(j, l)));
+        expect = qadd(expect, horner(k.poly[j], 8, y));
+        out[j] = qmul(z, qsub(next[j], expect));
+        out[4 + j] = qsub(cur[4 + j], qmul(cur[j], cur[j]));
+        out[8 + j] = qsub(cur[8 + j], qmul(cur[4 + j], cur[j]));
+      }
+      break;
+    }
     case AIR_LINEAR_EXAMPLE:  // examples/ml_linear/src/main.zig:84-87
       out[0] = qsub(qsub(next[0], cur[0]), horner(k.poly[0], k.poly_len, x));
       break;
@@ -93,13 +114,14 @@ struct AirInfo {
   uint32_t fixed_n = 0;  // 0 = any trace length
   uint32_t sel[kMaxRel] = {}, mult[kMaxRel] = {};
   uint32_t n_keys[kMaxRel] = {}, keys[kMaxRel][kMaxKey] = {}, tabs[kMaxRel][kMaxKey] = {};
-  uint64_t dc_mul = 1;  // maxConstraintDegree(n) = dc_mul * (n - 1)
+  uint64_t dc_mul = 1;  // maxConstraintDegree(n) = dc_mul * (n - 1) (+ n/8 if dc_plus_n8)
+  bool dc_plus_n8 = false;
   std::vector<qm31> pi;  // public inputs (QM31 fields in declaration order)
   std::vector<qm31> x_inputs;  // linear example: public x
   AirConsts consts{};
 
   uint64_t max_constraint_degree(uint64_t n) const {  // stark.zig:217-221 incl. LogUp padding
-    uint64_t d = dc_mul * (n - 1);
+    uint64_t d = dc_mul * (n - 1) + (dc_plus_n8 ? n / 8 : 0);
     if (n_rel > 0 && 3 * (n - 1) > d) d = 3 * (n - 1);
     return d;
   }

@@ -246,6 +246,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   if (lN > 26 || lb > 3) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 26 or log_blowup above 3");
   const uint32_t n = 1u << tl, N = 1u << lN, shift = 1u << lb;
   if (air.fixed_n && n != air.fixed_n) throw Error(ZS_EMALFORMED, "the AIR is defined for a fixed trace length");
+  if (air.id == AIR_RESCUE_STACKED && n < 8) throw Error(ZS_EMALFORMED, "stacked rescue needs at least 8 rows");
   if (trace.size() != air.m || pre.size() != air.n_pre) throw Error(ZS_EMALFORMED, "column count mismatch");
   for (auto& c : trace)
     if (c.size() != n) throw Error(ZS_EMALFORMED, "column length mismatch");
@@ -314,6 +315,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   // ---- LogUp challenges and accumulators ---------------------------------------
   QuotConsts kc{};
   kc.air = air.consts;
+  kc.air.n_div8 = n / 8;
   kc.m = m, kc.m_total = m_total, kc.n_pre = n_pre, kc.num_trans = air.num_trans, kc.n_rel = n_rel;
   kc.total_bound = total_bound, kc.shift = shift, kc.log_N = lN, kc.log_blowup = lb;
   kc.offset = offset;

@@ -195,6 +195,8 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
   const uint32_t total_bound = air.num_bound + n_rel;
   if (m_total > kMaxCols || air.num_trans > kMaxTrans || total_bound > kMaxBound || n_pre > kMaxPre)
     throw Error(ZS_EGENERIC, "AIR exceeds the compiled-in limits");
+  if (air.fixed_n && n != air.fixed_n) throw Error(ZS_EMALFORMED, "the AIR is defined for a fixed trace length");
+  if (air.id == AIR_RESCUE_STACKED && n < 8) throw Error(ZS_EMALFORMED, "stacked rescue needs at least 8 rows");
   if (p.trace_roots.size() != m || p.deep.size() != n_deep) return false;
   if (n_pre > 0 && (!p.has_pre || p.pre_roots.size() != n_pre)) return false;
   if (n_rel > 0 && (!p.has_acc || p.acc_roots.size() != n_rel)) return false;
@@ -219,6 +221,7 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
   for (auto& d : p.trace_roots) ch.absorb(d);
   QuotConsts kc{};
   kc.air = air.consts;
+  kc.air.n_div8 = n / 8;
   kc.m = m, kc.m_total = m_total, kc.n_pre = n_pre, kc.num_trans = air.num_trans, kc.n_rel = n_rel;
   kc.total_bound = total_bound;
   kc.last_point = qpow(w, n - 1);

@@ -243,3 +243,47 @@ def linear_example(x=None):
         col.append(acc)
     pi = wire.u64(8) + b"".join(wire.qm31(v) for v in x) + wire.qm31(acc)
     return [np.array(col, dtype=np.uint32)], pi
+
+
+AIR_RESCUE_STACKED = 7
+SEED_RESCUE = 0x5EED0005
+
+
+def _m31_pow5(v):
+    v = v.astype(np.uint64)
+    v2 = v * v % P
+    return v2 * v2 % P * v % P
+
+
+def rescue_stacked(trace_log, seed=SEED_RESCUE):
+    """Independent Rescue permutations (the example's 7 rounds, 8 rows each) stacked to
+    2^trace_log rows; initial states uniform M31 from `seed`. Columns s_0..s_3,
+    q_j = s_j^2 and t_j = q_j s_j. Returns (trace, public_inputs) for AIR_RESCUE_STACKED with
+    PublicInputs {initial: first permutation's input, final: last permutation's output}."""
+    n = 1 << trace_log
+    if n < 8:
+        raise ValueError("stacked rescue needs at least 8 rows")
+    perms = n // 8
+    rc = rescue_round_constants()
+    state = uniform_m31(seed, 4 * perms).reshape(perms, 4).astype(np.uint64)
+    s = np.zeros((perms, 8, 4), dtype=np.uint64)
+    for t in range(8):
+        s[:, t, :] = state
+        if t < 7:
+            boxed = _m31_pow5(state)
+            new = np.zeros_like(state)
+            for j in range(4):
+                acc = np.zeros(perms, dtype=np.uint64)
+                for l in range(4):
+                    acc = (acc + boxed[:, l] * RESCUE_MDS[j][l]) % P
+                new[:, j] = (acc + rc[t][j][0]) % P
+            state = new
+    flat = s.reshape(n, 4)
+    cols = [wire.m31_column_as_qm31(flat[:, j]) for j in range(4)]
+    sq = flat * flat % P
+    cols += [wire.m31_column_as_qm31(sq[:, j]) for j in range(4)]
+    cols += [wire.m31_column_as_qm31(sq[:, j] * flat[:, j] % P) for j in range(4)]
+    initial = [(int(flat[0, j]), 0, 0, 0) for j in range(4)]
+    final = [(int(flat[n - 1, j]), 0, 0, 0) for j in range(4)]
+    pi = b"".join(wire.qm31(v) for v in initial) + b"".join(wire.qm31(v) for v in final)
+    return cols, pi
