@@ -73,6 +73,51 @@ int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t *par
                      size_t preprocessed_len, const uint8_t *trace, size_t trace_len, const uint8_t *channel_sep,
                      size_t channel_sep_len, uint8_t **out_proof, size_t *out_len);
 
+/* ---- batched and served proving ---------------------------------------------
+ * One proof job: the arguments of zs_m31_prove. */
+typedef struct {
+    uint32_t air_id;
+    const uint8_t *params;
+    size_t params_len;
+    const uint8_t *public_inputs;
+    size_t public_inputs_len;
+    const uint8_t *preprocessed;
+    size_t preprocessed_len;
+    const uint8_t *trace;
+    size_t trace_len;
+    const uint8_t *channel_sep;
+    size_t channel_sep_len;
+} zs_m31_job;
+
+/* A finished job: status 0 and a proof allocated with the caller's allocator
+ * (release with zs_free), or a negative code; status 1 = still pending (poll). */
+typedef struct {
+    uint8_t *proof;
+    size_t len;
+    int32_t status;
+} zs_m31_result;
+
+/* Proves n_jobs independent traces with `concurrency` workers, each with its own
+ * CUDA stream and transcript, so the device interleaves the proofs' kernels.
+ * Admission keeps the estimated device footprint of the proofs in flight under
+ * hbm_budget_bytes (0 = 70 % of the free device memory). results[i] is jobs[i]'s
+ * proof, byte-identical to zs_m31_prove on the same job. No counterpart in the
+ * reference (its prover is single-threaded and proves one trace per call). */
+int32_t zs_m31_prove_batch(zs_host_allocator host, size_t n_jobs, const zs_m31_job *jobs, uint32_t concurrency,
+                           uint64_t hbm_budget_bytes, zs_m31_result *results);
+
+/* A proof server: requests are admitted as workers and device memory free up
+ * (continuous batching), their device work overlaps, and each request's latency
+ * (submit to done) is recorded. submit copies the job's buffers. poll returns the
+ * result (status 1 while pending; wait != 0 blocks until done) and the latency in
+ * milliseconds; a finished ticket is released by the poll that returns it. */
+typedef struct zs_m31_server zs_m31_server;
+int32_t zs_m31_server_create(uint32_t workers, uint64_t hbm_budget_bytes, zs_m31_server **out);
+void zs_m31_server_destroy(zs_m31_server *server);
+int32_t zs_m31_server_submit(zs_m31_server *server, const zs_m31_job *job, uint64_t *ticket);
+int32_t zs_m31_server_poll(zs_m31_server *server, uint64_t ticket, int32_t wait, zs_host_allocator host,
+                           zs_m31_result *result, double *latency_ms);
+
 /* Replaces GenericStark(Air).verify (src/m31/stark.zig:660-784); conventions of
  * zs_binius_verify (zig-capi.h:53-63). Sets *out_ok to 1 when the proof verifies and
  * 0 otherwise; returns 0, or a negative code when the inputs cannot be parsed. Runs

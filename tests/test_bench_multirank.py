@@ -16,7 +16,8 @@ world, rank, local = bench.dist_setup(None, backend="gloo")
 bench.barrier(world)
 m = bench.max_over_ranks(1.5 + rank, world)
 bench.barrier(world)
-print(json.dumps({{"rank": rank, "world": world, "max": m}}))
+with open(os.path.join({out!r}, "rank%d.json" % rank), "w") as f:
+    f.write(json.dumps({{"rank": rank, "world": world, "max": m}}))
 import torch.distributed as dist
 dist.destroy_process_group()
 """
@@ -32,14 +33,12 @@ def _free_port():
 
 def test_two_rank_max_and_barrier(tmp_path):
     script = tmp_path / "ranks.py"
-    script.write_text(SCRIPT.format(root=ROOT))
+    script.write_text(SCRIPT.format(root=ROOT, out=str(tmp_path)))
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
            "--master-addr", "127.0.0.1", "--master-port", str(_free_port()), str(script)]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=240, env={**os.environ, "OMP_NUM_THREADS": "1"})
     assert out.returncode == 0, out.stderr[-2000:]
-    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
-    assert len(lines) == 2
     import json
-    res = [json.loads(l) for l in lines]
+    res = [json.loads((tmp_path / f"rank{r}.json").read_text()) for r in range(2)]
     assert {r["rank"] for r in res} == {0, 1}
     assert all(r["world"] == 2 and r["max"] == 2.5 for r in res)

@@ -20,14 +20,14 @@ __global__ void k_fold_tables(qm31 w0inv, qm31* tabs) {
   tabs[k] = qpow(base, e);
 }
 
-FoldTables::FoldTables(unsigned d, cudaStream_t st) : dlog(d) {
+FoldTables::FoldTables(unsigned d, cudaStream_t s) : dlog(d), st(s) {
   if (dlog > 32) throw Error(ZS_EMALFORMED, "FRI domain log size above 32");
   ZS_CUDA(cudaMallocAsync(&tables, 3 * 2048 * sizeof(qm31), st));
   const qm31 w0 = q_root_of_unity(dlog);
   k_fold_tables<<<(3 * 2048 + 255) / 256, 256, 0, st>>>(qinv(w0), tables);
   ZS_CUDA(cudaGetLastError());
 }
-FoldTables::~FoldTables() { cudaFree(tables); }
+FoldTables::~FoldTables() { cudaFreeAsync(tables, st); }
 
 qm31 FoldTables::offset_inv(unsigned layer) const { return qinv(qpow(q_fri_offset(), (uint64_t)1 << layer)); }
 

@@ -10,6 +10,7 @@ namespace zs {
 struct FoldTables {
   unsigned dlog = 0;
   qm31* tables = nullptr;  // 3 * 2048 entries
+  cudaStream_t st = nullptr;  // freed in stream order
   explicit FoldTables(unsigned dlog, cudaStream_t st);
   ~FoldTables();
   FoldTables(const FoldTables&) = delete;

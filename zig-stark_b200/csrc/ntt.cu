@@ -33,7 +33,7 @@ void qm31_powers(qm31 x, qm31* pows, uint32_t count, cudaStream_t st) {
   ZS_CUDA(cudaGetLastError());
 }
 
-NttTables::NttTables(unsigned l, cudaStream_t st) : log_n(l) {
+NttTables::NttTables(unsigned l, cudaStream_t s) : log_n(l), st(s) {
   if (log_n > 30) throw Error(ZS_EMALFORMED, "NTT size above 2^30");
   const uint32_t half = log_n == 0 ? 1 : (1u << (log_n - 1));
   ZS_CUDA(cudaMallocAsync(&fwd, half * sizeof(qm31), st));
@@ -43,8 +43,8 @@ NttTables::NttTables(unsigned l, cudaStream_t st) : log_n(l) {
   qm31_powers(qinv(w), inv, half, st);
 }
 NttTables::~NttTables() {
-  cudaFree(fwd);
-  cudaFree(inv);
+  cudaFreeAsync(fwd, st);
+  cudaFreeAsync(inv, st);
 }
 
 // dst[bitrev(i)] = src[i], i < 2^logN.

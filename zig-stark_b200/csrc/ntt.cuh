@@ -12,6 +12,7 @@ struct NttTables {
   unsigned log_n = 0;
   qm31* fwd = nullptr;
   qm31* inv = nullptr;
+  cudaStream_t st = nullptr;  // freed in stream order, so concurrent provers never synchronize the device
   NttTables(unsigned log_n, cudaStream_t st);
   ~NttTables();
   NttTables(const NttTables&) = delete;

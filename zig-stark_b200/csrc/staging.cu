@@ -1,0 +1,241 @@
+// Pinned, double-buffered, multi-threaded host staging for uploads.
+#include <algorithm>
+#include <condition_variable>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "staging.cuh"
+
+namespace zs {
+
+namespace {
+
+constexpr size_t kChunk = (size_t)16 << 20;  // bytes per staging buffer
+constexpr size_t kSmall = (size_t)1 << 20;   // below this the driver's pageable path is as fast
+
+// A fork-join pool of host threads: run(n, f) calls f(0..n-1) spread over the pool
+// and the caller, and returns when every call has finished. A caller that finds the
+// pool busy runs its calls itself.
+class HostPool {
+ public:
+  static HostPool& get() {
+    static HostPool pool;
+    return pool;
+  }
+  size_t width() const { return threads_.size() + 1; }
+  void run(size_t n, const std::function<void(size_t)>& f) {
+    std::unique_lock<std::mutex> call(call_mu_, std::try_to_lock);
+    if (!call.owns_lock()) {  // the pool serves another caller: copy on this thread
+      for (size_t i = 0; i < n; ++i) f(i);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      task_ = &f;
+      n_ = n;
+      next_ = 0;
+      busy_ = threads_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return busy_ == 0; });
+    task_ = nullptr;
+  }
+  ~HostPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+      ++gen_;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+
+ private:
+  HostPool() {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned extra = std::min(7u, std::max(1u, hw / 2) - 1);  // up to half the cores
+    for (unsigned i = 0; i < extra; ++i) threads_.emplace_back([this] { loop(); });
+  }
+  void work() {
+    for (;;) {
+      size_t i;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (!task_ || next_ >= n_) return;
+        i = next_++;
+      }
+      (*task_)(i);
+    }
+  }
+  void loop() {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+        if (stop_) return;
+      }
+      work();
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        --busy_;
+      }
+      done_cv_.notify_all();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex call_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  const std::function<void(size_t)>* task_ = nullptr;
+  size_t n_ = 0, next_ = 0, busy_ = 0;
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
+
+// Two pinned upload buffers, each guarded by the event of the DMA that last read it.
+struct Stager {
+  void* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  uint64_t next = 0;  // alternates across calls too
+  bool ok = false;
+  Stager() {
+    ok = cudaHostAlloc(&buf[0], kChunk, cudaHostAllocDefault) == cudaSuccess &&
+         cudaHostAlloc(&buf[1], kChunk, cudaHostAllocDefault) == cudaSuccess &&
+         cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) == cudaSuccess;
+  }
+};
+
+// Bump-allocated pinned blocks; a region stays valid until the next reset.
+struct Arena {
+  std::vector<std::pair<uint8_t*, size_t>> blocks;  // (base, capacity)
+  size_t cur = 0, used = 0;
+  void reset() {
+    cur = 0;
+    used = 0;
+  }
+  uint8_t* take(size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    while (cur < blocks.size() && used + bytes > blocks[cur].second) ++cur, used = 0;
+    if (cur == blocks.size()) {
+      size_t cap = blocks.empty() ? ((size_t)1 << 20) : blocks.back().second * 2;
+      while (cap < bytes) cap *= 2;
+      void* p = nullptr;
+      ZS_CUDA(cudaHostAlloc(&p, cap, cudaHostAllocDefault));
+      blocks.emplace_back(static_cast<uint8_t*>(p), cap);
+      used = 0;
+    }
+    uint8_t* r = blocks[cur].first + used;
+    used += bytes;
+    return r;
+  }
+};
+
+struct Slot {
+  Stager stager;
+  Arena arena;
+};
+
+// Slots are created on demand and kept for the life of the process.
+class SlotBank {
+ public:
+  static SlotBank& get() {
+    static SlotBank* bank = new SlotBank();
+    return *bank;
+  }
+  Slot* take() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      if (!idle_.empty()) {
+        Slot* s = idle_.back();
+        idle_.pop_back();
+        return s;
+      }
+    }
+    return new Slot();
+  }
+  void give(Slot* s) {
+    std::lock_guard<std::mutex> lk(mu_);
+    idle_.push_back(s);
+  }
+
+ private:
+  std::mutex mu_;
+  std::vector<Slot*> idle_;
+};
+
+thread_local Slot* t_slot = nullptr;
+
+}  // namespace
+
+PinnedScope::PinnedScope(cudaStream_t st) : st_(st), slot_(SlotBank::get().take()), prev_(t_slot) {
+  Slot* s = static_cast<Slot*>(slot_);
+  s->arena.reset();
+  t_slot = s;
+}
+
+PinnedScope::~PinnedScope() {
+  cudaStreamSynchronize(st_);
+  t_slot = static_cast<Slot*>(prev_);
+  SlotBank::get().give(static_cast<Slot*>(slot_));
+}
+
+void h2d_small(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes == 0) return;
+  if (!t_slot) {
+    ZS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    return;
+  }
+  uint8_t* r = t_slot->arena.take(bytes);
+  std::memcpy(r, src, bytes);
+  ZS_CUDA(cudaMemcpyAsync(dst, r, bytes, cudaMemcpyHostToDevice, st));
+}
+
+void d2h_small(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes == 0) return;
+  if (!t_slot) {
+    ZS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  uint8_t* r = t_slot->arena.take(bytes);
+  ZS_CUDA(cudaMemcpyAsync(r, src, bytes, cudaMemcpyDeviceToHost, st));
+  ZS_CUDA(cudaStreamSynchronize(st));
+  std::memcpy(dst, r, bytes);
+}
+
+void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes == 0) return;
+  Stager* sg = (bytes < kSmall || !t_slot) ? nullptr : &t_slot->stager;
+  if (!sg || !sg->ok) {
+    ZS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    return;
+  }
+  HostPool& pool = HostPool::get();
+  const size_t parts = pool.width();
+  const uint8_t* s = static_cast<const uint8_t*>(src);
+  uint8_t* d = static_cast<uint8_t*>(dst);
+  for (size_t off = 0; off < bytes; off += kChunk) {
+    const size_t len = std::min(kChunk, bytes - off);
+    const int b = (int)(sg->next++ & 1);
+    ZS_CUDA(cudaEventSynchronize(sg->ev[b]));  // the DMA that last read this buffer is done
+    uint8_t* pin = static_cast<uint8_t*>(sg->buf[b]);
+    const size_t piece = ((len + parts - 1) / parts + 63) & ~(size_t)63;
+    pool.run(parts, [&](size_t i) {
+      const size_t a = std::min(len, i * piece), e = std::min(len, a + piece);
+      if (e > a) std::memcpy(pin + a, s + off + a, e - a);
+    });
+    ZS_CUDA(cudaMemcpyAsync(d + off, pin, len, cudaMemcpyHostToDevice, st));
+    ZS_CUDA(cudaEventRecord(sg->ev[b], st));
+  }
+}
+
+}  // namespace zs

@@ -13,6 +13,7 @@
 // All device arithmetic is exact, so every root, layer and proof byte equals the
 // reference's.
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "airs.cuh"
@@ -22,6 +23,7 @@
 #include "merkle.cuh"
 #include "ntt.cuh"
 #include "stark.cuh"
+#include "staging.cuh"
 
 namespace zs {
 
@@ -194,8 +196,7 @@ struct DevBuf {
 
 Digest root_of(const DeviceTree& t, cudaStream_t st) {
   Digest d;
-  ZS_CUDA(cudaMemcpyAsync(d.data(), t.root(), 32, cudaMemcpyDeviceToHost, st));
-  ZS_CUDA(cudaStreamSynchronize(st));
+  d2h_small(d.data(), t.root(), 32, st);
   return d;
 }
 
@@ -209,19 +210,76 @@ struct OwnedTree {
   ~OwnedTree() { cudaFreeAsync(t.words, st); }
 };
 
-std::vector<std::vector<qm31>> read_columns(const uint8_t* d, size_t n) {
-  std::vector<std::vector<qm31>> cols;
-  if (n == 0) return cols;
+// The columns of a wire []const []const QM31, located but not decoded: each element
+// is four little-endian u32 words, the device layout of a qm31, so a column's bytes
+// go to the device as they are and M31.fromBytes' reduction (m31.zig:97-100) runs
+// there (k_from_bytes).
+struct WireColumns {
+  std::vector<const uint8_t*> data;
+  std::vector<uint64_t> len;
+  size_t size() const { return data.size(); }
+};
+
+WireColumns locate_columns(const uint8_t* d, size_t n) {
+  WireColumns c;
+  if (n == 0) return c;
   WireReader r(d, n);
   const uint64_t m = r.len(8);
   for (uint64_t j = 0; j < m; ++j) {
     const uint64_t len = r.len(16);
-    std::vector<qm31> c(len);
-    for (auto& v : c) v = r.q();
-    cols.push_back(std::move(c));
+    c.data.push_back(r.take(16 * len));
+    c.len.push_back(len);
   }
   r.end();
-  return cols;
+  return c;
+}
+
+// Column data of the wire span -> canonical M31 words. Column j's element words
+// start 2 + 4n words after column j-1's (its u64 length prefix sits between them);
+// raw < 2^32 <= 2p + 2, so at most two subtractions reduce it.
+__global__ void k_from_wire(const uint32_t* __restrict__ raw, uint32_t* __restrict__ out, uint64_t col_words,
+                            uint64_t count) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint64_t j = i / col_words;
+  uint32_t v = raw[i + 2 * j];
+  v = v >= P ? v - P : v;
+  v = v >= P ? v - P : v;
+  out[i] = v;
+}
+
+// Copies the columns of `c` (each of n elements) to dst (column k at dst + k * n) and
+// reduces them: the span of the caller's buffer that holds all columns goes over in
+// one upload, and a kernel drops the length prefixes between the columns.
+void upload_columns(const WireColumns& c, qm31* dst, uint32_t n, cudaStream_t st) {
+  if (c.size() == 0) return;
+  const uint64_t col_words = (uint64_t)4 * n, count = col_words * c.size();
+  const size_t span = (size_t)(c.data.back() - c.data.front()) + (size_t)16 * n;
+  DevBuf<uint32_t> raw((span + 3) / 4, st);
+  upload_bytes(raw.p, c.data.front(), span, st);
+  k_from_wire<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(raw.p, reinterpret_cast<uint32_t*>(dst), col_words,
+                                                              count);
+  ZS_CUDA(cudaGetLastError());
+}
+
+// Freed blocks stay in the device's stream-ordered pool instead of going back to the
+// driver at every synchronization, so repeated proofs do not map their memory again.
+void retain_pool_memory() {
+  static std::mutex mu;
+  static uint64_t done = 0;
+  int dev = 0;
+  ZS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 64 && (done >> dev & 1)) return;
+  cudaMemPool_t pool;
+  ZS_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t keep = UINT64_MAX;
+  ZS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  // A block freed on one prover's stream is reused by another only once the free has
+  // completed: the pool never makes one proof's stream wait on another's.
+  int no = 0;
+  ZS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+  if (dev < 64) done |= 1ull << dev;
 }
 
 }  // namespace
@@ -240,18 +298,20 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     r.end();
   }
   const AirInfo air = make_air(air_id, pi, pi_len);
-  const auto pre = read_columns(pre_b, pre_len);
-  const auto trace = read_columns(trace_b, trace_len);
+  const WireColumns pre = locate_columns(pre_b, pre_len);
+  const WireColumns trace = locate_columns(trace_b, trace_len);
   const unsigned tl = sp.trace_log, lb = sp.log_blowup, lN = tl + lb;
   if (lN > 26 || lb > 3) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 26 or log_blowup above 3");
   const uint32_t n = 1u << tl, N = 1u << lN, shift = 1u << lb;
   if (air.fixed_n && n != air.fixed_n) throw Error(ZS_EMALFORMED, "the AIR is defined for a fixed trace length");
   if (air.id == AIR_RESCUE_STACKED && n < 8) throw Error(ZS_EMALFORMED, "stacked rescue needs at least 8 rows");
   if (trace.size() != air.m || pre.size() != air.n_pre) throw Error(ZS_EMALFORMED, "column count mismatch");
-  for (auto& c : trace)
-    if (c.size() != n) throw Error(ZS_EMALFORMED, "column length mismatch");
-  for (auto& c : pre)
-    if (c.size() != n) throw Error(ZS_EMALFORMED, "column length mismatch");
+  retain_pool_memory();
+  PinnedScope pinned(st);
+  for (uint64_t l : trace.len)
+    if (l != n) throw Error(ZS_EMALFORMED, "column length mismatch");
+  for (uint64_t l : pre.len)
+    if (l != n) throw Error(ZS_EMALFORMED, "column length mismatch");
   const uint32_t m = air.m, n_pre = air.n_pre, n_rel = air.n_rel, m_total = m + n_rel;
   const uint32_t n_trans_total = air.num_trans + 2 * n_rel, total_bound = air.num_bound + n_rel;
   const uint32_t n_deep = 2 * m_total + 1, reveal_len = 2 * m_total + 1 + n_pre;
@@ -283,13 +343,8 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   DevBuf<qm31> offset_pows(n, st);
   qm31_powers(offset, offset_pows.p, n, st);
   DevBuf<qm31> vals((size_t)ncol * n, st), coeffs((size_t)ncol * n, st), cw((size_t)ncol * N, st);
-  {
-    std::vector<qm31> host((size_t)(n_pre + m) * n);
-    for (uint32_t j = 0; j < n_pre; ++j) std::copy(pre[j].begin(), pre[j].end(), host.begin() + (size_t)j * n);
-    for (uint32_t j = 0; j < m; ++j) std::copy(trace[j].begin(), trace[j].end(), host.begin() + (size_t)(n_pre + j) * n);
-    ZS_CUDA(cudaMemcpyAsync(vals.p, host.data(), host.size() * sizeof(qm31), cudaMemcpyHostToDevice, st));
-    ZS_CUDA(cudaStreamSynchronize(st));
-  }
+  upload_columns(pre, vals.p, n, st);
+  upload_columns(trace, vals.p + (size_t)n_pre * n, n, st);
   lde_qm31(vals.p, n, coeffs.p, n, cw.p, N, n_pre + m, small, big, offset_pows.p, st);
 
   std::vector<std::unique_ptr<OwnedTree>> trees;
@@ -327,7 +382,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     for (uint32_t j = 0; j < air.n_keys[r]; ++j) kc.keys[r][j] = air.keys[r][j], kc.tabs[r][j] = air.tabs[r][j];
   }
   DevBuf<QuotConsts> d_kc(1, st);
-  ZS_CUDA(cudaMemcpyAsync(d_kc.p, &kc, sizeof(kc), cudaMemcpyHostToDevice, st));
+  h2d_small(d_kc.p, &kc, sizeof(kc), st);
   if (n_rel > 0) {
     DevBuf<qm31> contrib(n, st);
     const uint32_t nb = (n + 1023) / 1024;
@@ -387,7 +442,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
       acc = qmul(acc, wb);
     }
   }
-  ZS_CUDA(cudaMemcpyAsync(d_kc.p, &kc, sizeof(kc), cudaMemcpyHostToDevice, st));
+  h2d_small(d_kc.p, &kc, sizeof(kc), st);
   DevBuf<qm31> q(N, st);
   k_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_kc.p);
   ZS_CUDA(cudaGetLastError());
@@ -412,8 +467,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     k_eval_sum<<<(2 * ncol + 63) / 64, 64, 0, st>>>(partial.p, nblk, 2 * ncol, sums.p);
     ZS_CUDA(cudaGetLastError());
     std::vector<qm31> hs(2 * ncol);
-    ZS_CUDA(cudaMemcpyAsync(hs.data(), sums.p, hs.size() * sizeof(qm31), cudaMemcpyDeviceToHost, st));
-    ZS_CUDA(cudaStreamSynchronize(st));
+    d2h_small(hs.data(), sums.p, hs.size() * sizeof(qm31), st);
     for (uint32_t j = 0; j < m_total; ++j) {
       deep[j] = hs[n_pre + j];                  // f_j(z)
       deep[m_total + j] = hs[ncol + n_pre + j];  // f_j(w z)
@@ -434,7 +488,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   for (uint32_t j = 0; j < n_deep; ++j) dc.gammas[j] = ch.sample_q();
   for (uint32_t j = 0; j < 2 * m_total; ++j) dc.evals[j] = deep[j];
   DevBuf<DeepConsts> d_dc(1, st);
-  ZS_CUDA(cudaMemcpyAsync(d_dc.p, &dc, sizeof(dc), cudaMemcpyHostToDevice, st));
+  h2d_small(d_dc.p, &dc, sizeof(dc), st);
   std::vector<std::unique_ptr<DevBuf<qm31>>> layers;
   layers.push_back(std::make_unique<DevBuf<qm31>>(N, st));
   k_deep<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_dc.p, layers[0]->p);
@@ -457,8 +511,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   // points of layer L on the host (at most a few dozen values).
   const uint32_t rem = 1u << (fp.remainder_log - fp.log_blowup);
   std::vector<qm31> last(rem);
-  ZS_CUDA(cudaMemcpyAsync(last.data(), layers[L]->p, rem * sizeof(qm31), cudaMemcpyDeviceToHost, st));
-  ZS_CUDA(cudaStreamSynchronize(st));
+  d2h_small(last.data(), layers[L]->p, rem * sizeof(qm31), st);
   std::vector<qm31> xs(rem);
   {
     const qm31 wl = q_root_of_unity(lN - L);
@@ -519,11 +572,10 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   if (!reqs.empty()) {
     DevBuf<GatherReq> d_reqs(reqs.size(), st);
     DevBuf<uint32_t> d_out(off, st);
-    ZS_CUDA(cudaMemcpyAsync(d_reqs.p, reqs.data(), reqs.size() * sizeof(GatherReq), cudaMemcpyHostToDevice, st));
+    h2d_small(d_reqs.p, reqs.data(), reqs.size() * sizeof(GatherReq), st);
     k_gather<<<((uint32_t)reqs.size() + kT - 1) / kT, kT, 0, st>>>(d_reqs.p, (uint32_t)reqs.size(), d_out.p);
     ZS_CUDA(cudaGetLastError());
-    ZS_CUDA(cudaMemcpyAsync(gathered.data(), d_out.p, off * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    ZS_CUDA(cudaStreamSynchronize(st));
+    d2h_small(gathered.data(), d_out.p, off * sizeof(uint32_t), st);
   }
   size_t cursor = 0;
   auto next_value = [&]() {
@@ -590,12 +642,14 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
 // as a wire []Digest (u64 count, then 32 bytes per column).
 std::vector<uint8_t> commit_columns(const uint8_t* cols_b, size_t cols_len, unsigned trace_log, unsigned log_blowup,
                                     cudaStream_t st) {
-  const auto cols = read_columns(cols_b, cols_len);
+  const WireColumns cols = locate_columns(cols_b, cols_len);
   const unsigned lN = trace_log + log_blowup;
   if (lN > 26) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 26");
   const uint32_t n = 1u << trace_log, N = 1u << lN, C = (uint32_t)cols.size();
-  for (auto& c : cols)
-    if (c.size() != n) throw Error(ZS_EMALFORMED, "column length is not 2^trace_log");
+  for (uint64_t l : cols.len)
+    if (l != n) throw Error(ZS_EMALFORMED, "column length is not 2^trace_log");
+  retain_pool_memory();
+  PinnedScope pinned(st);
   WireWriter out;
   out.u64(C);
   if (C == 0) return out.out;
@@ -603,12 +657,7 @@ std::vector<uint8_t> commit_columns(const uint8_t* cols_b, size_t cols_len, unsi
   DevBuf<qm31> offset_pows(n, st);
   qm31_powers(q_fri_offset(), offset_pows.p, n, st);
   DevBuf<qm31> vals((size_t)C * n, st), coeffs((size_t)C * n, st), cw((size_t)C * N, st);
-  {
-    std::vector<qm31> host((size_t)C * n);
-    for (uint32_t j = 0; j < C; ++j) std::copy(cols[j].begin(), cols[j].end(), host.begin() + (size_t)j * n);
-    ZS_CUDA(cudaMemcpyAsync(vals.p, host.data(), host.size() * sizeof(qm31), cudaMemcpyHostToDevice, st));
-    ZS_CUDA(cudaStreamSynchronize(st));
-  }
+  upload_columns(cols, vals.p, n, st);
   lde_qm31(vals.p, n, coeffs.p, n, cw.p, N, C, small, big, offset_pows.p, st);
   OwnedTree tree(lN, st);
   for (uint32_t j = 0; j < C; ++j) {

@@ -325,3 +325,128 @@ def commit_columns(columns, trace_log, log_blowup):
     roots = r.digests()
     r.end()
     return roots
+
+
+# ---------------------------------------------------------------------------
+# batched and served proving (zs_m31_prove_batch, zs_m31_server_*)
+# ---------------------------------------------------------------------------
+
+class Job(ctypes.Structure):
+    """zs_m31_job: the arguments of one zs_m31_prove call."""
+    _fields_ = [("air_id", ctypes.c_uint32),
+                ("params", ctypes.c_char_p), ("params_len", ctypes.c_size_t),
+                ("public_inputs", ctypes.c_char_p), ("public_inputs_len", ctypes.c_size_t),
+                ("preprocessed", ctypes.c_char_p), ("preprocessed_len", ctypes.c_size_t),
+                ("trace", ctypes.c_char_p), ("trace_len", ctypes.c_size_t),
+                ("channel_sep", ctypes.c_char_p), ("channel_sep_len", ctypes.c_size_t)]
+
+
+class Result(ctypes.Structure):
+    """zs_m31_result: a proof in host memory and its status (1 = pending)."""
+    _fields_ = [("proof", ctypes.c_void_p), ("len", ctypes.c_size_t), ("status", ctypes.c_int32)]
+
+
+PENDING = 1
+
+
+def _job_bytes(air_id, params, public_inputs, trace, preprocessed=b"", channel_sep=b""):
+    from . import wire
+    if not isinstance(params, (bytes, bytearray)):
+        params = params.encode()
+    if not isinstance(trace, (bytes, bytearray)):
+        trace = wire.columns(trace)
+    if not isinstance(preprocessed, (bytes, bytearray)):
+        preprocessed = wire.columns(preprocessed)
+    return (int(air_id), bytes(params), bytes(public_inputs), bytes(preprocessed), bytes(trace), bytes(channel_sep))
+
+
+def _make_job(b):
+    air_id, params, pi, pre, trace, sep = b
+    return Job(air_id, params, len(params), pi, len(pi), pre, len(pre), trace, len(trace), sep, len(sep))
+
+
+def _bind_batch():
+    L = _bind_prove()
+    if not getattr(L, "_batch_bound", False):
+        L.zs_m31_prove_batch.argtypes = [HostAllocator, ctypes.c_size_t, ctypes.POINTER(Job), ctypes.c_uint32,
+                                         ctypes.c_uint64, ctypes.POINTER(Result)]
+        L.zs_m31_server_create.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]
+        L.zs_m31_server_destroy.argtypes = [ctypes.c_void_p]
+        L.zs_m31_server_destroy.restype = None
+        L.zs_m31_server_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(Job), ctypes.POINTER(ctypes.c_uint64)]
+        L.zs_m31_server_poll.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int32, HostAllocator,
+                                         ctypes.POINTER(Result), ctypes.POINTER(ctypes.c_double)]
+        L._batch_bound = True
+    return L
+
+
+def _take(L, res):
+    """Copies a finished result's proof out of the host allocator's buffer and frees it."""
+    if res.status != 0:
+        return None
+    data = ctypes.string_at(res.proof, res.len)
+    L.zs_free(HOST, res.proof, res.len)
+    return data
+
+
+def prove_batch(jobs, concurrency=8, hbm_budget=0):
+    """Proves independent traces together (zs_m31_prove_batch).
+
+    jobs: tuples or dicts of prove()'s arguments (air_id, params, public_inputs,
+    trace[, preprocessed[, channel_sep]]). Returns one entry per job: the proof bytes,
+    or the negative status code of a job that failed (the others still complete)."""
+    packed = [_job_bytes(**j) if isinstance(j, dict) else _job_bytes(*j) for j in jobs]
+    arr = (Job * max(len(packed), 1))(*[_make_job(b) for b in packed])
+    res = (Result * max(len(packed), 1))()
+    L = _bind_batch()
+    check(L.zs_m31_prove_batch(HOST, len(packed), arr, concurrency, hbm_budget, res), "zs_m31_prove_batch")
+    out = []
+    for i in range(len(packed)):
+        d = _take(L, res[i])
+        out.append(d if d is not None else int(res[i].status))
+    return out
+
+
+class Server:
+    """A proof server (zs_m31_server_*): submit() queues a request and returns a
+    ticket; poll(ticket) returns (proof bytes or negative status, latency_ms), or None
+    while the request is pending and wait is False."""
+
+    def __init__(self, workers=8, hbm_budget=0):
+        self._L = _bind_batch()
+        h = ctypes.c_void_p()
+        check(self._L.zs_m31_server_create(workers, hbm_budget, ctypes.byref(h)), "zs_m31_server_create")
+        self._h = h
+
+    def submit(self, air_id, params, public_inputs, trace, preprocessed=b"", channel_sep=b""):
+        job = _make_job(_job_bytes(air_id, params, public_inputs, trace, preprocessed, channel_sep))
+        t = ctypes.c_uint64()
+        check(self._L.zs_m31_server_submit(self._h, ctypes.byref(job), ctypes.byref(t)), "zs_m31_server_submit")
+        return t.value
+
+    def poll(self, ticket, wait=True):
+        res = Result()
+        lat = ctypes.c_double()
+        check(self._L.zs_m31_server_poll(self._h, ticket, 1 if wait else 0, HOST, ctypes.byref(res),
+                                         ctypes.byref(lat)), "zs_m31_server_poll")
+        if res.status == PENDING:
+            return None
+        d = _take(self._L, res)
+        return (d if d is not None else int(res.status)), lat.value
+
+    def close(self):
+        if self._h:
+            self._L.zs_m31_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -70,13 +70,27 @@ def qm31_add(a, b):
 # ---------------------------------------------------------------------------
 
 def fib_trace(n, a0=0, a1=1):
-    """FibAir.generateTrace (stark.zig:908-925) with configurable a_0, a_1 (M31)."""
-    a = np.zeros(n, dtype=np.uint64)
-    b = np.zeros(n, dtype=np.uint64)
-    x, y = a0 % P, a1 % P
-    for i in range(n):
-        a[i], b[i] = x, y
-        x, y = y, (x + y) % P
+    """FibAir.generateTrace (stark.zig:908-925) with configurable a_0, a_1 (M31).
+
+    Vectorised in blocks of B rows: with F the Fibonacci numbers (F(-1) = 1),
+    a_(j+t) = F(t-1) a_j + F(t) a_(j+1), so every block follows from its first two
+    values, and those follow from the previous block's by the same identity at t = B."""
+    x0, y0 = a0 % P, a1 % P
+    B = max(1, min(n, 1024))
+    F = np.zeros(B + 2, dtype=np.uint64)  # F[k] = F(k - 1), k = 0..B+1
+    F[0], F[1] = 1, 0
+    for k in range(2, B + 2):
+        F[k] = (F[k - 1] + F[k - 2]) % P
+    blocks = (n + B - 1) // B
+    xs = np.zeros(blocks, dtype=np.uint64)
+    ys = np.zeros(blocks, dtype=np.uint64)
+    x, y = x0, y0
+    fb_1, fb, fb1 = int(F[B]), int(F[B + 1]), int((F[B] + F[B + 1]) % P)  # F(B-1), F(B), F(B+1)
+    for k in range(blocks):
+        xs[k], ys[k] = x, y
+        x, y = (fb_1 * x + fb * y) % P, (fb * x + fb1 * y) % P
+    a = ((np.outer(xs, F[:B]) + np.outer(ys, F[1:B + 1])) % P).reshape(-1)[:n]
+    b = ((np.outer(xs, F[1:B + 1]) + np.outer(ys, F[2:B + 2])) % P).reshape(-1)[:n]
     return [wire.m31_column_as_qm31(a), wire.m31_column_as_qm31(b)]
 
 
@@ -287,3 +301,58 @@ def rescue_stacked(trace_log, seed=SEED_RESCUE):
     final = [(int(flat[n - 1, j]), 0, 0, 0) for j in range(4)]
     pi = b"".join(wire.qm31(v) for v in initial) + b"".join(wire.qm31(v) for v in final)
     return cols, pi
+
+
+# ---------------------------------------------------------------------------
+# Mixed-size proof streams (batched and served proving)
+# ---------------------------------------------------------------------------
+
+SEED_BATCH = 0x5EED0007
+SEED_SERVE = 0x5EED0008
+
+
+def _mix(seed, index):
+    return int(splitmix64((seed ^ (index * 0xD1B54A32D192ED03)) & MASK64, 1)[0])
+
+
+def proof_job(air, trace_log, seed, sep, num_queries=16, remainder_log=3):
+    """One proof request at blowup 4: (air, params bytes, public inputs, trace bytes, sep)."""
+    if air == AIR_SEEDED_FIB:
+        tr, pi = seeded_fib(trace_log, seed)
+    elif air == AIR_RESCUE_STACKED:
+        tr, pi = rescue_stacked(trace_log, seed)
+    else:
+        raise ValueError(f"no stream generator for AIR {air}")
+    params = wire.StarkParams(trace_log, 2, num_queries, remainder_log).encode()
+    return (air, params, pi, wire.columns(tr), sep)
+
+
+def batch_shapes(count, seed=SEED_BATCH, log_min=10, log_max=20):
+    """(air, trace_log, trace seed, channel separator) of `count` independent traces:
+    Fibonacci or stacked Rescue 50/50, log2 rows uniform in [log_min, log_max], a
+    distinct channel separator per trace."""
+    out = []
+    for i in range(count):
+        r = _mix(seed, i)
+        air = AIR_SEEDED_FIB if r & 1 else AIR_RESCUE_STACKED
+        lg = log_min + ((r >> 8) % (log_max - log_min + 1))
+        out.append((air, lg, (r >> 20) & MASK64, b"zig-stark:batch:" + i.to_bytes(8, "little")))
+    return out
+
+
+def serve_shapes(count, seed=SEED_SERVE, log_min=12, log_max=22, p_geo=0.5, mix=(0.5, 0.5)):
+    """Served-stream requests: AIR by `mix` (Fibonacci, stacked Rescue), log2 rows from a
+    geometric distribution (success probability p_geo) truncated to [log_min, log_max]."""
+    out = []
+    span = log_max - log_min + 1
+    w = np.array([(1 - p_geo) ** k * p_geo for k in range(span)])
+    cdf = np.cumsum(w / w.sum())
+    for i in range(count):
+        r = _mix(seed, i)
+        u = ((r >> 11) & ((1 << 53) - 1)) / float(1 << 53)
+        lg = log_min + int(np.searchsorted(cdf, u, side="right"))
+        lg = min(lg, log_max)
+        v = (r & 0x3FF) / 1024.0
+        air = AIR_SEEDED_FIB if v < mix[0] / sum(mix) else AIR_RESCUE_STACKED
+        out.append((air, lg, _mix(seed ^ 0xABCDEF, i), b"zig-stark:serve:" + i.to_bytes(8, "little")))
+    return out
