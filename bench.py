@@ -38,6 +38,15 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--log-rows", type=int, default=LOG_ROWS, help="smaller cases for profiling")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="commit", choices=["commit", "batch", "serve"],
+                    help="commit: the circle commit step (default); batch: mixed-size proof batch, "
+                         "batched vs one at a time; serve: Poisson request stream, p50/p99 latency")
+    ap.add_argument("--jobs", type=int, default=512, help="batch: number of traces")
+    ap.add_argument("--log-min", type=int, default=None)
+    ap.add_argument("--log-max", type=int, default=None)
+    ap.add_argument("--concurrency", type=int, default=8, help="batch / serve: prover workers")
+    ap.add_argument("--rate", type=float, default=400.0, help="serve: arrivals per second")
+    ap.add_argument("--duration", type=float, default=5.0, help="serve: seconds of arrivals")
     return ap.parse_args()
 
 
@@ -156,12 +165,169 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# proof workloads: a mixed-size batch, and a served request stream
+# ---------------------------------------------------------------------------
+
+def _proof_jobs(shapes, cache_variants=None):
+    """Wire-format jobs for (air, log_rows, seed, sep) shapes. With cache_variants,
+    traces repeat per (air, log_rows) across that many seeds (each request keeps its
+    own channel separator, so every proof differs)."""
+    from zs_b200 import workload as wl
+    cache, jobs = {}, []
+    for i, (air, lg, seed, sep) in enumerate(shapes):
+        key = (air, lg, i % cache_variants) if cache_variants else i
+        if key not in cache:
+            cache[key] = wl.proof_job(air, lg, seed, sep)
+        air_, params, pi, trace, _ = cache[key]
+        jobs.append((air_, params, pi, trace, sep))
+    return jobs
+
+
+def _cpu_prove_sample(jobs, max_log, count):
+    """The oracle prover (NTT route, OpenMP over the host cores) on the first `count`
+    jobs with at most 2^max_log rows."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    pick = [j for j in jobs if j[1][0] <= max_log][:count]
+    t0 = time.perf_counter()
+    for air, params, pi, trace, sep in pick:
+        oracle.prove(air, params, pi, b"", trace, sep, mode=1)
+    dt = time.perf_counter() - t0
+    return {"value": len(pick) / dt, "unit": "proofs/s", "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"{len(pick)} jobs of the stream with <= 2^{max_log} rows, oracle NTT prover, {dt:.2f} s"}
+
+
+def run_batch(args, world, rank, local):
+    """Independent traces (Fibonacci / stacked Rescue 50/50 by seed, log2 rows uniform
+    in 10..20, blowup 4, 16 queries, a channel separator per trace), proven batched
+    (zs_m31_prove_batch) and one at a time (zs_m31_prove), both from host buffers."""
+    import torch
+    from zs_b200 import native
+    from zs_b200 import workload as wl
+    torch.cuda.set_device(local)
+    lo, hi = args.log_min or 10, args.log_max or 20
+    shapes = wl.batch_shapes(args.jobs, log_min=lo, log_max=hi)[rank::world]
+    jobs = _proof_jobs(shapes)
+    kw = [dict(air_id=a, params=p, public_inputs=pi, trace=t, channel_sep=sp) for a, p, pi, t, sp in jobs]
+    h2d = sum(len(j[3]) + len(j[1]) + len(j[2]) for j in jobs)
+
+    def batched():
+        return native.prove_batch(kw, concurrency=args.concurrency)
+
+    def plain():
+        return [native.prove(**k) for k in kw]
+
+    ref = batched()  # grows the device pool to the batch's working set
+    assert all(isinstance(p, bytes) for p in ref), "a batch job failed"
+    for _ in range(max(0, args.warmup - 1)):
+        batched()
+    d2h = sum(len(p) for p in ref)
+
+    def timed(fn, k):
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            out = fn()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        barrier(world)
+        return max_over_ranks(dt, world) / k, out
+
+    with ClockSampler(local) as clocks:
+        t_b, got = timed(batched, args.steps)
+    assert got == ref, "batched proofs changed between runs"
+    plain()  # warm the one-at-a-time path
+    t_p, got_p = timed(plain, args.steps)
+    assert got_p == ref, "one-at-a-time proofs differ from the batched ones"
+    value = args.jobs / t_b
+    line = {
+        "metric": "proofs/s, batched (mixed-size Fibonacci/Rescue stream)", "value": value,
+        "unit": "proofs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_b * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "u32 (M31 / QM31 exact)", "data": "synthetic (SplitMix64 seeded)",
+        "config": {"workload": f"{args.jobs} traces, SeededFib / stacked Rescue 50/50 by seed, log2 rows "
+                               f"uniform in {lo}..{hi}, blowup 4, 16 queries, per-trace channel separator",
+                   "concurrency": args.concurrency, "parallelism": f"jobs sharded over {world} replica(s)",
+                   "l2": "working set far above L2"},
+        "plain_value": args.jobs / t_p, "plain_ms_per_step": t_p * 1e3,
+        "batched_over_plain": t_p / t_b,
+        "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "note": "the prover API takes host buffers and returns host proofs: every step is end to end"},
+        "roofline": None,
+        "gpu_launches": None,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = _cpu_prove_sample(jobs, 13, 24)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_serve(args, world, rank, local):
+    """Poisson arrivals at --rate per second for --duration seconds; each request a
+    Fibonacci or stacked Rescue proof (50/50) with log2 rows from a geometric
+    distribution (p = 0.5) truncated to 12..22. Served with continuous batching
+    (--concurrency workers) and, on the same arrivals, one request at a time."""
+    import torch
+    from zs_b200 import serving
+    from zs_b200 import workload as wl
+    torch.cuda.set_device(local)
+    lo, hi = args.log_min or 12, args.log_max or 22
+    arrivals = serving.poisson_arrivals(args.rate, args.duration, wl.SEED_SERVE + rank)
+    shapes = wl.serve_shapes(len(arrivals), seed=wl.SEED_SERVE + 7919 * rank, log_min=lo, log_max=hi)
+    jobs = _proof_jobs(shapes, cache_variants=2)
+    # warm-up: the largest shapes, so the device pool already holds the working set
+    warm = sorted(set((j[0], j[1][0]) for j in jobs), key=lambda x: -x[1])[:4]
+    wjobs = [next(j for j in jobs if (j[0], j[1][0]) == w) for w in warm]
+    serving.replay(wjobs * 2, [0.0] * (2 * len(wjobs)), args.concurrency)
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        served = serving.replay(jobs, arrivals, args.concurrency)
+    plain = serving.replay(jobs, arrivals, 1)
+    barrier(world)
+    wall = max_over_ranks(served["wall_s"], world)
+    wall_p = max_over_ranks(plain["wall_s"], world)
+    n_total = len(jobs) * world
+    lat, lat_p = served["latency_ms"], plain["latency_ms"]
+    line = {
+        "metric": "proofs/s and p50/p99 latency, served stream (continuous batching)",
+        "value": n_total / wall, "unit": "proofs/s", "n_gpus": world, "steps": 1, "warmup": 1,
+        "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32 (M31 / QM31 exact)", "data": "synthetic (SplitMix64 seeded; traces repeat over 2 seeds "
+                                                   "per shape, every request has its own channel separator)",
+        "config": {"workload": f"Poisson {args.rate:g} req/s for {args.duration:g} s per GPU, SeededFib / "
+                               f"stacked Rescue 50/50, log2 rows geometric(0.5) truncated to {lo}..{hi}, "
+                               "blowup 4, 16 queries", "requests": n_total, "concurrency": args.concurrency,
+                   "parallelism": f"replicas x{world}"},
+        "latency_ms": {"p50": serving.percentile(lat, 50), "p99": serving.percentile(lat, 99),
+                       "max": max(lat) if lat else None},
+        "plain": {"value": n_total / wall_p, "p50": serving.percentile(lat_p, 50),
+                  "p99": serving.percentile(lat_p, 99)},
+        "failed": served["failed"] + plain["failed"],
+        "e2e": {"value": n_total / wall, "unit": "proofs/s",
+                "h2d_bytes_per_step": sum(len(j[3]) for j in jobs), "d2h_bytes_per_step": None,
+                "note": "requests arrive as host buffers and proofs return to the host"},
+        "roofline": None, "gpu_launches": None, "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)
         barrier(world)
+        return
+    if args.workload in ("batch", "serve"):
+        (run_batch if args.workload == "batch" else run_serve)(args, world, rank, local)
+        barrier(world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     import numpy as np
     import torch

@@ -336,7 +336,7 @@ def batch_shapes(count, seed=SEED_BATCH, log_min=10, log_max=20):
         r = _mix(seed, i)
         air = AIR_SEEDED_FIB if r & 1 else AIR_RESCUE_STACKED
         lg = log_min + ((r >> 8) % (log_max - log_min + 1))
-        out.append((air, lg, (r >> 20) & MASK64, b"zig-stark:batch:" + i.to_bytes(8, "little")))
+        out.append((air, lg, (r >> 20) & MASK64, b"zs-batch:%d" % i))
     return out
 
 
@@ -354,5 +354,5 @@ def serve_shapes(count, seed=SEED_SERVE, log_min=12, log_max=22, p_geo=0.5, mix=
         lg = min(lg, log_max)
         v = (r & 0x3FF) / 1024.0
         air = AIR_SEEDED_FIB if v < mix[0] / sum(mix) else AIR_RESCUE_STACKED
-        out.append((air, lg, _mix(seed ^ 0xABCDEF, i), b"zig-stark:serve:" + i.to_bytes(8, "little")))
+        out.append((air, lg, _mix(seed ^ 0xABCDEF, i), b"zs-serve:%d" % i))
     return out
