@@ -306,31 +306,85 @@ __device__ __forceinline__ void run_layers(uint32_t* s, uint32_t gstride, unsign
 // Pass kernels. blockIdx.y = column; columns are `col_stride` words apart.
 // ---------------------------------------------------------------------------
 
-// Inverse layers [0, K) of a size-2^L transform. Reads natural-order evaluations
-// (the reference bit-reverses them first), writes position order to `tmp`.
-__global__ void __launch_bounds__(512) k_ifft_low(const uint32_t* __restrict__ in, size_t in_stride,
-                                                  uint32_t* __restrict__ tmp, unsigned L, unsigned K, unsigned G,
-                                                  const uint32_t* __restrict__ ITW) {
+// 4-byte asynchronous global -> shared copies (LDGSTS): the copy of the next batch
+// of groups runs while the current batch is transformed.
+__device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// The low pass of the inverse (INV) or forward transform over `iters` consecutive
+// batches of G groups of 2^K elements per CTA (blockIdx.y = column), double-buffered:
+// batch j + 1 is copied into shared memory while batch j is transformed and stored.
+//   inverse: layers [0, K) of a size-2^LG transform; reads natural-order evaluations
+//            through the reference's bit reversal, writes position order.
+//   forward: layers [0, K) of a size-2^LG transform over contiguous groups, then the
+//            reference's final bit reversal on the store (natural-order evaluations).
+// Shared memory: two buffers of G padded groups, then two G-entry arrays of virtual
+// group bases.
+template <bool INV>
+__global__ void __launch_bounds__(256, 3) k_low(const uint32_t* __restrict__ src, size_t src_stride,
+                                             uint32_t* __restrict__ dst, size_t dst_stride, unsigned LG, unsigned K,
+                                             unsigned G, unsigned iters, const uint32_t* __restrict__ TW) {
   extern __shared__ uint32_t sm[];
-  const uint32_t n = 1u << L, gsz = 1u << K, gstride = group_stride(K);
-  const unsigned hb = L - K;
-  uint32_t* vb = sm + G * gstride;
-  const uint32_t gp0 = blockIdx.x * G;
-  const uint32_t* col = in + (size_t)blockIdx.y * in_stride;
-  uint32_t* out = tmp + (size_t)blockIdx.y * n;
-  if (threadIdx.x < G) vb[threadIdx.x] = bitrev(gp0 + threadIdx.x, hb) << K;
-  const unsigned lg_g = 31 - __clz(G);
-  #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-    const uint32_t t = idx & (G - 1), v = idx >> lg_g;
-    sm[t * gstride + padx(bitrev(v, K))] = __ldg(col + ((size_t)v << hb) + gp0 + t);
-  }
-  __syncthreads();
-  run_layers<true>(sm, gstride, G, K, 0, ITW, n, vb);
-  #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-    const uint32_t t = idx >> K, e = idx & (gsz - 1);
-    out[vb[t] + e] = sm[t * gstride + padx(e)];
+  const uint32_t N = 1u << LG, gsz = 1u << K, gstride = group_stride(K);
+  const unsigned hb = LG - K, lg_g = 31 - __clz(G);
+  // buffer b at sm + b * G * gstride, its group bases at sm + 2 * G * gstride + b * G
+  auto buf = [&](int b) { return sm + (uint32_t)b * G * gstride; };
+  auto vbs = [&](int b) { return sm + 2 * G * gstride + (uint32_t)b * G; };
+  const uint32_t* col = src + (size_t)blockIdx.y * src_stride;
+  uint32_t* out = dst + (size_t)blockIdx.y * dst_stride;
+  const uint32_t batch0 = blockIdx.x * iters;
+
+  auto issue = [&](uint32_t j, int b) {
+    const uint32_t g0 = (batch0 + j) * G;
+    if (threadIdx.x < G) vbs(b)[threadIdx.x] = bitrev(g0 + threadIdx.x, hb) << K;
+    uint32_t* s = buf(b);
+    if (INV) {
+      #pragma unroll 8
+      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+        const uint32_t t = idx & (G - 1), v = idx >> lg_g;
+        cp_async4(s + t * gstride + padx(bitrev(v, K)), col + ((size_t)v << hb) + g0 + t);
+      }
+    } else {
+      #pragma unroll 8
+      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+        const uint32_t t = idx >> K, e = idx & (gsz - 1);
+        cp_async4(s + t * gstride + padx(e), col + ((size_t)bitrev(g0 + t, hb) << K) + e);
+      }
+    }
+    cp_async_commit();
+  };
+
+  issue(0, 0);
+  for (uint32_t j = 0; j < iters; ++j) {
+    const int b = (int)(j & 1);
+    if (j + 1 < iters)
+      issue(j + 1, b ^ 1);
+    else
+      cp_async_commit();  // an empty group keeps "all but the newest group" meaning batch j
+    cp_async_wait_one();
+    __syncthreads();
+    uint32_t* s = buf(b);
+    const uint32_t* vb = vbs(b);
+    const uint32_t g0 = (batch0 + j) * G;
+    run_layers<INV>(s, gstride, G, K, 0, TW, N, vb);  // ends with a barrier
+    if (INV) {
+      #pragma unroll 8
+      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+        const uint32_t t = idx >> K, e = idx & (gsz - 1);
+        out[vb[t] + e] = s[t * gstride + padx(e)];
+      }
+    } else {
+      #pragma unroll 8
+      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+        const uint32_t t = idx & (G - 1), v = idx >> lg_g;
+        out[((size_t)v << hb) + g0 + t] = s[t * gstride + padx(bitrev(v, K))];
+      }
+    }
+    __syncthreads();  // buffer b is refilled by the next iteration's issue
   }
 }
 
@@ -414,35 +468,6 @@ __global__ void __launch_bounds__(512, 2) k_mid(const uint32_t* __restrict__ in,
   }
 }
 
-// Forward layers [0, K) of a size-2^LB transform over contiguous groups, then the
-// reference's final bit reversal on the store (natural-order evaluations).
-__global__ void __launch_bounds__(512) k_fft_low(const uint32_t* __restrict__ mid, size_t mid_stride,
-                                                 uint32_t* __restrict__ out, size_t out_stride, unsigned LB,
-                                                 unsigned K, unsigned G, const uint32_t* __restrict__ TW) {
-  extern __shared__ uint32_t sm[];
-  const uint32_t N = 1u << LB, gsz = 1u << K, gstride = group_stride(K);
-  const unsigned hb = LB - K;
-  uint32_t* vb = sm + G * gstride;
-  const uint32_t q0 = blockIdx.x * G;
-  const uint32_t* src = mid + (size_t)blockIdx.y * mid_stride;
-  uint32_t* dst = out + (size_t)blockIdx.y * out_stride;
-  if (threadIdx.x < G) vb[threadIdx.x] = bitrev(q0 + threadIdx.x, hb) << K;
-  __syncthreads();
-  #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-    const uint32_t t = idx >> K, e = idx & (gsz - 1);
-    sm[t * gstride + padx(e)] = __ldg(src + vb[t] + e);
-  }
-  __syncthreads();
-  run_layers<false>(sm, gstride, G, K, 0, TW, N, vb);
-  const unsigned lg_g = 31 - __clz(G);
-  #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-    const uint32_t t = idx & (G - 1), v = idx >> lg_g;
-    dst[((size_t)v << hb) + q0 + t] = sm[t * gstride + padx(bitrev(v, K))];
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Host launch helpers
 // ---------------------------------------------------------------------------
@@ -469,6 +494,22 @@ size_t smem_bytes(unsigned M, unsigned G, unsigned buffers) {
 void set_smem(const void* fn, size_t bytes) {
   ZS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
+// The low pass (k_low) over C columns of a size-2^LG transform split at K: batches of
+// G groups (at most kLowWords words each), `iters` batches per CTA.
+constexpr uint32_t kLowWords = 8192;
+constexpr unsigned kLowThreads = 256;
+template <bool INV>
+void launch_low(const uint32_t* src, size_t src_stride, uint32_t* dst, size_t dst_stride, uint32_t C, unsigned LG,
+                unsigned K, const uint32_t* tw, cudaStream_t st) {
+  const uint32_t ngroups = 1u << (LG - K);
+  const unsigned G = pick_groups(K, ngroups, kLowWords);
+  const uint32_t batches = ngroups / G;
+  unsigned iters = 1;
+  while (iters < 8 && batches % (iters * 2) == 0 && batches / (iters * 2) >= 16) iters *= 2;
+  const size_t sb = ((size_t)2 * G * group_stride(K) + 2 * G) * sizeof(uint32_t);
+  set_smem((const void*)k_low<INV>, sb);
+  k_low<INV><<<dim3(batches / iters, C), kLowThreads, sb, st>>>(src, src_stride, dst, dst_stride, LG, K, G, iters, tw);
+}
 }  // namespace
 
 size_t lde_scratch_words(unsigned L, unsigned B, uint32_t C) {
@@ -484,13 +525,7 @@ void circle_lde(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, size_t 
   const uint32_t n = 1u << L;
   uint32_t* tmp = scratch;
   uint32_t* mid = scratch + (size_t)C * n;
-  {
-    const uint32_t ngroups = 1u << (L - K);
-    const unsigned G = pick_groups(K, ngroups);
-    const size_t sb = smem_bytes(K, G, 1);
-    set_smem((const void*)k_ifft_low, sb);
-    k_ifft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_in, in_stride, tmp, L, K, G, small.itw);
-  }
+  launch_low<true>(d_in, in_stride, tmp, n, C, L, K, small.itw, st);
   {
     const unsigned M = L - K;
     const uint32_t ngroups = 1u << K;
@@ -500,14 +535,7 @@ void circle_lde(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, size_t 
     k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(tmp, n, mid, (size_t)n << B, L, K, B, G, small.itw, big.tw,
                                                       MID_LDE);
   }
-  {
-    const unsigned LB = L + B;
-    const uint32_t ngroups = 1u << (LB - K);
-    const unsigned G = pick_groups(K, ngroups);
-    const size_t sb = smem_bytes(K, G, 1);
-    set_smem((const void*)k_fft_low, sb);
-    k_fft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(mid, (size_t)n << B, d_out, out_stride, LB, K, G, big.tw);
-  }
+  launch_low<false>(mid, (size_t)n << B, d_out, out_stride, C, L + B, K, big.tw, st);
   ZS_CUDA(cudaGetLastError());
 }
 
@@ -523,13 +551,7 @@ void circle_fft(const uint32_t* d_coeffs, uint32_t* d_evals, uint32_t C, const C
     k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_coeffs, n, scratch, n, L, K, 0, G, dom.itw, dom.tw,
                                                       MID_FFT_ONLY);
   }
-  {
-    const uint32_t ngroups = 1u << (L - K);
-    const unsigned G = pick_groups(K, ngroups);
-    const size_t sb = smem_bytes(K, G, 1);
-    set_smem((const void*)k_fft_low, sb);
-    k_fft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(scratch, n, d_evals, n, L, K, G, dom.tw);
-  }
+  launch_low<false>(scratch, n, d_evals, n, C, L, K, dom.tw, st);
   ZS_CUDA(cudaGetLastError());
 }
 
@@ -537,13 +559,7 @@ void circle_ifft(const uint32_t* d_evals, uint32_t* d_coeffs, uint32_t C, const 
                  cudaStream_t st) {
   const unsigned L = dom.lg, K = pick_split(L), M = L - K;
   const uint32_t n = 1u << L;
-  {
-    const uint32_t ngroups = 1u << (L - K);
-    const unsigned G = pick_groups(K, ngroups);
-    const size_t sb = smem_bytes(K, G, 1);
-    set_smem((const void*)k_ifft_low, sb);
-    k_ifft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_evals, n, scratch, L, K, G, dom.itw);
-  }
+  launch_low<true>(d_evals, n, scratch, n, C, L, K, dom.itw, st);
   {
     const uint32_t ngroups = 1u << K;
     const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
@@ -584,13 +600,7 @@ void circle_lde_tables(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, 
   const uint32_t n = 1u << L;
   uint32_t* tmp = scratch;
   uint32_t* mid = scratch + (size_t)C * n;
-  {
-    const uint32_t ngroups = 1u << (L - K);
-    const unsigned G = pick_groups(K, ngroups);
-    const size_t sb = smem_bytes(K, G, 1);
-    set_smem((const void*)k_ifft_low, sb);
-    k_ifft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_in, in_stride, tmp, L, K, G, itw_small);
-  }
+  launch_low<true>(d_in, in_stride, tmp, n, C, L, K, itw_small, st);
   {
     const unsigned M = L - K;
     const uint32_t ngroups = 1u << K;
@@ -600,14 +610,7 @@ void circle_lde_tables(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, 
     k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(tmp, n, mid, (size_t)n << B, L, K, B, G, itw_small, tw_big,
                                                       MID_LDE);
   }
-  {
-    const unsigned LB = L + B;
-    const uint32_t ngroups = 1u << (LB - K);
-    const unsigned G = pick_groups(K, ngroups);
-    const size_t sb = smem_bytes(K, G, 1);
-    set_smem((const void*)k_fft_low, sb);
-    k_fft_low<<<dim3(ngroups / G, C), kThreads, sb, st>>>(mid, (size_t)n << B, d_out, out_stride, LB, K, G, tw_big);
-  }
+  launch_low<false>(mid, (size_t)n << B, d_out, out_stride, C, L + B, K, tw_big, st);
   ZS_CUDA(cudaGetLastError());
 }
 
