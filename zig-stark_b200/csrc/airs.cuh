@@ -101,6 +101,21 @@ ZS_HD void air_eval(const AirConsts& k, const qm31& x, const qm31* cur, const qm
   }
 }
 
+// The stacked Rescue transitions with the row-periodic values read from `per`
+// ({y - w8^7, P_0(y), ..., P_3(y)} for y = x^(n/8)), which the quotient kernel takes from
+// a table instead of raising every domain point to n/8. Same values as air_eval.
+ZS_HD void rescue_stacked_eval(const qm31* per, const qm31* cur, const qm31* next, qm31* out) {
+  const qm31 z = per[0];
+  for (int j = 0; j < 4; ++j) {
+    qm31 expect = qzero();
+    for (int l = 0; l < 4; ++l) expect = qadd(expect, qmul_m(qmul(cur[8 + l], cur[4 + l]), rescue_mds(j, l)));
+    expect = qadd(expect, per[1 + j]);
+    out[j] = qmul(z, qsub(next[j], expect));
+    out[4 + j] = qsub(cur[4 + j], qmul(cur[j], cur[j]));
+    out[8 + j] = qsub(cur[8 + j], qmul(cur[4 + j], cur[j]));
+  }
+}
+
 struct Boundary {
   uint32_t column;
   uint64_t step;

@@ -5,6 +5,8 @@
 
 namespace zs {
 
+constexpr uint32_t kPerRows = 64;  // 8 rows per permutation x blowup <= 8
+
 // Everything the quotient and DEEP kernels need beyond the codewords.
 struct QuotConsts {
   AirConsts air;
@@ -17,6 +19,11 @@ struct QuotConsts {
   uint32_t b_col[kMaxBound];
   qm31 b_val[kMaxBound];
   qm31 b_pt[kMaxBound];  // p_k = w^step_k
+  uint32_t n_bpts;         // distinct boundary points, bpts[g], and b_grp[b] = g with bpts[g] = b_pt[b]
+  uint32_t b_grp[kMaxBound];
+  qm31 bpts[kMaxBound];
+  uint32_t per_mask;                 // stacked Rescue: per_tab[i & per_mask] holds the
+  qm31 per_tab[kPerRows][5];         // periodic values of domain point i (airs.cuh)
   qm31 zh[8], zh_inv[8];  // Z_H(d_i) depends on i mod 2^log_blowup
   qm31 ac[kMaxKey], ar[kMaxRel];
   uint32_t sel[kMaxRel], mult[kMaxRel], n_keys[kMaxRel], keys[kMaxRel][kMaxKey], tabs[kMaxRel][kMaxKey];
@@ -41,26 +48,72 @@ __device__ __host__ __forceinline__ qm31 lookup_constraint(const QuotConsts& k, 
   return qadd(qmul(sel, lb), qmul(qsub(qone(), sel), tb));
 }
 
+// Groups the boundary assertions by their point (host side, after b_pt is filled).
+inline void group_boundaries(QuotConsts& k) {
+  k.n_bpts = 0;
+  for (uint32_t b = 0; b < k.total_bound; ++b) {
+    uint32_t g = 0;
+    while (g < k.n_bpts && !qeq(k.bpts[g], k.b_pt[b])) ++g;
+    if (g == k.n_bpts) k.bpts[k.n_bpts++] = k.b_pt[b];
+    k.b_grp[b] = g;
+  }
+}
+
 // Hc(x) (stark.zig:505-533): transitions x (x - w^(n-1)), cyclic LogUp and
-// selector-binarity constraints, boundary terms with Z_H(x) / (x - p_k).
+// selector-binarity constraints, boundary terms with Z_H(x) / (x - p_k). `per`: the
+// periodic values of the stacked Rescue AIR at x (rescue_stacked_eval in airs.cuh).
+// Evaluated as sum_t alpha_t C_t(x) (x - w^(n-1)) = (x - w^(n-1)) sum_t alpha_t C_t(x) and
+// sum_k beta_k (f_k(x) - v_k) Z_H(x) / (x - p_k) = Z_H(x) sum_p (1 / (x - p)) sum_{k: p_k = p}
+// beta_k (f_k(x) - v_k): equal in the ring by distributivity, with one inverse per
+// distinct boundary point. `units`: every x - p is a unit (true on the evaluation domain,
+// whose offset lies outside every 2-power subgroup in both CRT components), so the
+// inverses come from one batch inversion.
 __device__ __host__ inline qm31 composition(const QuotConsts& k, const qm31& x, const qm31* cur, const qm31* next,
-                                            const qm31* pre, const qm31& zh) {
+                                            const qm31* pre, const qm31& zh, const qm31* per = nullptr,
+                                            bool units = false) {
   qm31 res[kMaxTrans];
-  air_eval(k.air, x, cur, next, res);
-  qm31 h = qzero();
-  const qm31 xl = qsub(x, k.last_point);
-  for (uint32_t t = 0; t < k.num_trans; ++t) h = qadd(h, qmul(k.alphas[t], qmul(res[t], xl)));
+  if (per)
+    rescue_stacked_eval(per, cur, next, res);
+  else
+    air_eval(k.air, x, cur, next, res);
+  qm31 tsum = qzero();
+  for (uint32_t t = 0; t < k.num_trans; ++t) tsum = qadd(tsum, qmul(k.alphas[t], res[t]));
+  qm31 h = qmul(tsum, qsub(x, k.last_point));
   for (uint32_t r = 0; r < k.n_rel; ++r)
     h = qadd(h, qmul(k.alphas[k.num_trans + r], lookup_constraint(k, r, cur, pre, cur[k.m + r], next[k.m + r])));
   for (uint32_t r = 0; r < k.n_rel; ++r) {
     const qm31 sel = cur[k.sel[r]];
     h = qadd(h, qmul(k.alphas[k.num_trans + k.n_rel + r], qmul(sel, qsub(qone(), sel))));
   }
-  for (uint32_t b = 0; b < k.total_bound; ++b) {
-    const qm31 term = qmul(qmul(qsub(cur[k.b_col[b]], k.b_val[b]), zh), qinv(qsub(x, k.b_pt[b])));
-    h = qadd(h, qmul(k.betas[b], term));
+  if (k.total_bound == 0) return h;
+  // acc_g = sum_{k: p_k = p_g} beta_k (f_k(x) - v_k), accumulated per group in a
+  // register: local arrays written at run-time indices gave wrong results in this
+  // kernel on the device, so the grouping is a comparison and the batch inversion keeps
+  // no array of prefix products.
+  qm31 bsum = qzero();
+  if (units) {
+    // 1 / (x - p_g) = prod_{h != g} (x - p_h) / prod_h (x - p_h): one inversion
+    qm31 run = qone();
+    for (uint32_t g = 0; g < k.n_bpts; ++g) run = qmul(run, qsub(x, k.bpts[g]));
+    const qm31 inv = qinv(run);
+    for (uint32_t g = 0; g < k.n_bpts; ++g) {
+      qm31 ig = inv;
+      for (uint32_t h2 = 0; h2 < k.n_bpts; ++h2)
+        if (h2 != g) ig = qmul(ig, qsub(x, k.bpts[h2]));
+      qm31 acc = qzero();
+      for (uint32_t b = 0; b < k.total_bound; ++b)
+        if (k.b_grp[b] == g) acc = qadd(acc, qmul(k.betas[b], qsub(cur[k.b_col[b]], k.b_val[b])));
+      bsum = qadd(bsum, qmul(acc, ig));
+    }
+  } else {
+    for (uint32_t g = 0; g < k.n_bpts; ++g) {
+      qm31 acc = qzero();
+      for (uint32_t b = 0; b < k.total_bound; ++b)
+        if (k.b_grp[b] == g) acc = qadd(acc, qmul(k.betas[b], qsub(cur[k.b_col[b]], k.b_val[b])));
+      bsum = qadd(bsum, qmul(acc, qinv(qsub(x, k.bpts[g]))));
+    }
   }
-  return h;
+  return qadd(h, qmul(bsum, zh));
 }
 
 }  // namespace zs

@@ -10,8 +10,9 @@ namespace zs {
 // inv[k] = w^-k for k < 2^(log_n-1).
 struct NttTables {
   unsigned log_n = 0;
-  qm31* fwd = nullptr;
-  qm31* inv = nullptr;
+  qm31* fwd = nullptr;      // w^k, k < n/2 (QM31; the domain points of D)
+  qm31* fwd_crt = nullptr;  // phi(w^k): forward twiddles in the CRT domain (ntt.cu)
+  qm31* inv_crt = nullptr;  // phi(w^-k)
   cudaStream_t st = nullptr;  // freed in stream order, so concurrent provers never synchronize the device
   NttTables(unsigned log_n, cudaStream_t st);
   ~NttTables();

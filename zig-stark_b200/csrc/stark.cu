@@ -63,7 +63,8 @@ __global__ void __launch_bounds__(kT) k_quotient(const qm31* __restrict__ cw, qm
   }
   const qm31 x = domain_point(k, wpow, i);
   const uint32_t zi = i & ((1u << k.log_blowup) - 1);
-  const qm31 h = composition(k, x, cur, next, pre, k.zh[zi]);
+  const qm31* per = k.air.id == AIR_RESCUE_STACKED ? k.per_tab[i & k.per_mask] : nullptr;
+  const qm31 h = composition(k, x, cur, next, pre, k.zh[zi], per, true);
   stq(q + i, qmul(h, k.zh_inv[zi]));
 }
 
@@ -431,6 +432,21 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     kc.b_col[b] = bnd[b].column;
     kc.b_val[b] = bnd[b].value;
     kc.b_pt[b] = qpow(w, bnd[b].step);
+  }
+  group_boundaries(kc);
+  if (air.id == AIR_RESCUE_STACKED) {
+    // y_i = d_i^(n/8) = offset^(n/8) (w_N^(n/8))^i repeats with period 8 * 2^lb
+    const uint32_t period = 8u << lb;
+    if (period > kPerRows) throw Error(ZS_EGENERIC, "blowup too large for the periodic table");
+    kc.per_mask = period - 1;
+    const qm31 wN = q_root_of_unity(lN);
+    qm31 wr = qone();
+    for (uint32_t r = 0; r < period; ++r) {
+      const qm31 y = qpow(qmul(offset, wr), n / 8);
+      kc.per_tab[r][0] = qsub(y, kc.air.w8_7);
+      for (int j = 0; j < 4; ++j) kc.per_tab[r][1 + j] = horner(kc.air.poly[j], 8, y);
+      wr = qmul(wr, wN);
+    }
   }
   {
     // Z_H(d_i) = offset^n * (w_N^n)^(i mod 2^lb) - 1

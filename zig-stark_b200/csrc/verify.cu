@@ -242,6 +242,7 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
     kc.b_val[b] = bnd[b].value;
     kc.b_pt[b] = qpow(w, bnd[b].step);
   }
+  group_boundaries(kc);
   ch.absorb(p.qroot);
   const qm31 z = ch.sample_q();
   for (auto& v : p.deep) ch.absorb(v);
