@@ -126,6 +126,25 @@ int32_t zs_m31_verify(zs_host_allocator host, uint32_t air_id, const uint8_t *pa
                       const uint8_t *public_inputs, size_t public_inputs_len, const uint8_t *proof, size_t proof_len,
                       const uint8_t *channel_sep, size_t channel_sep_len, int *out_ok);
 
+/* Many independent verifications (serving acceptance checks): jobs[i] is checked as
+ * zs_m31_verify would check it, on `threads` host threads (0 = all hardware threads).
+ * out_ok[i] = 1 when proof i verifies, 0 otherwise; statuses[i] = 0, or the negative
+ * code zs_m31_verify would return for job i. Returns 0 unless the arguments themselves
+ * are malformed. No counterpart in the reference (its verify checks one proof). */
+typedef struct {
+    uint32_t air_id;
+    const uint8_t *params;
+    size_t params_len;
+    const uint8_t *public_inputs;
+    size_t public_inputs_len;
+    const uint8_t *proof;
+    size_t proof_len;
+    const uint8_t *channel_sep;
+    size_t channel_sep_len;
+} zs_m31_verify_job;
+int32_t zs_m31_verify_batch(size_t n_jobs, const zs_m31_verify_job *jobs, uint32_t threads, int *out_ok,
+                            int32_t *statuses);
+
 /* The commitment path alone (stark.zig:397-414): each column (wire
  * []const []const QM31, 2^trace_log values each) is interpolated on H, evaluated on
  * D = FRI_OFFSET * <w_N> with N = 2^(trace_log + log_blowup) and committed as a

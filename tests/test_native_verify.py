@@ -88,3 +88,35 @@ def test_rescue_stacked(orc):
     bad = bytearray(pi)
     bad[70] ^= 1
     assert not native.verify(wl.AIR_RESCUE_STACKED, params, bytes(bad), proof, b"v")
+
+
+@pytest.mark.parametrize("threads", [1, 3, 0])
+def test_verify_batch_matches_single(orc, threads):
+    """zs_m31_verify_batch gives each job the single call's answer: valid proofs,
+    false statements, tampered and malformed proofs mixed in one batch."""
+    jobs = []
+    for i, lg in enumerate([3, 4, 5, 6]):
+        params = wire.StarkParams(lg, 2, 16, 3)
+        tr, pi = wl.seeded_fib(lg, 100 + i)
+        proof = _proof(orc, wl.AIR_SEEDED_FIB, params, pi, tr)
+        jobs.append((wl.AIR_SEEDED_FIB, params, pi, proof, b"v"))
+    tr, pi = wl.rescue_stacked(5)
+    params = wire.StarkParams(5, 2, 16, 3)
+    jobs.append((wl.AIR_RESCUE_STACKED, params, pi, _proof(orc, wl.AIR_RESCUE_STACKED, params, pi, tr), b"v"))
+    a, p, pi0, pr0, s0 = jobs[0]
+    bad_pi = bytearray(pi0)
+    bad_pi[32] ^= 1
+    sp = wire.StarkProof.decode(pr0)
+    sp.quotient_root = bytes(32)
+    jobs += [(a, p, bytes(bad_pi), pr0, s0), (a, p, pi0, sp.encode(), s0), (a, p, pi0, pr0[:-3], s0),
+             (a, p, pi0, pr0, b"other")]
+    got = native.verify_batch(jobs, threads=threads)
+    want = []
+    for j in jobs:
+        try:
+            want.append(native.verify(*j))
+        except native.ZsError as e:
+            want.append(e.code)
+    assert got == want
+    assert got[:5] == [True] * 5 and got[5] is False and got[6] is False and got[7] == -2 and got[8] is False
+    assert native.verify_batch([]) == []

@@ -1,7 +1,10 @@
 // extern "C" entry points declared in include/zs_m31.h.
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <new>
+#include <thread>
 
 #include "../../include/zs_m31.h"
 #include "circle.cuh"
@@ -223,6 +226,29 @@ int32_t zs_m31_verify(zs_host_allocator host, uint32_t air_id, const uint8_t* pa
                            channel_sep, channel_sep_len)
                   ? 1
                   : 0;
+  });
+}
+
+int32_t zs_m31_verify_batch(size_t n_jobs, const zs_m31_verify_job* jobs, uint32_t threads, int* out_ok,
+                            int32_t* statuses) {
+  return guarded([&] {
+    if (n_jobs && (!jobs || !out_ok || !statuses)) throw Error(ZS_EMALFORMED, "null argument");
+    if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
+    if (threads > n_jobs) threads = (uint32_t)std::max<size_t>(n_jobs, 1);
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+      for (size_t i; (i = next.fetch_add(1)) < n_jobs;) {
+        const zs_m31_verify_job& j = jobs[i];
+        int ok = 0;
+        statuses[i] = zs_m31_verify(zs_host_allocator{}, j.air_id, j.params, j.params_len, j.public_inputs,
+                                    j.public_inputs_len, j.proof, j.proof_len, j.channel_sep, j.channel_sep_len, &ok);
+        out_ok[i] = ok;
+      }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
   });
 }
 

@@ -303,6 +303,38 @@ def verify(air_id, params, public_inputs, proof, channel_sep=b""):
     return bool(ok.value)
 
 
+class VerifyJob(ctypes.Structure):
+    """zs_m31_verify_job: the arguments of one zs_m31_verify call."""
+    _fields_ = [("air_id", ctypes.c_uint32),
+                ("params", ctypes.c_char_p), ("params_len", ctypes.c_size_t),
+                ("public_inputs", ctypes.c_char_p), ("public_inputs_len", ctypes.c_size_t),
+                ("proof", ctypes.c_char_p), ("proof_len", ctypes.c_size_t),
+                ("channel_sep", ctypes.c_char_p), ("channel_sep_len", ctypes.c_size_t)]
+
+
+def verify_batch(jobs, threads=0):
+    """zs_m31_verify_batch over (air_id, params, public_inputs, proof, channel_sep)
+    tuples; returns one entry per job: True / False, or the negative status code of a
+    job whose inputs could not be parsed."""
+    L = _bind_prove()
+    if not getattr(L, "_verify_batch_bound", False):
+        L.zs_m31_verify_batch.argtypes = [ctypes.c_size_t, ctypes.POINTER(VerifyJob), ctypes.c_uint32,
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int32)]
+        L._verify_batch_bound = True
+    packed = []
+    for air, params, pi, proof, sep in jobs:
+        if not isinstance(params, (bytes, bytearray)):
+            params = params.encode()
+        packed.append(VerifyJob(air, bytes(params), len(params), bytes(pi), len(pi), bytes(proof), len(proof),
+                                bytes(sep), len(sep)))
+    n = len(packed)
+    arr = (VerifyJob * max(n, 1))(*packed)
+    ok = (ctypes.c_int * max(n, 1))()
+    st = (ctypes.c_int32 * max(n, 1))()
+    check(L.zs_m31_verify_batch(n, arr, threads, ok, st), "zs_m31_verify_batch")
+    return [bool(ok[i]) if st[i] == 0 else int(st[i]) for i in range(n)]
+
+
 def commit_columns(columns, trace_log, log_blowup):
     """Per-column commitment roots (zs_m31_commit_columns); columns: wire bytes or a
     list of (2^trace_log, 4) uint32 arrays. Returns a list of 32-byte roots."""
