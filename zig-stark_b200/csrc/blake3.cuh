@@ -193,8 +193,15 @@ ZS_HD void hash_words(int nwords, Loader load, uint32_t out[8]) {
 
 }  // namespace b3
 
-// Host-side incremental Blake3 over arbitrary lengths (chunk state plus the
-// chaining-value stack), copyable so the transcript can be snapshotted.
+// Incremental Blake3 over arbitrary lengths (chunk state plus the chaining-value
+// stack) for the transcript, on the host and, in one thread, on the device. Copyable,
+// so the transcript can be snapshotted; snapshot_from copies only the live stack.
+ZS_HD void copy_bytes(void* dst, const void* src, size_t n) {
+  uint8_t* d = static_cast<uint8_t*>(dst);
+  const uint8_t* s = static_cast<const uint8_t*>(src);
+  for (size_t i = 0; i < n; ++i) d[i] = s[i];
+}
+
 struct Hasher {
   uint32_t cv[8];
   uint64_t chunk_counter = 0;
@@ -203,32 +210,43 @@ struct Hasher {
   uint32_t stack[54][8];
   unsigned depth = 0;
 
-  Hasher() { reset(); }
-  void reset() {
+  ZS_HD Hasher() { reset(); }
+  ZS_HD void reset() {
     b3::iv(cv);
     chunk_counter = 0;
-    std::memset(block, 0, 64);
+    for (int i = 0; i < 64; ++i) block[i] = 0;
     block_len = blocks_done = 0;
     depth = 0;
   }
-  static void words(const uint8_t* b, uint32_t w[16]) {
-    for (int i = 0; i < 16; ++i) std::memcpy(&w[i], b + 4 * i, 4);
+  ZS_HD void snapshot_from(const Hasher& o) {
+    copy_bytes(cv, o.cv, 32);
+    chunk_counter = o.chunk_counter;
+    copy_bytes(block, o.block, 64);
+    block_len = o.block_len;
+    blocks_done = o.blocks_done;
+    depth = o.depth;
+    copy_bytes(stack, o.stack, (size_t)32 * o.depth);
   }
-  uint32_t start() const { return blocks_done == 0 ? b3::CHUNK_START : 0; }
-  void push(uint32_t c[8], uint64_t total) {
+  ZS_HD static void words(const uint8_t* b, uint32_t w[16]) {
+    for (int i = 0; i < 16; ++i)
+      w[i] = (uint32_t)b[4 * i] | ((uint32_t)b[4 * i + 1] << 8) | ((uint32_t)b[4 * i + 2] << 16) |
+             ((uint32_t)b[4 * i + 3] << 24);
+  }
+  ZS_HD uint32_t start() const { return blocks_done == 0 ? b3::CHUNK_START : 0; }
+  ZS_HD void push(uint32_t c[8], uint64_t total) {
     while ((total & 1) == 0) {
       uint32_t m[16], out[16];
-      std::memcpy(m, stack[--depth], 32);
-      std::memcpy(m + 8, c, 32);
+      copy_bytes(m, stack[--depth], 32);
+      copy_bytes(m + 8, c, 32);
       uint32_t k[8];
       b3::iv(k);
       b3::compress_full(k, m, 0, 64, b3::PARENT, out);
-      std::memcpy(c, out, 32);
+      copy_bytes(c, out, 32);
       total >>= 1;
     }
-    std::memcpy(stack[depth++], c, 32);
+    copy_bytes(stack[depth++], c, 32);
   }
-  void update(const void* data, size_t len) {
+  ZS_HD void update(const void* data, size_t len) {
     const uint8_t* in = (const uint8_t*)data;
     while (len) {
       if (blocks_done * 64 + block_len == 1024) {
@@ -238,27 +256,27 @@ struct Hasher {
         ++chunk_counter;
         push(out, chunk_counter);
         b3::iv(cv);
-        std::memset(block, 0, 64);
+        for (int i = 0; i < 64; ++i) block[i] = 0;
         block_len = blocks_done = 0;
       }
       if (block_len == 64) {
         uint32_t m[16], out[16];
         words(block, m);
         b3::compress_full(cv, m, chunk_counter, 64, start(), out);
-        std::memcpy(cv, out, 32);
+        copy_bytes(cv, out, 32);
         ++blocks_done;
-        std::memset(block, 0, 64);
+        for (int i = 0; i < 64; ++i) block[i] = 0;
         block_len = 0;
       }
       size_t take = 64 - block_len;
       if (take > len) take = len;
-      std::memcpy(block + block_len, in, take);
+      copy_bytes(block + block_len, in, take);
       block_len += (uint32_t)take;
       in += take;
       len -= take;
     }
   }
-  void finalize(uint8_t out32[32]) const {
+  ZS_HD void finalize(uint8_t out32[32]) const {
     uint32_t m[16], out[16];
     words(block, m);
     uint32_t flags = start() | b3::CHUNK_END;
@@ -268,13 +286,18 @@ struct Hasher {
       b3::compress_full(cv, m, chunk_counter, block_len, flags, out);
       for (unsigned k = depth; k-- > 0;) {
         uint32_t pm[16], key[8];
-        std::memcpy(pm, stack[k], 32);
-        std::memcpy(pm + 8, out, 32);
+        copy_bytes(pm, stack[k], 32);
+        copy_bytes(pm + 8, out, 32);
         b3::iv(key);
         b3::compress_full(key, pm, 0, 64, b3::PARENT | (k == 0 ? b3::ROOT : 0), out);
       }
     }
-    std::memcpy(out32, out, 32);
+    for (int i = 0; i < 8; ++i) {
+      out32[4 * i] = (uint8_t)out[i];
+      out32[4 * i + 1] = (uint8_t)(out[i] >> 8);
+      out32[4 * i + 2] = (uint8_t)(out[i] >> 16);
+      out32[4 * i + 3] = (uint8_t)(out[i] >> 24);
+    }
   }
 };
 

@@ -42,10 +42,12 @@ __device__ __forceinline__ qm31 ld_q(const qm31* p) {
 
 // One fold output per thread, plus its hashQM31 leaf when the folded layer is committed.
 __global__ void __launch_bounds__(kThreads) k_fold(const qm31* __restrict__ in, qm31* __restrict__ out, uint32_t half,
-                                                   qm31 alpha, qm31 off_inv, unsigned layer,
-                                                   const qm31* __restrict__ tabs, uint32_t* leaf_words) {
+                                                   qm31 alpha, const qm31* __restrict__ alpha_dev, qm31 off_inv,
+                                                   unsigned layer, const qm31* __restrict__ tabs,
+                                                   uint32_t* leaf_words) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= half) return;
+  if (alpha_dev) alpha = ld_q(alpha_dev);
   const qm31 y0 = ld_q(in + j), y1 = ld_q(in + j + half);
   const uint64_t k = (uint64_t)j << layer;
   qm31 xinv = qmul(ld_q(tabs + (k & 2047)), ld_q(tabs + 2048 + ((k >> 11) & 2047)));
@@ -66,10 +68,20 @@ __global__ void __launch_bounds__(kThreads) k_fold(const qm31* __restrict__ in, 
 
 void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31& alpha, unsigned layer,
               const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st, bool finish_tree) {
-  k_fold<<<(half + kThreads - 1) / kThreads, kThreads, 0, st>>>(d_in, d_out, half, alpha, tabs.offset_inv(layer), layer,
-                                                                tabs.tables, next_tree ? next_tree->words : nullptr);
+  k_fold<<<(half + kThreads - 1) / kThreads, kThreads, 0, st>>>(d_in, d_out, half, alpha, nullptr,
+                                                                tabs.offset_inv(layer), layer, tabs.tables,
+                                                                next_tree ? next_tree->words : nullptr);
   ZS_CUDA(cudaGetLastError());
   if (next_tree && finish_tree) tree_finish(*next_tree, 0, st);
+}
+
+void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31* d_alpha, unsigned layer,
+              const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st) {
+  k_fold<<<(half + kThreads - 1) / kThreads, kThreads, 0, st>>>(d_in, d_out, half, qzero(), d_alpha,
+                                                                tabs.offset_inv(layer), layer, tabs.tables,
+                                                                next_tree ? next_tree->words : nullptr);
+  ZS_CUDA(cudaGetLastError());
+  if (next_tree) tree_finish(*next_tree, 0, st);
 }
 
 }  // namespace zs

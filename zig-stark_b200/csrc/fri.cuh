@@ -25,5 +25,9 @@ struct FoldTables {
 // finishes it elsewhere), the rest of the folded layer's tree.
 void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31& alpha, unsigned layer,
               const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st, bool finish_tree = true);
+// The same fold with the challenge read from device memory (written there by the
+// device transcript step that precedes it on `st`).
+void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31* d_alpha, unsigned layer,
+              const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st);
 
 }  // namespace zs

@@ -93,22 +93,36 @@ struct FriParamsH {
 
 // Fiat-Shamir channel (channel.zig): one running Blake3 over
 // "zig-stark:channel" || separator || absorbed bytes; sample block k is
-// Blake3(state || "zig-stark:sample" || u64le(k)) and is absorbed back.
+// Blake3(state || "zig-stark:sample" || u64le(k)) and is absorbed back. Usable on the
+// host and, in one thread, on the device (the FRI commit phase runs its transcript
+// steps there); the layout is the same on both sides, so the state is copied across.
+ZS_HD uint32_t m31_from_le(const uint8_t* b) {  // M31.fromBytes (m31.zig:97-100)
+  const uint32_t r = (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
+  return r >= P ? r % P : r;
+}
+
 struct Channel {
   Hasher h;
-  Channel(const void* sep, size_t n) {
+  ZS_HD Channel(const void* sep, size_t n) {
     h.update("zig-stark:channel", 17);
     h.update(sep, n);
   }
   void absorb(const Digest& d) { h.update(d.data(), 32); }
-  void absorb(const qm31& v) {
+  ZS_HD void absorb_bytes(const void* p, size_t n) { h.update(p, n); }
+  ZS_HD void absorb(const qm31& v) {
     const uint32_t w[4] = {v.a.a, v.a.b, v.b.a, v.b.b};
-    h.update(w, 16);
+    uint8_t b[16];
+    for (int i = 0; i < 4; ++i)
+      for (int k = 0; k < 4; ++k) b[4 * i + k] = (uint8_t)(w[i] >> (8 * k));
+    h.update(b, 16);
   }
-  void sample_bytes(uint8_t* out, size_t len) {
+  // `scratch` holds the snapshot of the state (a local copy when null).
+  ZS_HD void sample_bytes(uint8_t* out, size_t len, Hasher* scratch = nullptr) {
     uint64_t counter = 0;
     while (len) {
-      Hasher snap = h;
+      Hasher local;
+      Hasher& snap = scratch ? *scratch : local;
+      snap.snapshot_from(h);
       snap.update("zig-stark:sample", 16);
       uint8_t cb[8];
       for (int i = 0; i < 8; ++i) cb[i] = (uint8_t)(counter >> (8 * i));
@@ -117,16 +131,16 @@ struct Channel {
       snap.finalize(blk);
       h.update(blk, 32);
       const size_t k = len < 32 ? len : 32;
-      std::memcpy(out, blk, k);
+      copy_bytes(out, blk, k);
       out += k;
       len -= k;
       ++counter;
     }
   }
-  qm31 sample_q() {
+  ZS_HD qm31 sample_q(Hasher* scratch = nullptr) {
     uint8_t b[16];
-    sample_bytes(b, 16);
-    return qmake(WireReader::m31(b), WireReader::m31(b + 4), WireReader::m31(b + 8), WireReader::m31(b + 12));
+    sample_bytes(b, 16, scratch);
+    return qmake(m31_from_le(b), m31_from_le(b + 4), m31_from_le(b + 8), m31_from_le(b + 12));
   }
   // channel.zig:79-101.
   uint64_t sample_index(uint64_t n) {

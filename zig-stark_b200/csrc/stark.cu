@@ -172,6 +172,22 @@ struct GatherReq {
   uint32_t words;
   uint32_t out_off;
 };
+// One FRI transcript step on the device (fri.zig:199-206): absorb the layer root,
+// sample the folding challenge. One thread; the snapshot lives in shared memory.
+__global__ void k_fri_transcript(Channel* ch, const uint32_t* __restrict__ root, uint32_t* __restrict__ root_out,
+                                 qm31* __restrict__ alpha) {
+  __shared__ __align__(16) unsigned char snap_raw[sizeof(Hasher)];  // filled by snapshot_from
+  Hasher* snap = reinterpret_cast<Hasher*>(snap_raw);
+  uint8_t b[32];
+  for (int w = 0; w < 8; ++w) {
+    const uint32_t v = root[w];
+    root_out[w] = v;
+    for (int k = 0; k < 4; ++k) b[4 * w + k] = (uint8_t)(v >> (8 * k));
+  }
+  ch->absorb_bytes(b, 32);
+  *alpha = ch->sample_q(snap);
+}
+
 __global__ void k_gather(const GatherReq* __restrict__ reqs, uint32_t count, uint32_t* __restrict__ out) {
   const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= count) return;
@@ -514,14 +530,28 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   std::vector<std::unique_ptr<OwnedTree>> ftrees;
   for (unsigned i = 0; i < L; ++i) ftrees.push_back(std::make_unique<OwnedTree>(lN - i, st));
   if (L > 0) build_qm31_tree(layers[0]->p, ftrees[0]->t, st);
-  std::vector<Digest> froots;
-  for (unsigned i = 0; i < L; ++i) {
-    froots.push_back(root_of(ftrees[i]->t, st));
-    ch.absorb(froots.back());
-    const qm31 alpha = ch.sample_q();
-    const uint32_t half = N >> (i + 1);
-    layers.push_back(std::make_unique<DevBuf<qm31>>(half, st));
-    fri_fold(layers[i]->p, layers[i + 1]->p, half, alpha, i, ftabs, i + 1 < L ? &ftrees[i + 1]->t : nullptr, st);
+  // The commit phase (fri.zig:195-227) runs without host round trips: per layer a
+  // one-thread kernel absorbs the layer's root into the device copy of the transcript
+  // and samples the folding challenge, which the fold reads from device memory.
+  std::vector<Digest> froots(L);
+  if (L > 0) {
+    DevBuf<Channel> d_ch(1, st);
+    h2d_small(d_ch.p, &ch, sizeof(Channel), st);
+    DevBuf<qm31> d_alpha(L, st);
+    DevBuf<uint32_t> d_roots((size_t)8 * L, st);
+    for (unsigned i = 0; i < L; ++i) {
+      k_fri_transcript<<<1, 1, 0, st>>>(d_ch.p, ftrees[i]->t.root(), d_roots.p + 8 * i, d_alpha.p + i);
+      ZS_CUDA(cudaGetLastError());
+      const uint32_t half = N >> (i + 1);
+      layers.push_back(std::make_unique<DevBuf<qm31>>(half, st));
+      fri_fold(layers[i]->p, layers[i + 1]->p, half, d_alpha.p + i, i, ftabs,
+               i + 1 < L ? &ftrees[i + 1]->t : nullptr, st);
+    }
+    d2h_small(&ch, d_ch.p, sizeof(Channel), st);  // the transcript continues on the host
+    std::vector<uint32_t> words((size_t)8 * L);
+    d2h_small(words.data(), d_roots.p, words.size() * sizeof(uint32_t), st);
+    for (unsigned i = 0; i < L; ++i)
+      for (int b = 0; b < 32; ++b) froots[i][b] = (uint8_t)(words[8 * i + b / 4] >> (8 * (b % 4)));
   }
   // remainder (fri.zig:228-233): interpolate the first 2^(remainder_log - log_blowup)
   // points of layer L on the host (at most a few dozen values).
