@@ -38,9 +38,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--log-rows", type=int, default=LOG_ROWS, help="smaller cases for profiling")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="commit", choices=["commit", "batch", "serve"],
-                    help="commit: the circle commit step (default); batch: mixed-size proof batch, "
-                         "batched vs one at a time; serve: Poisson request stream, p50/p99 latency")
+    ap.add_argument("--workload", default="commit", choices=["commit", "prove", "batch", "serve"],
+                    help="commit: the circle commit step (default); prove: single proofs (Fibonacci 2^12, "
+                         "stacked Rescue 2^18); batch: mixed-size proof batch, batched vs one at a time; "
+                         "serve: Poisson request stream, p50/p99 latency")
     ap.add_argument("--jobs", type=int, default=512, help="batch: number of traces")
     ap.add_argument("--log-min", type=int, default=None)
     ap.add_argument("--log-max", type=int, default=None)
@@ -198,6 +199,64 @@ def _cpu_prove_sample(jobs, max_log, count):
             "sample": f"{len(pick)} jobs of the stream with <= 2^{max_log} rows, oracle NTT prover, {dt:.2f} s"}
 
 
+def run_prove(args, world, rank, local):
+    """Single proofs through zs_m31_prove from host buffers, one at a time: the
+    2^12-row Fibonacci AIR (a_1 seeded, blowup 4, 16 queries, separator
+    "zig-stark:fibonacci:example") and stacked Rescue at 2^18 rows (blowup 4)."""
+    import torch
+    from zs_b200 import native, wire
+    from zs_b200 import workload as wl
+    torch.cuda.set_device(local)
+    fib_tr, fib_pi = wl.seeded_fib(12)
+    fib = (wl.AIR_SEEDED_FIB, wire.StarkParams(12, 2, 16, 3).encode(), fib_pi, wire.columns(fib_tr),
+           b"zig-stark:fibonacci:example")
+    cases = {"seeded_fib_2^12": fib,
+             "rescue_stacked_2^18": wl.proof_job(wl.AIR_RESCUE_STACKED, 18, wl.SEED_RESCUE, b"zig-stark:rescue:stacked")}
+    out = {}
+    with ClockSampler(local) as clocks:
+        for name, (air, params, pi, trace, sep) in cases.items():
+            proof = None
+            for _ in range(args.warmup):
+                proof = native.prove(air, params, pi, trace, b"", sep)
+            barrier(world)
+            ts = []
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                p = native.prove(air, params, pi, trace, b"", sep)
+                ts.append(time.perf_counter() - t0)
+            assert p == proof, "proof changed between runs"
+            ms = max_over_ranks(sorted(ts)[len(ts) // 2], world) * 1e3
+            out[name] = {"ms_per_proof_median": ms, "ms_min": min(ts) * 1e3, "proofs_per_s": world * 1e3 / ms,
+                         "proof_bytes": len(proof), "trace_bytes": len(trace)}
+    line = {
+        "metric": "single-proof latency through zs_m31_prove (host buffers in, proof bytes out)",
+        "value": out["rescue_stacked_2^18"]["proofs_per_s"], "unit": "proofs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": out["rescue_stacked_2^18"]["ms_per_proof_median"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31 / QM31 exact)", "data": "synthetic (seeded)",
+        "config": {"workload": "stacked Rescue 2^18 rows (value); SeededFib 2^12 rows also timed; blowup 4, "
+                               "16 queries", "parallelism": f"replicas x{world}"},
+        "cases": out,
+        "e2e": {"value": out["rescue_stacked_2^18"]["proofs_per_s"], "unit": "proofs/s",
+                "h2d_bytes_per_step": out["rescue_stacked_2^18"]["trace_bytes"],
+                "d2h_bytes_per_step": out["rescue_stacked_2^18"]["proof_bytes"]},
+        "roofline": None, "gpu_launches": None, "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        air, params, pi, trace, sep = fib
+        t0 = time.perf_counter()
+        want = oracle.prove(air, params, pi, b"", trace, sep, mode=1)
+        dt = time.perf_counter() - t0
+        got = native.prove(air, params, pi, trace, b"", sep)
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "proofs/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"SeededFib 2^12 proof by the oracle (NTT route), {dt * 1e3:.1f} ms"}
+        line["parity"] = {"seeded_fib_2^12_bytes_equal_oracle": got == want}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_batch(args, world, rank, local):
     """Independent traces (Fibonacci / stacked Rescue 50/50 by seed, log2 rows uniform
     in 10..20, blowup 4, 16 queries, a channel separator per trace), proven batched
@@ -322,8 +381,8 @@ def main():
         run_reference(args, world, rank)
         barrier(world)
         return
-    if args.workload in ("batch", "serve"):
-        (run_batch if args.workload == "batch" else run_serve)(args, world, rank, local)
+    if args.workload in ("prove", "batch", "serve"):
+        {"prove": run_prove, "batch": run_batch, "serve": run_serve}[args.workload](args, world, rank, local)
         barrier(world)
         if world > 1:
             import torch.distributed as dist
