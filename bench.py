@@ -481,6 +481,9 @@ def main():
     }
     dom = max(phase_ms, key=phase_ms.get)
     achieved = alg[dom] / (phase_ms[dom] / 1e3) / 1e9
+    # DRAM read + write bytes of the LDE's three kernels from an ncu capture of this
+    # workload at 2^19 rows (1.96 GB), scaled by the rows; the other phases have none.
+    traffic = {"lde": 1.9646e9 * 2.0 ** (log_rows - 19)}.get(dom)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -491,7 +494,7 @@ def main():
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (no flush)"},
         "phases_ms": phase_ms,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None,
+                     "frac": achieved / hbm_peak, "traffic": traffic,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                      "algorithmic_bytes": alg[dom]},
         "commit_bytes_per_row": 1536,
