@@ -166,10 +166,17 @@ struct Server {
   }
 
   // Each worker proves on its own stream.
+  // Each worker proves on its own streams: proofs with a footprint of at least
+  // kLargeProof bytes on a high-priority stream, so a long proof is not stretched by
+  // the many short ones sharing the device with it (their blocks fill its gaps).
+  static constexpr uint64_t kLargeProof = (uint64_t)1 << 30;
   void loop() {
     cudaSetDevice(device);
-    cudaStream_t st = nullptr;
-    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    int lo_prio = 0, hi_prio = 0;
+    cudaDeviceGetStreamPriorityRange(&lo_prio, &hi_prio);
+    cudaStream_t st_lo = nullptr, st_hi = nullptr;
+    cudaStreamCreateWithPriority(&st_lo, cudaStreamNonBlocking, lo_prio);
+    cudaStreamCreateWithPriority(&st_hi, cudaStreamNonBlocking, hi_prio);
     for (;;) {
       uint64_t ticket;
       Entry* e;
@@ -184,7 +191,7 @@ struct Server {
       budget.acquire(e->job.footprint);
       e->t_start = std::chrono::steady_clock::now();
       std::vector<uint8_t> out;
-      const int32_t rc = run_job(e->job, st, out);
+      const int32_t rc = run_job(e->job, e->job.footprint >= kLargeProof ? st_hi : st_lo, out);
       budget.release(e->job.footprint);
       {
         std::lock_guard<std::mutex> lk(mu);
@@ -195,7 +202,8 @@ struct Server {
       }
       cv_done.notify_all();
     }
-    cudaStreamDestroy(st);
+    cudaStreamDestroy(st_lo);
+    cudaStreamDestroy(st_hi);
   }
 
   // Queues a job; `copy` makes the server's own copy of the caller's buffers.
