@@ -1,4 +1,4 @@
-// Radix-2 decimation-in-time NTT over QM31, computed in the CRT domain.
+// NTTs over QM31 for the low-degree extension, computed in the CRT domain.
 //
 // QM31 = CM31[j]/(j^2 + i), and -i = s^2 with s = 2^15 (1 - i), so
 //   phi: a + b j  ->  (a + b s, a - b s)
@@ -11,9 +11,15 @@
 // results equal the reference's Lagrange interpolation / Horner evaluation value for
 // value (the DFT over the subgroup is invertible in both components).
 //
-// A transform of 2^logN points: a bit-reversed load (with phi), stages 2..2^S inside
-// 2^S-point blocks held in shared memory (S <= 11), then one global pass per larger
-// stage; results leave the CRT domain in the finishing kernels.
+// The LDE: the inverse transform on H runs decimation-in-frequency (natural-order
+// values in, bit-reversed coefficients out), so the zero-padded input of the forward
+// decimation-in-time transform is written contiguously and its output is in natural
+// order; neither needs a separate bit-reversal pass. Each transform is one pass over
+// contiguous 2^11-element blocks plus passes of up to 11 stages over strided groups,
+// two stages per shared-memory round trip; results leave the CRT domain in the
+// finishing kernels.
+#include <vector>
+
 #include "ntt.cuh"
 
 namespace zs {
@@ -92,72 +98,123 @@ NttTables::~NttTables() {
   cudaFreeAsync(inv_crt, st);
 }
 
-// dst[bitrev(i)] = phi(src[i]), i < 2^logN.
-__global__ void k_bitrev_load(const qm31* __restrict__ src, size_t s_stride, qm31* __restrict__ dst, size_t d_stride,
-                              unsigned logN) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (1u << logN)) return;
-  const qm31* s = src + (size_t)blockIdx.y * s_stride;
-  qm31* d = dst + (size_t)blockIdx.y * d_stride;
-  stq(d + bitrev(i, logN), to_crt(ldq(s + i)));
+// Two stages (b, b + 1) on the four elements m0 + {0, 1, 2, 3} * 2^b of each group in
+// shared memory (see k_ntt_pass), one quadruple per thread iteration, then a barrier.
+template <bool DIF>
+__device__ __forceinline__ void ntt_radix4(qm31* s, unsigned M, uint32_t G, unsigned lo, unsigned logN, uint32_t l0,
+                                           unsigned b, const qm31* __restrict__ tw) {
+  const uint32_t hb = 1u << b, total = G << M;
+  const unsigned st = lo + 1 + b;
+  for (uint32_t q = threadIdx.x; q < (total >> 2); q += blockDim.x) {
+    const uint32_t t = q >> (M - 2), r = q & ((1u << (M - 2)) - 1);
+    const uint32_t m0 = ((r >> b) << (b + 2)) | (r & (hb - 1));
+    const uint32_t k = ((m0 & (hb - 1)) << lo) | (l0 + t);
+    const qm31 t1 = ldq(tw + ((size_t)k << (logN - st)));
+    const qm31 t2a = ldq(tw + ((size_t)k << (logN - st - 1)));
+    const qm31 t2b = ldq(tw + ((size_t)(k + (hb << lo)) << (logN - st - 1)));
+    qm31* p = s + (t << M) + m0;
+    qm31 e0 = p[0], e1 = p[hb], e2 = p[2 * hb], e3 = p[3 * hb];
+    if (!DIF) {
+      qm31 u = crt_mul(t1, e1);
+      e1 = crt_sub(e0, u), e0 = crt_add(e0, u);
+      u = crt_mul(t1, e3);
+      e3 = crt_sub(e2, u), e2 = crt_add(e2, u);
+      u = crt_mul(t2a, e2);
+      e2 = crt_sub(e0, u), e0 = crt_add(e0, u);
+      u = crt_mul(t2b, e3);
+      e3 = crt_sub(e1, u), e1 = crt_add(e1, u);
+    } else {
+      qm31 d = crt_sub(e0, e2);
+      e0 = crt_add(e0, e2), e2 = crt_mul(d, t2a);
+      d = crt_sub(e1, e3);
+      e1 = crt_add(e1, e3), e3 = crt_mul(d, t2b);
+      d = crt_sub(e0, e1);
+      e0 = crt_add(e0, e1), e1 = crt_mul(d, t1);
+      d = crt_sub(e2, e3);
+      e2 = crt_add(e2, e3), e3 = crt_mul(d, t1);
+    }
+    p[0] = e0, p[hb] = e1, p[2 * hb] = e2, p[3 * hb] = e3;
+  }
+  __syncthreads();
 }
 
-// Stages first..S (len 2^first..2^S) inside 2^S-point blocks, CRT domain.
-__global__ void __launch_bounds__(kThreads) k_ntt_smem(qm31* a, size_t stride, unsigned logN, unsigned first,
-                                                       unsigned S, const qm31* __restrict__ tw) {
+// One stage b on the pairs m0 + {0, 1} * 2^b, then a barrier.
+template <bool DIF>
+__device__ __forceinline__ void ntt_radix2(qm31* s, unsigned M, uint32_t G, unsigned lo, unsigned logN, uint32_t l0,
+                                           unsigned b, const qm31* __restrict__ tw) {
+  const uint32_t hb = 1u << b, total = G << M;
+  const unsigned st = lo + 1 + b;
+  for (uint32_t q = threadIdx.x; q < (total >> 1); q += blockDim.x) {
+    const uint32_t t = q >> (M - 1), r = q & ((1u << (M - 1)) - 1);
+    const uint32_t m0 = ((r >> b) << (b + 1)) | (r & (hb - 1));
+    const uint32_t k = ((m0 & (hb - 1)) << lo) | (l0 + t);
+    const qm31 tv = ldq(tw + ((size_t)k << (logN - st)));
+    qm31* p = s + (t << M) + m0;
+    const qm31 x = p[0], y = p[hb];
+    if (!DIF) {
+      const qm31 u = crt_mul(tv, y);
+      p[0] = crt_add(x, u);
+      p[hb] = crt_sub(x, u);
+    } else {
+      p[0] = crt_add(x, y);
+      p[hb] = crt_mul(crt_sub(x, y), tv);
+    }
+  }
+  __syncthreads();
+}
+
+// x[i] = phi(x[i]) for the elements of C columns (count each), out of place allowed.
+__global__ void k_to_crt_cols(const qm31* in, size_t in_stride, qm31* out, size_t out_stride, uint32_t count) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < count)
+    stq(out + (size_t)blockIdx.y * out_stride + k, to_crt(ldq(in + (size_t)blockIdx.y * in_stride + k)));
+}
+
+// One pass of radix-2/4 butterflies over groups held in shared memory. Global index
+// j = (hi << (lo + M)) | (mid << lo) | l with mid < 2^M: a CTA holds the 2^M elements of
+// G consecutive l values (one hi), s[t * 2^M + mid], so global stage lo + 1 + b pairs
+// mid values that differ in bit b. lo = 0 with G = 1 is a contiguous 2^M block.
+// The twiddle of the lower element j at stage st is tw[(j mod 2^(st-1)) << (logN - st)]
+// in both directions:
+//   DIT (bit-reversed in, natural out), stages ascending:  x, y -> x + t y, x - t y;
+//   DIF (natural in, bit-reversed out), stages descending: x, y -> x + y, (x - y) t.
+// Local stages [b_lo, b_hi) run two at a time (four elements per thread in registers)
+// with a barrier per pair. `src`, when given, is read instead of `a` (QM31 values,
+// mapped into the CRT domain) and the pass writes `a`.
+template <bool DIF>
+__global__ void __launch_bounds__(kThreads) k_ntt_pass(qm31* a, size_t stride, const qm31* __restrict__ src,
+                                                       size_t src_stride, unsigned logN, unsigned lo, unsigned M,
+                                                       unsigned G, unsigned b_lo, unsigned b_hi,
+                                                       const qm31* __restrict__ tw) {
   extern __shared__ uint4 smem_raw[];
   qm31* s = reinterpret_cast<qm31*>(smem_raw);
-  const uint32_t B = 1u << S;
-  qm31* col = a + (size_t)blockIdx.y * stride + (size_t)blockIdx.x * B;
-  for (uint32_t i = threadIdx.x; i < B; i += blockDim.x) s[i] = ldq(col + i);
-  __syncthreads();
-  for (unsigned st = first; st <= S; ++st) {
-    const uint32_t half = 1u << (st - 1);
-    for (uint32_t b = threadIdx.x; b < (B >> 1); b += blockDim.x) {
-      const uint32_t k = b & (half - 1);
-      const uint32_t j = ((b >> (st - 1)) << st) + k;
-      const qm31 t = crt_mul(ldq(tw + ((size_t)k << (logN - st))), s[j + half]);
-      const qm31 u = s[j];
-      s[j] = crt_add(u, t);
-      s[j + half] = crt_sub(u, t);
-    }
-    __syncthreads();
-  }
-  for (uint32_t i = threadIdx.x; i < B; i += blockDim.x) stq(col + i, s[i]);
-}
-
-// Stages lo+1..lo+M in one pass: index j = (hi << (lo + M)) | (mid << lo) | l with
-// mid < 2^M; a CTA holds the 2^M elements of G consecutive l values (one hi) in shared
-// memory, so a stage's butterflies pair mid values that differ in one bit. The twiddle
-// of the lower element j at stage lo + 1 + b is tw[(j mod 2^(lo + b)) << (logN - lo - 1 - b)].
-__global__ void __launch_bounds__(kThreads) k_ntt_strided(qm31* a, size_t stride, unsigned logN, unsigned lo,
-                                                          unsigned M, unsigned G, const qm31* __restrict__ tw) {
-  extern __shared__ uint4 smem_raw[];
-  qm31* s = reinterpret_cast<qm31*>(smem_raw);  // s[t * 2^M + mid]
-  const uint32_t lcount = 1u << lo, gpl = lcount / G;  // CTAs per hi value
+  const uint32_t gpl = (1u << lo) / G;  // CTAs per hi value
   const uint32_t hi = blockIdx.x / gpl, l0 = (blockIdx.x % gpl) * G;
-  qm31* col = a + (size_t)blockIdx.y * stride + ((size_t)hi << (lo + M)) + l0;
+  const size_t off = ((size_t)hi << (lo + M)) + l0;
+  qm31* col = a + (size_t)blockIdx.y * stride + off;
   const uint32_t total = G << M;
   const unsigned lg_g = 31 - __clz(G);
-  for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const uint32_t t = idx & (G - 1), mid = idx >> lg_g;
-    s[(t << M) + mid] = ldq(col + ((size_t)mid << lo) + t);
+  if (src) {
+    const qm31* in = src + (size_t)blockIdx.y * src_stride + off;
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), mid = idx >> lg_g;
+      s[(t << M) + mid] = to_crt(ldq(in + ((size_t)mid << lo) + t));
+    }
+  } else {
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), mid = idx >> lg_g;
+      s[(t << M) + mid] = ldq(col + ((size_t)mid << lo) + t);
+    }
   }
   __syncthreads();
-  for (unsigned b = 0; b < M; ++b) {
-    const unsigned st = lo + 1 + b;
-    const uint32_t half = 1u << b;
-    for (uint32_t q = threadIdx.x; q < (total >> 1); q += blockDim.x) {
-      const uint32_t t = q >> (M - 1), r = q & ((1u << (M - 1)) - 1);
-      const uint32_t m0 = ((r >> b) << (b + 1)) | (r & (half - 1));
-      const uint32_t k = ((m0 & (half - 1)) << lo) | (l0 + t);
-      qm31* p = s + (t << M) + m0;
-      const qm31 tv = crt_mul(ldq(tw + ((size_t)k << (logN - st))), p[half]);
-      const qm31 u = p[0];
-      p[0] = crt_add(u, tv);
-      p[half] = crt_sub(u, tv);
-    }
-    __syncthreads();
+  if (!DIF) {
+    unsigned b = b_lo;
+    for (; b + 1 < b_hi; b += 2) ntt_radix4<false>(s, M, G, lo, logN, l0, b, tw);
+    if (b < b_hi) ntt_radix2<false>(s, M, G, lo, logN, l0, b, tw);
+  } else {
+    int b = (int)b_hi - 1;
+    for (; b - 1 >= (int)b_lo; b -= 2) ntt_radix4<true>(s, M, G, lo, logN, l0, (unsigned)(b - 1), tw);
+    if (b >= (int)b_lo) ntt_radix2<true>(s, M, G, lo, logN, l0, (unsigned)b, tw);
   }
   for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const uint32_t t = idx & (G - 1), mid = idx >> lg_g;
@@ -175,62 +232,88 @@ __global__ void k_from_crt(qm31* a, size_t stride, uint32_t n, unsigned shift) {
   stq(p, v);
 }
 
-// Stages first..logN of a transform whose stages below `first` are done: one
-// shared-memory pass over 2^11-point blocks, then passes of up to 11 stages over
-// strided groups (at most 4096 elements, 64 KB, per CTA).
-static void run_stages(qm31* a, size_t stride, uint32_t C, unsigned logN, const qm31* tw, cudaStream_t st,
-                       unsigned first = 1) {
-  if (logN == 0 || first > logN) return;
+// The passes of a size-2^logN transform: one over contiguous 2^S-element blocks
+// (S = min(logN, 11), stages 1..S) and passes of up to 11 stages over strided groups
+// (at most 4096 elements, 64 KB, per CTA) for stages S+1..logN.
+struct PassPlan {
+  unsigned lo, M;
+  uint32_t G;
+};
+static std::vector<PassPlan> plan_passes(unsigned logN) {
+  std::vector<PassPlan> v;
   const unsigned S = logN < kSmemLog ? logN : kSmemLog;
-  if (first <= S) {
-    const uint32_t B = 1u << S;
-    k_ntt_smem<<<dim3((1u << logN) / B, C), kThreads, B * sizeof(qm31), st>>>(a, stride, logN, first, S, tw);
-  }
-  unsigned lo = S > first - 1 ? S : first - 1;
+  v.push_back({0, S, 1});
+  unsigned lo = S;
   while (lo < logN) {
     const unsigned rem = logN - lo, passes = (rem + kSmemLog - 1) / kSmemLog;
     const unsigned M = (rem + passes - 1) / passes;
     uint32_t G = 4096u >> M;
     if (G < 2) G = 2;
     if (G > (1u << lo)) G = 1u << lo;
-    const size_t sb = ((size_t)G << M) * sizeof(qm31);
-    const uint32_t ctas = (1u << (logN - M)) / G;
-    ZS_CUDA(cudaFuncSetAttribute(k_ntt_strided, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
-    k_ntt_strided<<<dim3(ctas, C), kThreads, sb, st>>>(a, stride, logN, lo, M, G, tw);
+    v.push_back({lo, M, G});
     lo += M;
+  }
+  return v;
+}
+
+template <bool DIF>
+static void launch_pass(qm31* a, size_t stride, const qm31* src, size_t src_stride, uint32_t C, unsigned logN,
+                        const PassPlan& p, unsigned b_lo, unsigned b_hi, const qm31* tw, cudaStream_t st) {
+  const size_t sb = ((size_t)p.G << p.M) * sizeof(qm31);
+  ZS_CUDA(cudaFuncSetAttribute(k_ntt_pass<DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
+  const uint32_t ctas = (1u << (logN - p.M)) / p.G;
+  k_ntt_pass<DIF><<<dim3(ctas, C), kThreads, sb, st>>>(a, stride, src, src_stride, logN, p.lo, p.M, p.G, b_lo, b_hi,
+                                                       tw);
+}
+
+// Forward DIT stages first..logN (bit-reversed input in `a`, natural output).
+static void dit_stages(qm31* a, size_t stride, uint32_t C, unsigned logN, const qm31* tw, cudaStream_t st,
+                       unsigned first) {
+  if (logN == 0 || first > logN) return;
+  for (const PassPlan& p : plan_passes(logN)) {
+    const unsigned s_lo = p.lo + 1, s_hi = p.lo + p.M;  // global stages of this pass
+    if (s_hi < first) continue;
+    const unsigned b_lo = first > s_lo ? first - s_lo : 0;
+    launch_pass<false>(a, stride, nullptr, 0, C, logN, p, b_lo, p.M, tw, st);
   }
   ZS_CUDA(cudaGetLastError());
 }
 
-void ntt(const qm31* in, qm31* out, size_t stride, uint32_t C, const NttTables& t, bool inverse, cudaStream_t st) {
-  const unsigned logN = t.log_n;
-  const uint32_t N = 1u << logN;
-  if (in == out) throw Error(ZS_EGENERIC, "ntt: in-place transform needs a separate buffer for the bit reversal");
-  k_bitrev_load<<<dim3((N + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(in, stride, out, stride, logN);
-  run_stages(out, stride, C, logN, inverse ? t.inv_crt : t.fwd_crt, st);
-  k_from_crt<<<dim3((N + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(out, stride, N,
-                                                                          inverse ? (31 - logN) % 31 : 0);
+// Inverse DIF over all stages: natural-order QM31 values in `src` (mapped into the CRT
+// domain by the first pass), bit-reversed CRT-domain output in `a`.
+static void dif_all(const qm31* src, size_t src_stride, qm31* a, size_t stride, uint32_t C, unsigned logN,
+                    const qm31* tw, cudaStream_t st) {
+  if (logN == 0) {
+    k_to_crt_cols<<<dim3(1, C), 32, 0, st>>>(src, src_stride, a, stride, 1);
+    ZS_CUDA(cudaGetLastError());
+    return;
+  }
+  const std::vector<PassPlan> plan = plan_passes(logN);
+  for (size_t i = plan.size(); i-- > 0;)
+    launch_pass<true>(a, stride, i + 1 == plan.size() ? src : nullptr, src_stride, C, logN, plan[i], 0, plan[i].M,
+                      tw, st);
   ZS_CUDA(cudaGetLastError());
 }
 
-// coeffs[c][k] = phi^-1 of the scaled inverse-transform result (in place), and
-// v = phi(coeffs[c][k] * offset^k) for k < n goes to the bit-reversed input of the
-// size-N forward transform. That input is zero except at position bitrev_N(k) =
-// bitrev_n(k) << B, so its first B stages only copy v across the 2^B-element block
-// (each stage pairs a filled element with a zero one): the block is written as 2^B
-// copies of v and the forward transform starts at stage B + 1. offset_crt[k] = phi(offset^k).
+// The inverse DIF leaves phi(n c_k) at position j = bitrev_n(k). For each j:
+// coeffs[c][j] = c_k (QM31, kept in bit-reversed order), and the forward input
+// phi(c_k offset^k) goes to position bitrev_N(k) = j << B of the size-N transform. That
+// input is zero elsewhere, so its first B stages only copy the value across the 2^B
+// block at j << B (each stage pairs a filled element with a zero one): the block is
+// written as 2^B copies and the forward transform starts at stage B + 1.
+// offset_crt[k] = phi(offset^k).
 __global__ void k_coeff_finish(qm31* coeffs, size_t c_stride, qm31* big, size_t b_stride, unsigned log_n,
                                unsigned log_N, const qm31* __restrict__ offset_crt) {
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= (1u << log_n)) return;
-  qm31* cp = coeffs + (size_t)blockIdx.y * c_stride + k;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (1u << log_n)) return;
+  qm31* cp = coeffs + (size_t)blockIdx.y * c_stride + j;
   qm31 v = ldq(cp);
   const unsigned sh = (31 - log_n) % 31;
   v = qmake(mshl(v.a.a, sh), mshl(v.a.b, sh), mshl(v.b.a, sh), mshl(v.b.b, sh));
   stq(cp, from_crt(v));
-  const qm31 w = crt_mul(v, ldq(offset_crt + k));
+  const qm31 w = crt_mul(v, ldq(offset_crt + bitrev(j, log_n)));
   const unsigned B = log_N - log_n;
-  qm31* dst = big + (size_t)blockIdx.y * b_stride + ((size_t)bitrev(k, log_n) << B);
+  qm31* dst = big + (size_t)blockIdx.y * b_stride + ((size_t)j << B);
   for (uint32_t r = 0; r < (1u << B); ++r) stq(dst + r, w);
 }
 
@@ -238,10 +321,8 @@ void lde_qm31(const qm31* values, size_t v_stride, qm31* coeffs, size_t c_stride
               uint32_t C, const NttTables& small, const NttTables& big, const qm31* offset_pows, cudaStream_t st) {
   const unsigned log_n = small.log_n, log_N = big.log_n;
   const uint32_t n = 1u << log_n, N = 1u << log_N;
-  // inverse transform on H (bit-reversed load into the CRT domain, stages)
-  k_bitrev_load<<<dim3((n + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(values, v_stride, coeffs, c_stride,
-                                                                             log_n);
-  run_stages(coeffs, c_stride, C, log_n, small.inv_crt, st);
+  // inverse transform on H: natural-order values in, bit-reversed CRT-domain n c_k out
+  dif_all(values, v_stride, coeffs, c_stride, C, log_n, small.inv_crt, st);
   // scale by 1/n, leave the CRT domain for the coefficients, and fill the forward
   // input after its first log_N - log_n stages
   qm31* off_crt = nullptr;
@@ -250,7 +331,7 @@ void lde_qm31(const qm31* values, size_t v_stride, qm31* coeffs, size_t c_stride
   k_coeff_finish<<<dim3((n + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(coeffs, c_stride, codeword, w_stride,
                                                                               log_n, log_N, off_crt);
   ZS_CUDA(cudaFreeAsync(off_crt, st));
-  run_stages(codeword, w_stride, C, log_N, big.fwd_crt, st, log_N - log_n + 1);
+  dit_stages(codeword, w_stride, C, log_N, big.fwd_crt, st, log_N - log_n + 1);
   k_from_crt<<<dim3((N + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(codeword, w_stride, N, 0);
   ZS_CUDA(cudaGetLastError());
 }

@@ -20,13 +20,10 @@ struct NttTables {
   NttTables& operator=(const NttTables&) = delete;
 };
 
-// out[c][i] = sum_k in[c][k] * w^(i k) (forward) or n^-1 sum_k in[c][k] w^-(i k)
-// (inverse), C columns of 2^log_n values, `stride` elements apart. In place allowed.
-void ntt(const qm31* in, qm31* out, size_t stride, uint32_t C, const NttTables& t, bool inverse, cudaStream_t st);
-
 // Low-degree extension of C columns of 2^log_n trace values (natural order on
 // H = <w_n>) to 2^log_N evaluations on D = offset * <w_N> (natural order), keeping the
-// coefficients: coeffs[c] = interpolation of values[c] on H; codeword[c][i] = f_c(d_i).
+// coefficients in bit-reversed order: coeffs[c][j] = coefficient bitrev(j) of the
+// interpolation of values[c] on H; codeword[c][i] = f_c(d_i).
 // offset_pows: offset^k for k < 2^log_n.
 void lde_qm31(const qm31* values, size_t v_stride, qm31* coeffs, size_t c_stride, qm31* codeword, size_t w_stride,
               uint32_t C, const NttTables& small, const NttTables& big, const qm31* offset_pows, cudaStream_t st);

@@ -108,14 +108,15 @@ __global__ void k_scan_add(qm31* out, uint32_t n, const qm31* block_prefix) {
   if (i < n && blockIdx.x > 0) stq(out + i, qadd(ldq(out + i), ldq(block_prefix + blockIdx.x)));
 }
 
-// partial[pt][col][blk] = sum over the block's k of coeffs[col][k] * zpow[pt][k].
-__global__ void __launch_bounds__(kT) k_eval_partial(const qm31* __restrict__ coeffs, uint32_t n,
+// partial[pt][col][blk] = sum over the block's j of coeffs[col][j] * zpow[pt][bitrev(j)]
+// (the coefficients are stored in bit-reversed order, log_n = log2 n).
+__global__ void __launch_bounds__(kT) k_eval_partial(const qm31* __restrict__ coeffs, uint32_t n, unsigned log_n,
                                                      const qm31* __restrict__ zpow, uint32_t npt, qm31* partial) {
   __shared__ qm31 s[kT];
   const uint32_t col = blockIdx.y, pt = blockIdx.z;
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   qm31 v = qzero();
-  if (k < n) v = qmul(ldq(coeffs + (size_t)col * n + k), ldq(zpow + (size_t)pt * n + k));
+  if (j < n) v = qmul(ldq(coeffs + (size_t)col * n + j), ldq(zpow + (size_t)pt * n + bitrev(j, log_n)));
   s[threadIdx.x] = v;
   __syncthreads();
   for (uint32_t d = blockDim.x / 2; d > 0; d >>= 1) {
@@ -495,7 +496,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     qm31_powers(wz, zpow.p + n, n, st);
     const uint32_t nblk = (n + kT - 1) / kT;
     DevBuf<qm31> partial((size_t)2 * ncol * nblk, st), sums((size_t)2 * ncol, st);
-    k_eval_partial<<<dim3(nblk, ncol, 2), kT, 0, st>>>(coeffs.p, n, zpow.p, 2, partial.p);
+    k_eval_partial<<<dim3(nblk, ncol, 2), kT, 0, st>>>(coeffs.p, n, tl, zpow.p, 2, partial.p);
     k_eval_sum<<<(2 * ncol + 63) / 64, 64, 0, st>>>(partial.p, nblk, 2 * ncol, sums.p);
     ZS_CUDA(cudaGetLastError());
     std::vector<qm31> hs(2 * ncol);
