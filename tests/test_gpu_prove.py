@@ -113,3 +113,16 @@ def test_rescue_stacked_full_size(orc):
     """2^18 rows of stacked Rescue permutations (2^15 of them) at blowup 4."""
     tr, pi = wl.rescue_stacked(18)
     _check(orc, wl.AIR_RESCUE_STACKED, wire.StarkParams(18, 2, 16, 3), pi, tr, sep=b"zig-stark:rescue:example")
+
+
+def test_packed_upload_paths(orc):
+    """Traces of 4 MiB or more cross PCIe packed (the low word of each element): an M31
+    column with raw words at and above p (reduced like M31.fromBytes) next to a column of
+    general QM31 values (uploaded whole again), against the oracle."""
+    rng = np.random.default_rng(17)
+    n = 1 << 17
+    m31_col = np.zeros((n, 4), dtype=np.uint32)
+    m31_col[:, 0] = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)  # some >= p
+    m31_col[:4, 0] = [wl.P, wl.P + 1, 2**32 - 1, 0]
+    qm_col = rng.integers(0, wl.P, (n, 4), dtype=np.uint32)
+    _check(orc, wl.AIR_FIB, wire.StarkParams(17, 1, 8, 3), wire.qm31((1, 2, 3, 4)), [m31_col, qm_col], valid=False)

@@ -238,4 +238,39 @@ void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   }
 }
 
+void upload_low_words(uint32_t* dst, const uint8_t* const* cols, uint32_t C, size_t n, uint8_t* high,
+                      cudaStream_t st) {
+  Stager* sg = t_slot ? &t_slot->stager : nullptr;
+  if (!sg || !sg->ok) throw Error(ZS_EGENERIC, "upload_low_words needs pinned staging");
+  HostPool& pool = HostPool::get();
+  const size_t parts = pool.width();
+  const size_t per_chunk = kChunk / 4;  // elements per staging buffer
+  std::vector<uint8_t> part_high(parts);
+  for (uint32_t j = 0; j < C; ++j) {
+    high[j] = 0;
+    for (size_t off = 0; off < n; off += per_chunk) {
+      const size_t len = std::min(per_chunk, n - off);
+      const int b = (int)(sg->next++ & 1);
+      ZS_CUDA(cudaEventSynchronize(sg->ev[b]));
+      uint32_t* pin = static_cast<uint32_t*>(sg->buf[b]);
+      const uint8_t* src = cols[j] + 16 * off;
+      const size_t piece = (len + parts - 1) / parts;
+      pool.run(parts, [&](size_t i) {
+        const size_t a = std::min(len, i * piece), e = std::min(len, a + piece);
+        uint32_t acc = 0;
+        for (size_t k = a; k < e; ++k) {
+          uint32_t w[4];
+          std::memcpy(w, src + 16 * k, 16);
+          pin[k] = w[0];
+          acc |= w[1] | w[2] | w[3];
+        }
+        part_high[i] = acc != 0;
+      });
+      for (size_t i = 0; i < parts; ++i) high[j] |= part_high[i];
+      ZS_CUDA(cudaMemcpyAsync(dst + (size_t)j * n + off, pin, len * 4, cudaMemcpyHostToDevice, st));
+      ZS_CUDA(cudaEventRecord(sg->ev[b], st));
+    }
+  }
+}
+
 }  // namespace zs

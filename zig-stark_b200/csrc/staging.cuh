@@ -16,6 +16,14 @@ namespace zs {
 // `st`. Returns once `src` may be reused; the device copy completes in stream order.
 void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st);
 
+// Uploads the low 32-bit word of every 16-byte element of C columns (column j: n
+// elements at cols[j]) to dst (column j at dst + j * n), packing on the host so a
+// QM31-embedded M31 column crosses PCIe at a quarter of its wire size. high[j] is set
+// when some element of column j has a non-zero word among its upper three (that
+// column's packed words are then incomplete and the caller uploads it whole).
+void upload_low_words(uint32_t* dst, const uint8_t* const* cols, uint32_t C, size_t n, uint8_t* high,
+                      cudaStream_t st);
+
 // The small transfers of a proof (constants, roots, evaluations, query reveals) go
 // through pinned memory too: a pageable copy takes the driver's staging path, on which
 // concurrent provers would queue behind one another's uploads.

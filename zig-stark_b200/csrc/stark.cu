@@ -266,13 +266,44 @@ __global__ void k_from_wire(const uint32_t* __restrict__ raw, uint32_t* __restri
   out[i] = v;
 }
 
+// wire words of an M31 -> canonical QM31 (v, 0, 0, 0); raw < 2^32 <= 2p + 2
+__global__ void k_from_low(const uint32_t* __restrict__ low, qm31* __restrict__ out, uint64_t count) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t v = low[i];
+  v = v >= P ? v - P : v;
+  v = v >= P ? v - P : v;
+  reinterpret_cast<uint4*>(out)[i] = make_uint4(v, 0, 0, 0);
+}
+
 // Copies the columns of `c` (each of n elements) to dst (column k at dst + k * n) and
-// reduces them: the span of the caller's buffer that holds all columns goes over in
-// one upload, and a kernel drops the length prefixes between the columns.
+// reduces them. Large traces cross PCIe packed: the low word of every element, with the
+// columns whose upper words are not all zero (true QM31 values) uploaded again whole.
+// Small ones go as the span of the caller's buffer that holds all columns in one upload,
+// and a kernel drops the length prefixes between the columns.
+constexpr size_t kPackMin = (size_t)4 << 20;  // wire bytes from which packing pays
 void upload_columns(const WireColumns& c, qm31* dst, uint32_t n, cudaStream_t st) {
   if (c.size() == 0) return;
-  const uint64_t col_words = (uint64_t)4 * n, count = col_words * c.size();
+  const uint32_t C = (uint32_t)c.size();
+  const uint64_t col_words = (uint64_t)4 * n, count = col_words * C;
   const size_t span = (size_t)(c.data.back() - c.data.front()) + (size_t)16 * n;
+  if (span >= kPackMin) {
+    DevBuf<uint32_t> low((size_t)C * n, st);
+    std::vector<uint8_t> high(C);
+    upload_low_words(low.p, c.data.data(), C, n, high.data(), st);
+    const uint64_t elems = (uint64_t)C * n;
+    k_from_low<<<(unsigned)((elems + 255) / 256), 256, 0, st>>>(low.p, dst, elems);
+    ZS_CUDA(cudaGetLastError());
+    for (uint32_t j = 0; j < C; ++j) {
+      if (!high[j]) continue;
+      DevBuf<uint32_t> raw(col_words, st);
+      upload_bytes(raw.p, c.data[j], (size_t)16 * n, st);
+      k_from_wire<<<(unsigned)((col_words + 255) / 256), 256, 0, st>>>(raw.p, reinterpret_cast<uint32_t*>(dst + (size_t)j * n),
+                                                                       col_words, col_words);
+      ZS_CUDA(cudaGetLastError());
+    }
+    return;
+  }
   DevBuf<uint32_t> raw((span + 3) / 4, st);
   upload_bytes(raw.p, c.data.front(), span, st);
   k_from_wire<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(raw.p, reinterpret_cast<uint32_t*>(dst), col_words,
