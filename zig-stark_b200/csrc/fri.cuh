@@ -30,4 +30,25 @@ void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31& alpha, u
 void fri_fold(const qm31* d_in, qm31* d_out, uint32_t half, const qm31* d_alpha, unsigned layer,
               const FoldTables& tabs, DeviceTree* next_tree, cudaStream_t st);
 
+// The small layers of the commit phase in one CTA (fri.zig:195-227): for layers
+// first .. first + count - 1 (the first holding at most kTailMax values): commit the
+// layer (hashQM31 leaves and the whole tree), absorb its root into the device
+// transcript `ch` and sample the folding challenge, fold into the next layer. Every
+// step is a barrier apart, so the chain of small dependent steps costs no launches.
+constexpr uint32_t kTailMax = 1024;
+constexpr uint32_t kTailLayers = 16;
+struct FriTail {
+  uint32_t first, count;  // absolute index of the first layer, layers handled
+  unsigned log_size;      // log2 of the first layer's length
+  const qm31* tables;     // FoldTables::tables
+  qm31 off_inv[kTailLayers];
+  qm31* layer[kTailLayers + 1];  // layer[c] has 2^(log_size - c) values; the last is only written
+  uint32_t* tree[kTailLayers];   // DeviceTree words of layer c
+  uint32_t* roots;               // 8 words per handled layer
+  qm31* alphas;                  // one per handled layer
+};
+struct Channel;
+// Launch with one CTA of kTailMax / 4 threads; `ft` and `ch` are in device memory.
+void fri_tail(const FriTail* ft, Channel* ch, cudaStream_t st);
+
 }  // namespace zs

@@ -159,6 +159,18 @@ struct Channel {
   }
 };
 
+#ifdef __CUDACC__
+// Block-cooperative copy of a transcript state between global and shared memory (the
+// single-thread transcript steps run on the shared copy: byte-wise state updates cost
+// far less there than in global memory).
+__device__ __forceinline__ void copy_state(void* dst, const void* src, size_t bytes) {
+  uint2* d = static_cast<uint2*>(dst);
+  const uint2* s = static_cast<const uint2*>(src);
+  for (size_t i = threadIdx.x; i < bytes / 8; i += blockDim.x) d[i] = s[i];
+}
+static_assert(sizeof(Channel) % 8 == 0, "the transcript state is copied in 8-byte words");
+#endif
+
 // Lagrange interpolation through (xs[i], ys[i]), the reference's own O(n^2)
 // algorithm (univariate.zig:79-139); used on <= 8 points (AIR constants, the FRI
 // remainder).

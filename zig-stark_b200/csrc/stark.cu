@@ -174,19 +174,27 @@ struct GatherReq {
   uint32_t out_off;
 };
 // One FRI transcript step on the device (fri.zig:199-206): absorb the layer root,
-// sample the folding challenge. One thread; the snapshot lives in shared memory.
+// sample the folding challenge. One warp copies the state to shared memory and back;
+// one thread runs the step there.
 __global__ void k_fri_transcript(Channel* ch, const uint32_t* __restrict__ root, uint32_t* __restrict__ root_out,
                                  qm31* __restrict__ alpha) {
+  __shared__ __align__(16) unsigned char ch_raw[sizeof(Channel)];
   __shared__ __align__(16) unsigned char snap_raw[sizeof(Hasher)];  // filled by snapshot_from
-  Hasher* snap = reinterpret_cast<Hasher*>(snap_raw);
-  uint8_t b[32];
-  for (int w = 0; w < 8; ++w) {
-    const uint32_t v = root[w];
-    root_out[w] = v;
-    for (int k = 0; k < 4; ++k) b[4 * w + k] = (uint8_t)(v >> (8 * k));
+  copy_state(ch_raw, ch, sizeof(Channel));
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Channel* c = reinterpret_cast<Channel*>(ch_raw);
+    uint8_t b[32];
+    for (int w = 0; w < 8; ++w) {
+      const uint32_t v = root[w];
+      root_out[w] = v;
+      for (int k = 0; k < 4; ++k) b[4 * w + k] = (uint8_t)(v >> (8 * k));
+    }
+    c->absorb_bytes(b, 32);
+    *alpha = c->sample_q(reinterpret_cast<Hasher*>(snap_raw));
   }
-  ch->absorb_bytes(b, 32);
-  *alpha = ch->sample_q(snap);
+  __syncthreads();
+  copy_state(ch, ch_raw, sizeof(Channel));
 }
 
 __global__ void k_gather(const GatherReq* __restrict__ reqs, uint32_t count, uint32_t* __restrict__ out) {
@@ -561,23 +569,46 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   FoldTables ftabs(lN, st);
   std::vector<std::unique_ptr<OwnedTree>> ftrees;
   for (unsigned i = 0; i < L; ++i) ftrees.push_back(std::make_unique<OwnedTree>(lN - i, st));
-  if (L > 0) build_qm31_tree(layers[0]->p, ftrees[0]->t, st);
   // The commit phase (fri.zig:195-227) runs without host round trips: per layer a
   // one-thread kernel absorbs the layer's root into the device copy of the transcript
-  // and samples the folding challenge, which the fold reads from device memory.
+  // and samples the folding challenge, which the fold reads from device memory. The
+  // layers of at most kTailMax values are committed and folded by one CTA (fri_tail).
+  unsigned tail = L;  // first layer of the tail
+  for (unsigned i = 0; i < L; ++i)
+    if ((N >> i) <= kTailMax) {
+      tail = i;
+      break;
+    }
+  if (L - tail > kTailLayers) tail = L - kTailLayers;
+  if (tail > 0) build_qm31_tree(layers[0]->p, ftrees[0]->t, st);
   std::vector<Digest> froots(L);
   if (L > 0) {
     DevBuf<Channel> d_ch(1, st);
     h2d_small(d_ch.p, &ch, sizeof(Channel), st);
     DevBuf<qm31> d_alpha(L, st);
     DevBuf<uint32_t> d_roots((size_t)8 * L, st);
-    for (unsigned i = 0; i < L; ++i) {
-      k_fri_transcript<<<1, 1, 0, st>>>(d_ch.p, ftrees[i]->t.root(), d_roots.p + 8 * i, d_alpha.p + i);
+    for (unsigned i = 0; i < tail; ++i) {
+      k_fri_transcript<<<1, 32, 0, st>>>(d_ch.p, ftrees[i]->t.root(), d_roots.p + 8 * i, d_alpha.p + i);
       ZS_CUDA(cudaGetLastError());
       const uint32_t half = N >> (i + 1);
       layers.push_back(std::make_unique<DevBuf<qm31>>(half, st));
       fri_fold(layers[i]->p, layers[i + 1]->p, half, d_alpha.p + i, i, ftabs,
-               i + 1 < L ? &ftrees[i + 1]->t : nullptr, st);
+               i + 1 < tail ? &ftrees[i + 1]->t : nullptr, st);
+    }
+    DevBuf<FriTail> d_tail(1, st);
+    if (tail < L) {
+      FriTail ft{};
+      ft.first = tail, ft.count = L - tail, ft.log_size = lN - tail, ft.tables = ftabs.tables;
+      for (unsigned i = tail; i < L; ++i) layers.push_back(std::make_unique<DevBuf<qm31>>(N >> (i + 1), st));
+      for (unsigned c = 0; c <= ft.count; ++c) ft.layer[c] = layers[tail + c]->p;
+      for (unsigned c = 0; c < ft.count; ++c) {
+        ft.off_inv[c] = ftabs.offset_inv(tail + c);
+        ft.tree[c] = ftrees[tail + c]->t.words;
+      }
+      ft.roots = d_roots.p + 8 * tail;
+      ft.alphas = d_alpha.p + tail;
+      h2d_small(d_tail.p, &ft, sizeof(ft), st);
+      fri_tail(d_tail.p, d_ch.p, st);
     }
     d2h_small(&ch, d_ch.p, sizeof(Channel), st);  // the transcript continues on the host
     std::vector<uint32_t> words((size_t)8 * L);
