@@ -451,15 +451,13 @@ def main():
     e2e_s = float("nan")
     if not args.no_e2e:
         for _ in range(args.warmup):
-            plan.upload(pinned.data_ptr(), sp)
-            plan.run(None, sp)
+            plan.run_host(pinned.data_ptr(), sp)
             plan.results(sp)
         barrier(world)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            plan.upload(pinned.data_ptr(), sp)
-            plan.run(None, sp)
+            plan.run_host(pinned.data_ptr(), sp)  # the upload overlaps the LDE of earlier column groups
             r = plan.results(sp)
         e2e_s = max_over_ranks(time.perf_counter() - t0, world) / args.steps
         assert r["lde_root"] == ref_root, "e2e run changed the LDE root"

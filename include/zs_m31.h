@@ -194,6 +194,11 @@ int32_t zs_m31_commit_plan_upload(zs_commit_plan *plan, const uint32_t *host_tra
 /* Runs the whole workload on `stream` (a cudaStream_t; NULL = default stream) over a
  * device trace (NULL = the plan's own trace buffer). Asynchronous. */
 int32_t zs_m31_commit_plan_run_device(zs_commit_plan *plan, const uint32_t *d_trace, void *stream);
+/* The whole workload from a trace in pinned host memory (C x 2^log_rows words,
+ * column-major): column groups are copied on a copy stream while the LDE of the groups
+ * already on the device runs, then the rest of the step, all on `stream`. The trace
+ * must stay valid and unchanged until the step has run. Asynchronous. */
+int32_t zs_m31_commit_plan_run_host(zs_commit_plan *plan, const uint32_t *host_trace, void *stream);
 /* Runs one phase of run_device: 0 = circle LDE of all columns, 1 = row-leaf Merkle
  * tree with the gamma combination and the layer-0 tree, 2 = the fold chain. Running
  * 0, 1, 2 in order equals one run_device call. */

@@ -66,3 +66,23 @@ def test_commit_full_size_matches_oracle(orc):
         assert not coeffs[1 << 19:half].any() and not coeffs[half + (1 << 19):].any()
         assert np.array_equal(native.circle_fft(coeffs), lde[c])
     plan.close()
+
+
+@pytest.mark.parametrize("n_cols,log_rows,log_blowup,n_folds", [(13, 10, 2, 8), (64, 12, 2, 10), (3, 4, 1, 3)])
+def test_run_host_matches_oracle(orc, n_cols, log_rows, log_blowup, n_folds):
+    """run_host (column groups uploaded from pinned memory while earlier groups' LDE
+    runs), twice in a row on the same plan, equals the oracle."""
+    import torch
+    from zs_b200 import native
+    trace, gammas, alphas = _inputs(n_cols, log_rows, n_folds, 11 * n_cols + log_rows)
+    want = orc.circle_commit(trace, log_blowup, gammas, alphas)
+    pinned = torch.from_numpy(trace.view(np.int32)).pin_memory()
+    plan = native.CommitPlan(n_cols, log_rows, log_blowup, n_folds)
+    plan.set_challenges(gammas, alphas)
+    for _ in range(2):
+        plan.run_host(pinned.data_ptr())
+        got = plan.results()
+        assert got["lde_root"] == want["lde_root"]
+        assert np.array_equal(got["layer_roots"], want["layer_roots"])
+        assert np.array_equal(got["final_layer"], want["final_layer"])
+    plan.close()

@@ -122,6 +122,13 @@ int32_t zs_m31_commit_plan_run_device(zs_commit_plan* plan, const uint32_t* d_tr
   });
 }
 
+int32_t zs_m31_commit_plan_run_host(zs_commit_plan* plan, const uint32_t* host_trace, void* stream) {
+  return guarded([&] {
+    if (!plan || !host_trace) throw Error(ZS_EMALFORMED, "null argument");
+    plan->plan->run_host(host_trace, (cudaStream_t)stream);
+  });
+}
+
 int32_t zs_m31_commit_plan_run_phase(zs_commit_plan* plan, int32_t phase, const uint32_t* d_trace, void* stream) {
   return guarded([&] {
     if (!plan) throw Error(ZS_EMALFORMED, "null plan");

@@ -1,6 +1,7 @@
 // The circle commit workload as one device-resident plan: circle LDE of all
 // columns, row-leaf Merkle tree fused with the gamma combination and the layer-0
 // FRI commitment, then the fold chain with one fused fold+commit launch per layer.
+#include <algorithm>
 #include <cstdlib>
 #include <memory>
 #include <vector>
@@ -16,7 +17,10 @@ CommitPlan::CommitPlan(uint32_t C_, unsigned L_, unsigned B_, unsigned F_) : C(C
   if (L < 1 || L + B > 28) throw Error(ZS_EMALFORMED, "log_rows + log_blowup must be in [1, 28]");
   if (F > L + B) throw Error(ZS_EMALFORMED, "more folds than domain bits");
   ZS_CUDA(cudaStreamCreateWithFlags(&setup, cudaStreamNonBlocking));
+  ZS_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
   for (auto& s : sides) ZS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  up_events.resize(kUploadGroups + 1);
+  for (auto& e : up_events) ZS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   events.resize(F + 2 + kSides);
   for (auto& e : events) ZS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   const size_t n = (size_t)1 << L, N = (size_t)1 << (L + B);
@@ -57,6 +61,8 @@ CommitPlan::~CommitPlan() {
   big.reset();
   tabs.reset();
   for (auto& e : events) cudaEventDestroy(e);
+  for (auto& e : up_events) cudaEventDestroy(e);
+  cudaStreamDestroy(copy);
   for (auto& s : sides) cudaStreamDestroy(s);
   cudaStreamDestroy(setup);
 }
@@ -99,6 +105,56 @@ void CommitPlan::run_direct(const uint32_t* d_trace, cudaStream_t st) {
   const size_t n = (size_t)1 << L, N = (size_t)1 << (L + B);
   if (!d_trace) d_trace = trace;
   circle_lde(d_trace, n, lde, N, C, L, B, *small, *big, scratch, st);
+  after_lde(st);
+}
+
+// Column group g is copied on `copy` and its LDE waits for that copy only; the groups'
+// LDEs run in order on `st` and share the scratch buffer (sized for all C columns).
+void CommitPlan::run_host_direct(const uint32_t* h_trace, cudaStream_t st) {
+  const size_t n = (size_t)1 << L, N = (size_t)1 << (L + B);
+  const uint32_t per = (C + kUploadGroups - 1) / kUploadGroups;
+  ZS_CUDA(cudaEventRecord(up_events[kUploadGroups], st));  // the previous step is done with `trace`
+  ZS_CUDA(cudaStreamWaitEvent(copy, up_events[kUploadGroups], 0));
+  for (uint32_t g = 0, c0 = 0; c0 < C; ++g, c0 += per) {
+    const uint32_t cols = std::min(per, C - c0);
+    ZS_CUDA(cudaMemcpyAsync(trace + c0 * n, h_trace + c0 * n, (size_t)cols * n * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, copy));
+    ZS_CUDA(cudaEventRecord(up_events[g], copy));
+  }
+  for (uint32_t g = 0, c0 = 0; c0 < C; ++g, c0 += per) {
+    const uint32_t cols = std::min(per, C - c0);
+    ZS_CUDA(cudaStreamWaitEvent(st, up_events[g], 0));
+    circle_lde(trace + c0 * n, n, lde + c0 * N, N, cols, L, B, *small, *big, scratch, st);
+  }
+  after_lde(st);
+}
+
+void CommitPlan::run_host(const uint32_t* h_trace, cudaStream_t st) {
+  if (!use_graph) return run_host_direct(h_trace, st);
+  if (!host_exec || host_trace != h_trace) {
+    if (host_exec) cudaGraphExecDestroy(host_exec);
+    host_exec = nullptr;
+    cudaGraph_t g = nullptr;
+    ZS_CUDA(cudaStreamBeginCapture(setup, cudaStreamCaptureModeThreadLocal));
+    try {
+      run_host_direct(h_trace, setup);
+    } catch (...) {
+      cudaStreamEndCapture(setup, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    ZS_CUDA(cudaStreamEndCapture(setup, &g));
+    const cudaError_t e = cudaGraphInstantiate(&host_exec, g, 0);
+    cudaGraphDestroy(g);
+    ZS_CUDA(e);
+    host_trace = h_trace;
+  }
+  ZS_CUDA(cudaGraphLaunch(host_exec, st));
+}
+
+// Everything after the LDE: row leaves with the gamma combination, the trees, the folds.
+void CommitPlan::after_lde(cudaStream_t st) {
+  const size_t N = (size_t)1 << (L + B);
   build_row_leaves(lde, N, C, row_tree, gammas, layers[0], F > 0 ? &layer_trees[0] : nullptr, st);
   unsigned side = 0;
   bool used[kSides] = {};
@@ -132,6 +188,9 @@ void CommitPlan::drop_graph() {
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   graph_exec = nullptr;
   graph_trace = nullptr;
+  if (host_exec) cudaGraphExecDestroy(host_exec);
+  host_exec = nullptr;
+  host_trace = nullptr;
 }
 
 // The whole step is one CUDA graph (about a hundred launches, most of them small

@@ -38,6 +38,12 @@ struct CommitPlan {
   // tree fused with the gamma combination and the layer-0 tree; the fold chain.
   void run_phase(int phase, const uint32_t* d_trace, cudaStream_t st);
   uint32_t launches() const;
+  // The step from a trace in pinned host memory: column groups are copied on a copy
+  // stream while the LDE of the groups already on the device runs, then the rest of
+  // the step; replayed as one captured graph per host pointer.
+  void run_host(const uint32_t* h_trace, cudaStream_t st);
+  void run_host_direct(const uint32_t* h_trace, cudaStream_t st);
+  static constexpr unsigned kUploadGroups = 8;
 
  private:
   static constexpr unsigned kSides = 3;
@@ -47,7 +53,12 @@ struct CommitPlan {
   bool use_graph = true;
   cudaGraphExec_t graph_exec = nullptr;
   const uint32_t* graph_trace = nullptr;
+  cudaStream_t copy = nullptr;
+  std::vector<cudaEvent_t> up_events;  // kUploadGroups + 1
+  cudaGraphExec_t host_exec = nullptr;
+  const uint32_t* host_trace = nullptr;
   void drop_graph();
+  void after_lde(cudaStream_t st);
 };
 
 }  // namespace zs

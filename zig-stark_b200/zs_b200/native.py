@@ -43,6 +43,7 @@ def lib():
         L.zs_m31_commit_plan_trace_buffer.restype = ctypes.c_void_p
         L.zs_m31_commit_plan_upload.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.zs_m31_commit_plan_run_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.zs_m31_commit_plan_run_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.zs_m31_commit_plan_run_phase.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                                     ctypes.c_void_p]
         L.zs_m31_commit_plan_results.argtypes = [ctypes.c_void_p, ctypes.c_void_p, u8p, u8p, u32p]
@@ -176,6 +177,11 @@ class CommitPlan:
     def run(self, d_trace=None, stream=None):
         check(lib().zs_m31_commit_plan_run_device(self._h, ctypes.c_void_p(d_trace or 0),
                                                   ctypes.c_void_p(stream or 0)), "zs_m31_commit_plan_run_device")
+
+    def run_host(self, host_ptr, stream=None):
+        """The step from a pinned host trace (pointer), its upload overlapped with the LDE."""
+        check(lib().zs_m31_commit_plan_run_host(self._h, ctypes.c_void_p(int(host_ptr)), ctypes.c_void_p(stream or 0)),
+              "zs_m31_commit_plan_run_host")
 
     PHASES = ("lde", "row_tree", "folds")
 
