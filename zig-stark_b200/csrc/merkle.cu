@@ -161,25 +161,28 @@ __global__ void __launch_bounds__(kThreads) k_tree_up(uint32_t* tree_words, unsi
   thread_subtree<CNT>([&](int k, uint32_t d[8]) { get_digest(src, first + k, d); }, tree_words, log_n, level0, first);
 }
 
-// The top of a tree in one CTA: level `level0` holds cnt <= kTopMax digests; every
-// level above it is hashed in shared memory, one node per thread, with a barrier
-// between levels (these levels are latency-bound, so one launch replaces one launch
-// per level).
+// Subtrees of a tree in CTAs: CTA b takes the 2^levels <= kTopMax digests
+// [b 2^levels, (b + 1) 2^levels) of level `level0` and hashes the `levels` levels above
+// them in shared memory, one node per thread, a barrier between levels. These levels
+// are latency-bound (few nodes, each a chain of two compressions), so one launch
+// replaces one launch per level; with levels = log_n - level0 one CTA finishes the tree.
 constexpr unsigned kTopMax = 1024;
-__global__ void __launch_bounds__(kTopMax / 2) k_tree_top(uint32_t* tree_words, unsigned log_n, unsigned level0) {
+__global__ void __launch_bounds__(kTopMax / 2) k_tree_block(uint32_t* tree_words, unsigned log_n, unsigned level0,
+                                                            unsigned levels) {
   __shared__ uint32_t s[kTopMax][8];
   const size_t N2 = (size_t)2 << log_n;
-  uint32_t cnt = 1u << (log_n - level0);
+  uint32_t cnt = 1u << levels;
+  const uint32_t first = blockIdx.x << levels;  // first digest of this CTA at level0
   const uint32_t* src = tree_words + 8 * (N2 - (N2 >> level0));
-  for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) get_digest(src, i, s[i]);
+  for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) get_digest(src, first + i, s[i]);
   __syncthreads();
-  for (unsigned lvl = level0 + 1; lvl <= log_n; ++lvl) {
+  for (unsigned lvl = level0 + 1; lvl <= level0 + levels; ++lvl) {
     cnt >>= 1;
     uint32_t o[8];
     const bool active = threadIdx.x < cnt;
     if (active) {
       b3::hash2(s[2 * threadIdx.x], s[2 * threadIdx.x + 1], o);
-      put_digest(tree_words, (N2 - (N2 >> lvl)) + threadIdx.x, o);
+      put_digest(tree_words, (N2 - (N2 >> lvl)) + (first >> (lvl - level0)) + threadIdx.x, o);
     }
     __syncthreads();  // every child is read before a parent overwrites it
     if (active)
@@ -216,22 +219,24 @@ static unsigned levels_per_launch(unsigned log_n, unsigned lvl) {
 void tree_finish(DeviceTree& tree, unsigned from_level, cudaStream_t st) {
   unsigned lvl = from_level;
   while (lvl < tree.log_n) {
-    if ((1u << (tree.log_n - lvl)) <= kTopMax) {
-      k_tree_top<<<1, kTopMax / 2, 0, st>>>(tree.words, tree.log_n, lvl);
-      break;
+    const unsigned rem = tree.log_n - lvl;
+    if (levels_per_launch(tree.log_n, lvl) == 3) {  // wide levels: subtrees per thread
+      launch_up(tree, lvl, 3, st);
+      lvl += 3;
+      continue;
     }
-    const unsigned s = levels_per_launch(tree.log_n, lvl);
-    launch_up(tree, lvl, s, st);
-    lvl += s;
+    const unsigned levels = rem < 10 ? rem : 10;  // narrow levels: subtrees per CTA
+    k_tree_block<<<1u << (rem - levels), kTopMax / 2, 0, st>>>(tree.words, tree.log_n, lvl, levels);
+    lvl += levels;
   }
   ZS_CUDA(cudaGetLastError());
 }
 
 uint32_t tree_finish_launches(unsigned log_n, unsigned from_level) {
   uint32_t k = 0;
-  for (unsigned lvl = from_level; lvl < log_n; lvl += levels_per_launch(log_n, lvl)) {
-    ++k;
-    if ((1u << (log_n - lvl)) <= kTopMax) break;
+  for (unsigned lvl = from_level; lvl < log_n; ++k) {
+    const unsigned rem = log_n - lvl;
+    lvl += levels_per_launch(log_n, lvl) == 3 ? 3 : (rem < 10 ? rem : 10);
   }
   return k;
 }
