@@ -234,7 +234,8 @@ __global__ void k_from_crt(qm31* a, size_t stride, uint32_t n, unsigned shift) {
 
 // The passes of a size-2^logN transform: one over contiguous 2^S-element blocks
 // (S = min(logN, 11), stages 1..S) and passes of up to 11 stages over strided groups
-// (at most 4096 elements, 64 KB, per CTA) for stages S+1..logN.
+// (2048 elements, 32 KB, per CTA, or two groups of 2^11 at M = 11) for stages
+// S+1..logN; smaller CTAs keep more of them resident to cover the twiddle loads.
 struct PassPlan {
   unsigned lo, M;
   uint32_t G;
@@ -247,7 +248,7 @@ static std::vector<PassPlan> plan_passes(unsigned logN) {
   while (lo < logN) {
     const unsigned rem = logN - lo, passes = (rem + kSmemLog - 1) / kSmemLog;
     const unsigned M = (rem + passes - 1) / passes;
-    uint32_t G = 4096u >> M;
+    uint32_t G = 2048u >> M;
     if (G < 2) G = 2;
     if (G > (1u << lo)) G = 1u << lo;
     v.push_back({lo, M, G});
