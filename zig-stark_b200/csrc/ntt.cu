@@ -163,6 +163,12 @@ __device__ __forceinline__ void ntt_radix2(qm31* s, unsigned M, uint32_t G, unsi
   __syncthreads();
 }
 
+// out[j] = phi(in[bitrev(j)]) for j < 2^log_n.
+__global__ void k_to_crt_brev(const qm31* __restrict__ in, qm31* __restrict__ out, unsigned log_n) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < (1u << log_n)) stq(out + j, to_crt(ldq(in + bitrev(j, log_n))));
+}
+
 // x[i] = phi(x[i]) for the elements of C columns (count each), out of place allowed.
 __global__ void k_to_crt_cols(const qm31* in, size_t in_stride, qm31* out, size_t out_stride, uint32_t count) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -302,7 +308,7 @@ static void dif_all(const qm31* src, size_t src_stride, qm31* a, size_t stride, 
 // input is zero elsewhere, so its first B stages only copy the value across the 2^B
 // block at j << B (each stage pairs a filled element with a zero one): the block is
 // written as 2^B copies and the forward transform starts at stage B + 1.
-// offset_crt[k] = phi(offset^k).
+// offset_crt[j] = phi(offset^bitrev_n(j)) (bit-reversed, so every read is coalesced).
 __global__ void k_coeff_finish(qm31* coeffs, size_t c_stride, qm31* big, size_t b_stride, unsigned log_n,
                                unsigned log_N, const qm31* __restrict__ offset_crt) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -312,7 +318,7 @@ __global__ void k_coeff_finish(qm31* coeffs, size_t c_stride, qm31* big, size_t 
   const unsigned sh = (31 - log_n) % 31;
   v = qmake(mshl(v.a.a, sh), mshl(v.a.b, sh), mshl(v.b.a, sh), mshl(v.b.b, sh));
   stq(cp, from_crt(v));
-  const qm31 w = crt_mul(v, ldq(offset_crt + bitrev(j, log_n)));
+  const qm31 w = crt_mul(v, ldq(offset_crt + j));
   const unsigned B = log_N - log_n;
   qm31* dst = big + (size_t)blockIdx.y * b_stride + ((size_t)j << B);
   for (uint32_t r = 0; r < (1u << B); ++r) stq(dst + r, w);
@@ -328,7 +334,7 @@ void lde_qm31(const qm31* values, size_t v_stride, qm31* coeffs, size_t c_stride
   // input after its first log_N - log_n stages
   qm31* off_crt = nullptr;
   ZS_CUDA(cudaMallocAsync((void**)&off_crt, (size_t)n * sizeof(qm31), st));
-  k_to_crt<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(offset_pows, off_crt, n);
+  k_to_crt_brev<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(offset_pows, off_crt, log_n);
   k_coeff_finish<<<dim3((n + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(coeffs, c_stride, codeword, w_stride,
                                                                               log_n, log_N, off_crt);
   ZS_CUDA(cudaFreeAsync(off_crt, st));
