@@ -252,14 +252,14 @@ __device__ __forceinline__ void chunk_ct(uint32_t* s, uint32_t gstride, unsigned
   }
 }
 
-// All M layers with a compile-time chunk schedule (chunks of <= 4 layers, the
+// All M layers with a compile-time chunk schedule (chunks of <= 5 layers, the
 // largest first), DONE layers already applied.
 template <bool INV, unsigned M, unsigned DONE>
 __device__ __forceinline__ void run_layers_ct(uint32_t* s, uint32_t gstride, unsigned G, unsigned shift,
                                               const uint32_t* TW, uint32_t n_dom, const uint32_t* vb) {
   if constexpr (DONE < M) {
     constexpr unsigned REM = M - DONE;
-    constexpr unsigned NCH = (REM + 3) / 4;
+    constexpr unsigned NCH = (REM + 4) / 5;
     constexpr unsigned R = (REM + NCH - 1) / NCH;
     // forward: top-down, the chunk covers [M - DONE - R, M - DONE); inverse: bottom-up
     constexpr unsigned B0 = INV ? DONE : M - DONE - R;
