@@ -12,8 +12,9 @@
  *   - return codes: 0 ok, -1 generic, -2 malformed input, -3 out of memory,
  *     -4 protocol error (zig-capi.h:20-21), and -5 device error.
  *
- * Every entry point runs its hot path on the GPU; there is no CPU fallback. Without a
- * usable CUDA device the calls return -5.
+ * The prover, commitment and transform entry points run on the GPU, with no CPU
+ * fallback: without a usable CUDA device they return -5. The verifier entry points
+ * (zs_m31_verify, zs_m31_verify_batch) run on the host, as the reference's does.
  */
 #ifndef ZS_M31_H
 #define ZS_M31_H
