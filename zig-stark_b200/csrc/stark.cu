@@ -12,6 +12,7 @@
 //   and the gather of every revealed value and Merkle path.
 // All device arithmetic is exact, so every root, layer and proof byte equals the
 // reference's.
+#include <algorithm>
 #include <memory>
 #include <mutex>
 #include <vector>
@@ -319,6 +320,35 @@ void upload_columns(const WireColumns& c, qm31* dst, uint32_t n, cudaStream_t st
   ZS_CUDA(cudaGetLastError());
 }
 
+// A copy stream for one proof's uploads, forked from `st` (so it sees the buffers
+// allocated there before). join() makes `st` wait for everything issued on it so far; the destructor joins too (so stream-ordered frees on `st` follow every
+// copy) and releases the stream once it has drained.
+struct CopyStream {
+  cudaStream_t s = nullptr, st;
+  cudaEvent_t ev = nullptr;
+  explicit CopyStream(cudaStream_t main) : st(main) {
+    ZS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    ZS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    ZS_CUDA(cudaEventRecord(ev, st));  // buffers allocated on `st` so far are ready
+    ZS_CUDA(cudaStreamWaitEvent(s, ev, 0));
+  }
+  void join() {
+    ZS_CUDA(cudaEventRecord(ev, s));
+    ZS_CUDA(cudaStreamWaitEvent(st, ev, 0));
+  }
+  ~CopyStream() {
+    cudaEventRecord(ev, s);
+    cudaStreamWaitEvent(st, ev, 0);
+    cudaStreamSynchronize(s);
+    cudaEventDestroy(ev);
+    cudaStreamDestroy(s);
+  }
+  CopyStream(const CopyStream&) = delete;
+  CopyStream& operator=(const CopyStream&) = delete;
+};
+constexpr size_t kGroupMin = (size_t)8 << 20;    // wire bytes below which one group suffices
+constexpr size_t kGroupBytes = (size_t)16 << 20;  // wire bytes per upload group
+
 // Freed blocks stay in the device's stream-ordered pool instead of going back to the
 // driver at every synchronization, so repeated proofs do not map their memory again.
 void retain_pool_memory() {
@@ -400,13 +430,32 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   DevBuf<qm31> offset_pows(n, st);
   qm31_powers(offset, offset_pows.p, n, st);
   DevBuf<qm31> vals((size_t)ncol * n, st), coeffs((size_t)ncol * n, st), cw((size_t)ncol * N, st);
-  upload_columns(pre, vals.p, n, st);
-  upload_columns(trace, vals.p + (size_t)n_pre * n, n, st);
-  lde_qm31(vals.p, n, coeffs.p, n, cw.p, N, n_pre + m, small, big, offset_pows.p, st);
-
   std::vector<std::unique_ptr<OwnedTree>> trees;
   for (uint32_t j = 0; j < ncol; ++j) trees.push_back(std::make_unique<OwnedTree>(lN, st));
-  for (uint32_t j = 0; j < n_pre + m; ++j) build_qm31_tree(cw.p + (size_t)j * N, trees[j]->t, st);
+  {
+    // Columns [pre | main] in groups: group g+1 is packed on the host and copied on a
+    // copy stream while the LDE and trees of group g run on `st`. A proof whose columns
+    // are small goes as one group.
+    const uint32_t C = n_pre + m;
+    const size_t col_bytes = (size_t)16 * n;
+    const uint32_t per = col_bytes * C < kGroupMin ? C : std::max<uint32_t>(1, (uint32_t)(kGroupBytes / col_bytes));
+    std::unique_ptr<CopyStream> cs;
+    if (per < C) cs = std::make_unique<CopyStream>(st);
+    cudaStream_t up = cs ? cs->s : st;
+    for (uint32_t c0 = 0; c0 < C; c0 += per) {
+      const uint32_t c1 = std::min(C, c0 + per);
+      WireColumns gp, gt;  // this group's preprocessed and main columns
+      for (uint32_t j = c0; j < std::min(c1, n_pre); ++j) gp.data.push_back(pre.data[j]), gp.len.push_back(n);
+      for (uint32_t j = std::max(c0, n_pre); j < c1; ++j)
+        gt.data.push_back(trace.data[j - n_pre]), gt.len.push_back(n);
+      upload_columns(gp, vals.p + (size_t)c0 * n, n, up);
+      upload_columns(gt, vals.p + (size_t)std::max(c0, n_pre) * n, n, up);
+      if (cs) cs->join();  // `st` waits for this group's columns only
+      lde_qm31(vals.p + (size_t)c0 * n, n, coeffs.p + (size_t)c0 * n, n, cw.p + (size_t)c0 * N, N, c1 - c0, small,
+               big, offset_pows.p, st);
+      for (uint32_t j = c0; j < c1; ++j) build_qm31_tree(cw.p + (size_t)j * N, trees[j]->t, st);
+    }
+  }
 
   Channel ch(sep, sep_len);
   WireWriter proof;
