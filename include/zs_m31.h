@@ -74,6 +74,25 @@ int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t *par
                      size_t preprocessed_len, const uint8_t *trace, size_t trace_len, const uint8_t *channel_sep,
                      size_t channel_sep_len, uint8_t **out_proof, size_t *out_len);
 
+/* ---- device contexts ---------------------------------------------------------
+ * An explicit handle instead of process-global device state: a context binds one CUDA
+ * device ordinal and a stream of its own. zs_m31_prove_ctx is zs_m31_prove run on the
+ * context's device and stream; the caller's current device is restored on return.
+ * Calls on one context run one at a time (a mutex); calls on distinct contexts run
+ * concurrently, on one device or several. The reference keeps its one GPU context in a
+ * lazy process global under a spin mutex (circlefft_gpu.zig:21-39).
+ * zs_m31_ctx_create returns -5 when `device` is not a valid ordinal or no device is
+ * present. zs_m31_prove (no context) runs on the calling thread's current device. */
+typedef struct zs_m31_ctx zs_m31_ctx;
+int32_t zs_m31_ctx_create(int32_t device, zs_m31_ctx **out);
+void zs_m31_ctx_destroy(zs_m31_ctx *ctx);
+int32_t zs_m31_ctx_device(const zs_m31_ctx *ctx);
+int32_t zs_m31_prove_ctx(zs_m31_ctx *ctx, zs_host_allocator host, uint32_t air_id, const uint8_t *params,
+                         size_t params_len, const uint8_t *public_inputs, size_t public_inputs_len,
+                         const uint8_t *preprocessed, size_t preprocessed_len, const uint8_t *trace,
+                         size_t trace_len, const uint8_t *channel_sep, size_t channel_sep_len,
+                         uint8_t **out_proof, size_t *out_len);
+
 /* ---- batched and served proving ---------------------------------------------
  * One proof job: the arguments of zs_m31_prove. */
 typedef struct {

@@ -126,3 +126,43 @@ def test_packed_upload_paths(orc):
     m31_col[:4, 0] = [wl.P, wl.P + 1, 2**32 - 1, 0]
     qm_col = rng.integers(0, wl.P, (n, 4), dtype=np.uint32)
     _check(orc, wl.AIR_FIB, wire.StarkParams(17, 1, 8, 3), wire.qm31((1, 2, 3, 4)), [m31_col, qm_col], valid=False)
+
+
+def test_grouped_upload_with_preprocessed_columns(orc):
+    """2^18 rows of the AND-table lookup AIR: 2 preprocessed + 3 main columns of 4 MiB
+    each go up in column groups on a copy stream, the first group holding both
+    preprocessed columns and two main ones; against the oracle."""
+    tr, table = wl.and_table_trace(1 << 18)
+    _check(orc, wl.AIR_AND_TABLE, wire.StarkParams(18, 1, 8, 3), b"", tr, table, sep=b"zig-stark:stark:lookup")
+
+
+def test_context_prove_matches_prove():
+    """zs_m31_prove_ctx on two contexts of device 0, driven from two threads at once,
+    gives the bytes of zs_m31_prove for every job."""
+    import threading
+    from zs_b200 import native
+    jobs = [wl.proof_job(air, lg, 5, b"ctx") for air, lg in
+            [(wl.AIR_SEEDED_FIB, 10), (wl.AIR_RESCUE_STACKED, 12), (wl.AIR_SEEDED_FIB, 14), (wl.AIR_RESCUE_STACKED, 16)]]
+    want = [native.prove(j[0], j[1], j[2], j[3], b"", j[4]) for j in jobs]
+    got = [None] * len(jobs)
+    with native.Context(0) as c0, native.Context(0) as c1:
+        assert c0.device == 0 and c1.device == 0
+
+        def run(ctx, idx):
+            for i in idx:
+                j = jobs[i]
+                got[i] = ctx.prove(j[0], j[1], j[2], j[3], b"", j[4])
+
+        ts = [threading.Thread(target=run, args=(c0, [0, 2])), threading.Thread(target=run, args=(c1, [1, 3]))]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+    assert got == want
+
+
+def test_context_rejects_bad_device():
+    from zs_b200 import native
+    with pytest.raises(native.ZsError) as e:
+        native.Context(1 << 20)
+    assert e.value.code == -5

@@ -43,3 +43,14 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(native, "LIB_PATH", str(tmp_path / "absent.so"))
     with pytest.raises(ImportError):
         native.lib()
+
+
+def test_context_without_device_is_a_device_error():
+    """On a host without a CUDA device, zs_m31_ctx_create returns -5 (no device work)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from zs_b200 import native
+    with pytest.raises(native.ZsError) as e:
+        native.Context(0)
+    assert e.value.code == -5

@@ -3,6 +3,7 @@
 #include <atomic>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <thread>
 
@@ -189,33 +190,129 @@ int32_t zs_m31_circle_commit(const uint32_t* trace, uint32_t n_columns, uint32_t
   return rc;
 }
 
+namespace {
+
+// The calling thread's current device for the lifetime of the scope is `device`.
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int device) {
+    ZS_CUDA(cudaGetDevice(&prev));
+    if (prev != device) ZS_CUDA(cudaSetDevice(device));
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
+// The argument checks of zs_m31_prove, made before any device is touched.
+void check_prove_args(zs_host_allocator host, const uint8_t* params, size_t params_len, const uint8_t* public_inputs,
+                      size_t public_inputs_len, const uint8_t* preprocessed, size_t preprocessed_len,
+                      const uint8_t* trace, size_t trace_len, const uint8_t* channel_sep, size_t channel_sep_len,
+                      uint8_t** out_proof, size_t* out_len) {
+  if (!out_proof || !out_len || !host.alloc) throw Error(ZS_EMALFORMED, "null output or allocator");
+  if ((!params && params_len) || (!public_inputs && public_inputs_len) || (!preprocessed && preprocessed_len) ||
+      (!trace && trace_len) || (!channel_sep && channel_sep_len))
+    throw Error(ZS_EMALFORMED, "null input buffer with a non-zero length");
+}
+
+// zs_m31_prove on stream `st` of the current device: proves and hands the bytes to the
+// caller's allocator.
+void prove_on(cudaStream_t st, zs_host_allocator host, uint32_t air_id, const uint8_t* params, size_t params_len,
+              const uint8_t* public_inputs, size_t public_inputs_len, const uint8_t* preprocessed,
+              size_t preprocessed_len, const uint8_t* trace, size_t trace_len, const uint8_t* channel_sep,
+              size_t channel_sep_len, uint8_t** out_proof, size_t* out_len) {
+  std::vector<uint8_t> bytes;
+  try {
+    bytes = stark_prove(air_id, params, params_len, public_inputs, public_inputs_len, preprocessed, preprocessed_len,
+                        trace, trace_len, channel_sep, channel_sep_len, st);
+  } catch (...) {
+    cudaStreamSynchronize(st);
+    throw;
+  }
+  uint8_t* buf = (uint8_t*)host.alloc(host.ctx, bytes.size() ? bytes.size() : 1);
+  if (!buf) throw Error(ZS_ENOMEM, "host allocator returned null");
+  std::memcpy(buf, bytes.data(), bytes.size());
+  *out_proof = buf;
+  *out_len = bytes.size();
+}
+
+}  // namespace
+
+struct zs_m31_ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  std::mutex mu;  // one call at a time on this context
+};
+
 int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t* params, size_t params_len,
                      const uint8_t* public_inputs, size_t public_inputs_len, const uint8_t* preprocessed,
                      size_t preprocessed_len, const uint8_t* trace, size_t trace_len, const uint8_t* channel_sep,
                      size_t channel_sep_len, uint8_t** out_proof, size_t* out_len) {
   return guarded([&] {
-    if (!out_proof || !out_len || !host.alloc) throw Error(ZS_EMALFORMED, "null output or allocator");
-    if ((!params && params_len) || (!public_inputs && public_inputs_len) || (!preprocessed && preprocessed_len) ||
-        (!trace && trace_len) || (!channel_sep && channel_sep_len))
-      throw Error(ZS_EMALFORMED, "null input buffer with a non-zero length");
+    check_prove_args(host, params, params_len, public_inputs, public_inputs_len, preprocessed, preprocessed_len, trace,
+                     trace_len, channel_sep, channel_sep_len, out_proof, out_len);
     ensure_device();
     cudaStream_t st = nullptr;
     ZS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    std::vector<uint8_t> bytes;
     try {
-      bytes = stark_prove(air_id, params, params_len, public_inputs, public_inputs_len, preprocessed,
-                          preprocessed_len, trace, trace_len, channel_sep, channel_sep_len, st);
+      prove_on(st, host, air_id, params, params_len, public_inputs, public_inputs_len, preprocessed,
+               preprocessed_len, trace, trace_len, channel_sep, channel_sep_len, out_proof, out_len);
     } catch (...) {
-      cudaStreamSynchronize(st);
       cudaStreamDestroy(st);
       throw;
     }
     cudaStreamDestroy(st);
-    uint8_t* buf = (uint8_t*)host.alloc(host.ctx, bytes.size() ? bytes.size() : 1);
-    if (!buf) throw Error(ZS_ENOMEM, "host allocator returned null");
-    std::memcpy(buf, bytes.data(), bytes.size());
-    *out_proof = buf;
-    *out_len = bytes.size();
+  });
+}
+
+int32_t zs_m31_ctx_create(int32_t device, zs_m31_ctx** out) {
+  return guarded([&] {
+    if (!out) throw Error(ZS_EMALFORMED, "null output");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw Error(ZS_EDEVICE, "no CUDA device");
+    if (device < 0 || device >= n) throw Error(ZS_EDEVICE, "device ordinal out of range");
+    DeviceScope scope(device);
+    auto c = std::make_unique<zs_m31_ctx>();
+    c->device = device;
+    ZS_CUDA(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    *out = c.release();
+  });
+}
+
+void zs_m31_ctx_destroy(zs_m31_ctx* ctx) {
+  if (!ctx) return;
+  {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(ctx->device) == cudaSuccess) {
+      cudaStreamSynchronize(ctx->st);
+      cudaStreamDestroy(ctx->st);
+    }
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  delete ctx;
+}
+
+int32_t zs_m31_ctx_device(const zs_m31_ctx* ctx) { return ctx ? ctx->device : ZS_EMALFORMED; }
+
+int32_t zs_m31_prove_ctx(zs_m31_ctx* ctx, zs_host_allocator host, uint32_t air_id, const uint8_t* params,
+                         size_t params_len, const uint8_t* public_inputs, size_t public_inputs_len,
+                         const uint8_t* preprocessed, size_t preprocessed_len, const uint8_t* trace,
+                         size_t trace_len, const uint8_t* channel_sep, size_t channel_sep_len, uint8_t** out_proof,
+                         size_t* out_len) {
+  return guarded([&] {
+    if (!ctx) throw Error(ZS_EMALFORMED, "null context");
+    check_prove_args(host, params, params_len, public_inputs, public_inputs_len, preprocessed, preprocessed_len, trace,
+                     trace_len, channel_sep, channel_sep_len, out_proof, out_len);
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceScope scope(ctx->device);
+    prove_on(ctx->st, host, air_id, params, params_len, public_inputs, public_inputs_len, preprocessed,
+             preprocessed_len, trace, trace_len, channel_sep, channel_sep_len, out_proof, out_len);
   });
 }
 

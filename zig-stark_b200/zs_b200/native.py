@@ -294,6 +294,66 @@ def prove(air_id, params, public_inputs, trace, preprocessed=b"", channel_sep=b"
     return data
 
 
+class Context:
+    """A device context (zs_m31_ctx_*): a CUDA device ordinal and a stream of its own.
+    prove() is `prove` run on that device and stream; calls on one context run one at a
+    time, calls on distinct contexts concurrently."""
+
+    def __init__(self, device=0):
+        L = _bind_prove()
+        if not getattr(L, "_ctx_bound", False):
+            L.zs_m31_ctx_create.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+            L.zs_m31_ctx_destroy.argtypes = [ctypes.c_void_p]
+            L.zs_m31_ctx_destroy.restype = None
+            L.zs_m31_ctx_device.argtypes = [ctypes.c_void_p]
+            L.zs_m31_prove_ctx.argtypes = [ctypes.c_void_p] + L.zs_m31_prove.argtypes
+            L._ctx_bound = True
+        self._L = L
+        self._h = None
+        h = ctypes.c_void_p()
+        check(L.zs_m31_ctx_create(device, ctypes.byref(h)), "zs_m31_ctx_create")
+        self._h = h
+
+    @property
+    def device(self):
+        return self._L.zs_m31_ctx_device(self._h)
+
+    def prove(self, air_id, params, public_inputs, trace, preprocessed=b"", channel_sep=b""):
+        from . import wire
+        if not isinstance(params, (bytes, bytearray)):
+            params = params.encode()
+        if not isinstance(trace, (bytes, bytearray)):
+            trace = wire.columns(trace)
+        if not isinstance(preprocessed, (bytes, bytearray)):
+            preprocessed = wire.columns(preprocessed)
+        out = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        check(self._L.zs_m31_prove_ctx(self._h, HOST, air_id, params, len(params), public_inputs,
+                                       len(public_inputs), preprocessed, len(preprocessed), trace, len(trace),
+                                       channel_sep, len(channel_sep), ctypes.byref(out), ctypes.byref(n)),
+              "zs_m31_prove_ctx")
+        data = ctypes.string_at(out.value, n.value)
+        self._L.zs_free(HOST, out, n.value)
+        return data
+
+    def close(self):
+        if self._h:
+            self._L.zs_m31_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def verify(air_id, params, public_inputs, proof, channel_sep=b""):
     """GenericStark(Air).verify (zs_m31_verify, host-side); returns True / False."""
     if not isinstance(params, (bytes, bytearray)):
