@@ -52,29 +52,59 @@ def parse():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks / throttle reasons while the timed region runs."""
+    """Samples SM clocks and clock-event (throttle) reasons while the timed region runs:
+    through NVML every 10 ms (read-only queries, the GPU found by its UUID), else
+    nvidia-smi every 200 ms."""
 
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
-        self.rows = []
+        self.rows = []  # (sm_mhz, max_mhz, [active reason names])
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            try:
+                h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(torch.cuda.get_device_properties(device).uuid))
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self._nvml = (pynvml, h)
+        except Exception:
+            self._nvml = None
+
+    def _sample_nvml(self):
+        nv, h = self._nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.rows.append((float(sm), float(mx), [n for n, m in self.REASONS if bits & m]))
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                             timeout=5).stdout.strip()
+        r = [x.strip() for x in out.split(",")] if out else []
+        if len(r) >= 9 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+            self.rows.append((float(r[1]), float(r[2]),
+                              [n for i, (n, _) in enumerate(self.REASONS) if r[5 + i] == "Active"]))
 
     def _run(self):
-        while not self._stop.is_set():
+        period = 0.01 if self._nvml else 0.2
+        while True:
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([x.strip() for x in out.split(",")])
+                self._sample_nvml() if self._nvml else self._sample_smi()
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            if self._stop.wait(period):
+                break
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -88,12 +118,10 @@ class ClockSampler:
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = sorted(float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit())
-        mx = max(float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(self.rows)}
+        sm = sorted(r[0] for r in self.rows)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": sorted({n for r in self.rows for n in r[2]}), "samples": len(self.rows),
+                "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
 def dist_setup(args, backend="nccl"):
@@ -482,6 +510,30 @@ def main():
     # DRAM read + write bytes of the LDE's three kernels from an ncu capture of this
     # workload at 2^19 rows (1.96 GB), scaled by the rows; the other phases have none.
     traffic = {"lde": 1.9646e9 * 2.0 ** (log_rows - 19)}.get(dom)
+    # Integer co-roof. The path is exact integer work, so next to the HBM roof each phase
+    # is set against the issue bound of the SMs (4 schedulers x 32 lanes x 1 instruction
+    # per clock, at the sampled SM clock) with modelled int32 op counts: 13 per M31
+    # butterfly (multiply-reduce, add and subtract with their corrections), 700 per Blake3
+    # compression (7 rounds x 8 G x 12, plus the output xors), 36 per QM31 x M31
+    # multiply-add of the gamma combination, 60 per fold point. The ALU pipe (add, logic,
+    # shift, min) takes half the issue rate; Blake3 is ALU-pipe work alone, the
+    # butterflies put their multiplies on the FMA pipe.
+    cs = clocks.summary()
+    sm_mhz = cs.get("sm_mhz") or cs.get("sm_max_mhz") or 1965.0
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    int_peak = n_sm * 128 * sm_mhz * 1e6 / 1e12
+    lg_n, lg_N = log_rows, log_rows + LOG_BLOWUP
+    ops = {
+        "lde": 13 * N_COLS * (lg_n * (n >> 1) + lg_N * (N >> 1)),
+        "row_tree": 700 * (N * ((N_COLS * 4 + 63) // 64) + 2 * (N - 1)) + 36 * N * N_COLS,
+        "folds": sum(700 * ((N >> i) + 2 * ((N >> i) - 1)) + 60 * (N >> (i + 1)) for i in range(N_FOLDS)),
+    }
+    int_roof = {"bound": "int32 issue", "unit": "Tops/s", "peak": int_peak, "alu_pipe_peak": int_peak / 2,
+                "peak_source": f"nominal: {n_sm} SMs x 128 lanes x 1 instruction/clock at {sm_mhz:.0f} MHz",
+                "phases": {k: {"ops": ops[k], "achieved": ops[k] / (phase_ms[k] / 1e3) / 1e12,
+                               "frac": ops[k] / (phase_ms[k] / 1e3) / 1e12 / int_peak,
+                               "frac_alu_pipe": ops[k] / (phase_ms[k] / 1e3) / 1e12 / (int_peak / 2)}
+                           for k in ops}}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -495,11 +547,12 @@ def main():
                      "frac": achieved / hbm_peak, "traffic": traffic,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                      "algorithmic_bytes": alg[dom]},
+        "int_roofline": int_roof,
         "commit_bytes_per_row": 1536,
         "e2e": {"value": rows / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_s * 1e3},
         "gpu_launches": plan.launches() * args.steps,
-        "clocks": clocks.summary(),
+        "clocks": cs,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and log_rows == LOG_ROWS:
         line["cpu_baseline"] = cpu_baseline_sample(os.cpu_count() or 1)
