@@ -17,9 +17,12 @@ namespace {
 constexpr size_t kChunk = (size_t)16 << 20;  // bytes per staging buffer
 constexpr size_t kSmall = (size_t)1 << 20;   // below this the driver's pageable path is as fast
 
+thread_local bool t_upload_high = false;
+
 // A fork-join pool of host threads: run(n, f) calls f(0..n-1) spread over the pool
 // and the caller, and returns when every call has finished. A caller that finds the
-// pool busy runs its calls itself.
+// pool busy runs its calls itself, unless its uploads have priority: then it waits
+// for the pool.
 class HostPool {
  public:
   static HostPool& get() {
@@ -28,7 +31,11 @@ class HostPool {
   }
   size_t width() const { return threads_.size() + 1; }
   void run(size_t n, const std::function<void(size_t)>& f) {
-    std::unique_lock<std::mutex> call(call_mu_, std::try_to_lock);
+    std::unique_lock<std::mutex> call(call_mu_, std::defer_lock);
+    if (t_upload_high)
+      call.lock();
+    else
+      (void)call.try_lock();
     if (!call.owns_lock()) {  // the pool serves another caller: copy on this thread
       for (size_t i = 0; i < n; ++i) f(i);
       return;
@@ -175,6 +182,9 @@ class SlotBank {
 thread_local Slot* t_slot = nullptr;
 
 }  // namespace
+
+UploadPriority::UploadPriority(bool high) : prev_(t_upload_high) { t_upload_high = high; }
+UploadPriority::~UploadPriority() { t_upload_high = prev_; }
 
 PinnedScope::PinnedScope(cudaStream_t st) : st_(st), slot_(SlotBank::get().take()), prev_(t_slot) {
   Slot* s = static_cast<Slot*>(slot_);

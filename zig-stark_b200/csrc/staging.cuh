@@ -24,6 +24,21 @@ void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st);
 void upload_low_words(uint32_t* dst, const uint8_t* const* cols, uint32_t C, size_t n, uint8_t* high,
                       cudaStream_t st);
 
+// The calling thread's uploads wait for the host copy pool while the scope lives,
+// instead of packing on their own thread when another prover holds the pool. A large
+// proof sets it, so its upload keeps the pool's bandwidth while small proofs share the
+// device with it (their short copies run on their own threads meanwhile).
+class UploadPriority {
+ public:
+  explicit UploadPriority(bool high);
+  ~UploadPriority();
+  UploadPriority(const UploadPriority&) = delete;
+  UploadPriority& operator=(const UploadPriority&) = delete;
+
+ private:
+  bool prev_;
+};
+
 // The small transfers of a proof (constants, roots, evaluations, query reveals) go
 // through pinned memory too: a pageable copy takes the driver's staging path, on which
 // concurrent provers would queue behind one another's uploads.

@@ -346,6 +346,7 @@ struct CopyStream {
   CopyStream(const CopyStream&) = delete;
   CopyStream& operator=(const CopyStream&) = delete;
 };
+constexpr size_t kPriorityUpload = (size_t)64 << 20;  // wire bytes from which uploads wait for the copy pool
 constexpr size_t kGroupMin = (size_t)8 << 20;    // wire bytes below which one group suffices
 constexpr size_t kGroupBytes = (size_t)16 << 20;  // wire bytes per upload group
 
@@ -395,6 +396,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   if (trace.size() != air.m || pre.size() != air.n_pre) throw Error(ZS_EMALFORMED, "column count mismatch");
   retain_pool_memory();
   PinnedScope pinned(st);
+  UploadPriority upload_priority(trace_len + pre_len >= kPriorityUpload);
   for (uint64_t l : trace.len)
     if (l != n) throw Error(ZS_EMALFORMED, "column length mismatch");
   for (uint64_t l : pre.len)
