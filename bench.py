@@ -508,8 +508,8 @@ def main():
     dom = max(phase_ms, key=phase_ms.get)
     achieved = alg[dom] / (phase_ms[dom] / 1e3) / 1e9
     # DRAM read + write bytes of the LDE's three kernels from an ncu capture of this
-    # workload at 2^19 rows (1.96 GB), scaled by the rows; the other phases have none.
-    traffic = {"lde": 1.9646e9 * 2.0 ** (log_rows - 19)}.get(dom)
+    # workload at 2^19 rows (1.98 GB), scaled by the rows; the other phases have none.
+    traffic = {"lde": 1.9825e9 * 2.0 ** (log_rows - 19)}.get(dom)
     # Integer co-roof. The path is exact integer work, so next to the HBM roof each phase
     # is set against the issue bound of the SMs (4 schedulers x 32 lanes x 1 instruction
     # per clock, at the sampled SM clock) with modelled int32 op counts: 13 per M31
