@@ -7,6 +7,8 @@
 //     into its own s-level subtree with hash2 (= Blake3("zig-stark:pair" || L || R),
 //     two compressions), writing every node, because openings need all levels.
 // A tree over 2^22 leaves therefore takes one leaf launch and eight tree launches.
+#include <algorithm>
+
 #include "blake3.cuh"
 #include "merkle.cuh"
 
@@ -60,14 +62,15 @@ __device__ __forceinline__ void thread_subtree(Next&& next, uint32_t* tree_words
 }  // namespace
 
 // hashQM31 leaves (src/m31/hash.zig:33-37).
-__global__ void __launch_bounds__(kThreads) k_qm31_leaves(const qm31* __restrict__ vals, uint32_t* tree_words,
-                                                          uint64_t n) {
+// blockIdx.y selects the tree of a set (its values `v_stride` elements after the previous).
+__global__ void __launch_bounds__(kThreads) k_qm31_leaves(const qm31* __restrict__ vals, size_t v_stride,
+                                                          TreeSet ts, uint64_t n) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint4 raw = __ldg(reinterpret_cast<const uint4*>(vals) + i);
+  const uint4 raw = __ldg(reinterpret_cast<const uint4*>(vals + blockIdx.y * v_stride) + i);
   uint32_t o[8];
   b3::hash_qm31(qmake(raw.x, raw.y, raw.z, raw.w), o);
-  put_digest(tree_words, i, o);
+  put_digest(ts.words[blockIdx.y], i, o);
 }
 
 // Row leaves hashM31s(col_0[r], ..., col_{C-1}[r]) (src/m31/hash.zig:15-25), and
@@ -151,7 +154,8 @@ __global__ void __launch_bounds__(kThreads) k_row_leaves(const uint32_t* __restr
 
 // Levels level0+1 .. level0+log2(CNT): thread t folds digests [t*CNT, (t+1)*CNT) of level0.
 template <int CNT>
-__global__ void __launch_bounds__(kThreads) k_tree_up(uint32_t* tree_words, unsigned log_n, unsigned level0) {
+__global__ void __launch_bounds__(kThreads) k_tree_up(TreeSet ts, unsigned log_n, unsigned level0) {
+  uint32_t* tree_words = ts.words[blockIdx.y];
   const uint64_t count = ((uint64_t)1 << (log_n - level0)) / CNT;
   const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count) return;
@@ -167,9 +171,10 @@ __global__ void __launch_bounds__(kThreads) k_tree_up(uint32_t* tree_words, unsi
 // are latency-bound (few nodes, each a chain of two compressions), so one launch
 // replaces one launch per level; with levels = log_n - level0 one CTA finishes the tree.
 constexpr unsigned kTopMax = 1024;
-__global__ void __launch_bounds__(kTopMax / 2) k_tree_block(uint32_t* tree_words, unsigned log_n, unsigned level0,
+__global__ void __launch_bounds__(kTopMax / 2) k_tree_block(TreeSet ts, unsigned log_n, unsigned level0,
                                                             unsigned levels) {
   __shared__ uint32_t s[kTopMax][8];
+  uint32_t* tree_words = ts.words[blockIdx.y];
   const size_t N2 = (size_t)2 << log_n;
   uint32_t cnt = 1u << levels;
   const uint32_t first = blockIdx.x << levels;  // first digest of this CTA at level0
@@ -197,13 +202,14 @@ static unsigned log2u(uint64_t x) {
   return l;
 }
 
-static void launch_up(DeviceTree& tree, unsigned lvl, unsigned s, cudaStream_t st) {
-  const uint64_t threads_total = ((uint64_t)1 << (tree.log_n - lvl)) >> s;
-  const unsigned blocks = (unsigned)((threads_total + kThreads - 1) / kThreads);
+static void launch_up(const TreeSet& ts, uint32_t count, unsigned log_n, unsigned lvl, unsigned s,
+                      cudaStream_t st) {
+  const uint64_t threads_total = ((uint64_t)1 << (log_n - lvl)) >> s;
+  const dim3 grid((unsigned)((threads_total + kThreads - 1) / kThreads), count);
   switch (s) {
-    case 1: k_tree_up<2><<<blocks, kThreads, 0, st>>>(tree.words, tree.log_n, lvl); break;
-    case 2: k_tree_up<4><<<blocks, kThreads, 0, st>>>(tree.words, tree.log_n, lvl); break;
-    default: k_tree_up<8><<<blocks, kThreads, 0, st>>>(tree.words, tree.log_n, lvl); break;
+    case 1: k_tree_up<2><<<grid, kThreads, 0, st>>>(ts, log_n, lvl); break;
+    case 2: k_tree_up<4><<<grid, kThreads, 0, st>>>(ts, log_n, lvl); break;
+    default: k_tree_up<8><<<grid, kThreads, 0, st>>>(ts, log_n, lvl); break;
   }
 }
 
@@ -216,20 +222,30 @@ static unsigned levels_per_launch(unsigned log_n, unsigned lvl) {
   return 1;
 }
 
-void tree_finish(DeviceTree& tree, unsigned from_level, cudaStream_t st) {
+static void finish_set(const TreeSet& ts, uint32_t count, unsigned log_n, unsigned from_level, cudaStream_t st) {
   unsigned lvl = from_level;
-  while (lvl < tree.log_n) {
-    const unsigned rem = tree.log_n - lvl;
-    if (levels_per_launch(tree.log_n, lvl) == 3) {  // wide levels: subtrees per thread
-      launch_up(tree, lvl, 3, st);
+  while (lvl < log_n) {
+    const unsigned rem = log_n - lvl;
+    if (levels_per_launch(log_n, lvl) == 3) {  // wide levels: subtrees per thread
+      launch_up(ts, count, log_n, lvl, 3, st);
       lvl += 3;
       continue;
     }
     const unsigned levels = rem < 10 ? rem : 10;  // narrow levels: subtrees per CTA
-    k_tree_block<<<1u << (rem - levels), kTopMax / 2, 0, st>>>(tree.words, tree.log_n, lvl, levels);
+    k_tree_block<<<dim3(1u << (rem - levels), count), kTopMax / 2, 0, st>>>(ts, log_n, lvl, levels);
     lvl += levels;
   }
   ZS_CUDA(cudaGetLastError());
+}
+
+static TreeSet single(const DeviceTree& tree) {
+  TreeSet ts{};
+  ts.words[0] = tree.words;
+  return ts;
+}
+
+void tree_finish(DeviceTree& tree, unsigned from_level, cudaStream_t st) {
+  finish_set(single(tree), 1, tree.log_n, from_level, st);
 }
 
 uint32_t tree_finish_launches(unsigned log_n, unsigned from_level) {
@@ -242,16 +258,32 @@ uint32_t tree_finish_launches(unsigned log_n, unsigned from_level) {
 }
 
 void build_qm31_tree(const qm31* d_values, DeviceTree& tree, cudaStream_t st) {
-  const uint64_t n = (uint64_t)1 << tree.log_n;
-  k_qm31_leaves<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(d_values, tree.words, n);
-  ZS_CUDA(cudaGetLastError());
+  build_qm31_leaves(d_values, tree, st);
   tree_finish(tree, 0, st);
 }
 
 void build_qm31_leaves(const qm31* d_values, DeviceTree& tree, cudaStream_t st) {
   const uint64_t n = (uint64_t)1 << tree.log_n;
-  k_qm31_leaves<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(d_values, tree.words, n);
+  k_qm31_leaves<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(d_values, 0, single(tree), n);
   ZS_CUDA(cudaGetLastError());
+}
+
+void build_qm31_trees(const qm31* d_values, size_t v_stride, DeviceTree* const* trees, uint32_t count,
+                      cudaStream_t st) {
+  for (uint32_t t0 = 0; t0 < count; t0 += kTreeBatch) {
+    const uint32_t c = std::min<uint32_t>(kTreeBatch, count - t0);
+    const unsigned log_n = trees[t0]->log_n;
+    TreeSet ts{};
+    for (uint32_t k = 0; k < c; ++k) {
+      if (trees[t0 + k]->log_n != log_n) throw Error(ZS_EGENERIC, "build_qm31_trees: trees of different sizes");
+      ts.words[k] = trees[t0 + k]->words;
+    }
+    const uint64_t n = (uint64_t)1 << log_n;
+    k_qm31_leaves<<<dim3((unsigned)((n + kThreads - 1) / kThreads), c), kThreads, 0, st>>>(
+        d_values + (size_t)t0 * v_stride, v_stride, ts, n);
+    ZS_CUDA(cudaGetLastError());
+    finish_set(ts, c, log_n, 0, st);
+  }
 }
 
 void build_row_leaves(const uint32_t* d_cols, size_t col_stride, uint32_t C, DeviceTree& tree, const qm31* d_gammas,

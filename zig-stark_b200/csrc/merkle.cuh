@@ -25,6 +25,17 @@ struct DeviceTree {
 
 // Leaves hashQM31(values[i]) for 2^log_n QM31 values plus the whole tree.
 void build_qm31_tree(const qm31* d_values, DeviceTree& tree, cudaStream_t st);
+
+// Device tree pointers of a set of trees built by the same launches (blockIdx.y picks
+// the tree): small trees are latency-bound, so one launch per level range serves all.
+constexpr uint32_t kTreeBatch = 64;
+struct TreeSet {
+  uint32_t* words[kTreeBatch];
+};
+// build_qm31_tree for `count` trees of one size: tree k over the values at
+// d_values + k * v_stride.
+void build_qm31_trees(const qm31* d_values, size_t v_stride, DeviceTree* const* trees, uint32_t count,
+                      cudaStream_t st);
 // Leaves only (level 0) of build_qm31_tree.
 void build_qm31_leaves(const qm31* d_values, DeviceTree& tree, cudaStream_t st);
 // Completes levels above `from_level` (levels <= from_level must be written), three

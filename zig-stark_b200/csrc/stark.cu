@@ -237,6 +237,13 @@ struct OwnedTree {
   ~OwnedTree() { cudaFreeAsync(t.words, st); }
 };
 
+// The DeviceTree pointers of trees[a, b).
+std::vector<DeviceTree*> tree_ptrs(const std::vector<std::unique_ptr<OwnedTree>>& trees, uint32_t a, uint32_t b) {
+  std::vector<DeviceTree*> v;
+  for (uint32_t j = a; j < b; ++j) v.push_back(&trees[j]->t);
+  return v;
+}
+
 // The columns of a wire []const []const QM31, located but not decoded: each element
 // is four little-endian u32 words, the device layout of a qm31, so a column's bytes
 // go to the device as they are and M31.fromBytes' reduction (m31.zig:97-100) runs
@@ -455,7 +462,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
       if (cs) cs->join();  // `st` waits for this group's columns only
       lde_qm31(vals.p + (size_t)c0 * n, n, coeffs.p + (size_t)c0 * n, n, cw.p + (size_t)c0 * N, N, c1 - c0, small,
                big, offset_pows.p, st);
-      for (uint32_t j = c0; j < c1; ++j) build_qm31_tree(cw.p + (size_t)j * N, trees[j]->t, st);
+      build_qm31_trees(cw.p + (size_t)c0 * N, N, tree_ptrs(trees, c0, c1).data(), c1 - c0, st);
     }
   }
 
@@ -509,8 +516,9 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     ZS_CUDA(cudaGetLastError());
     lde_qm31(vals.p + (size_t)(n_pre + m) * n, n, coeffs.p + (size_t)(n_pre + m) * n, n,
              cw.p + (size_t)(n_pre + m) * N, N, n_rel, small, big, offset_pows.p, st);
+    build_qm31_trees(cw.p + (size_t)(n_pre + m) * N, N, tree_ptrs(trees, n_pre + m, n_pre + m + n_rel).data(), n_rel,
+                     st);
     for (uint32_t r = 0; r < n_rel; ++r) {
-      build_qm31_tree(cw.p + (size_t)(n_pre + m + r) * N, trees[n_pre + m + r]->t, st);
       acc_roots.push_back(root_of(trees[n_pre + m + r]->t, st));
       ch.absorb(acc_roots.back());
     }
@@ -819,10 +827,15 @@ std::vector<uint8_t> commit_columns(const uint8_t* cols_b, size_t cols_len, unsi
   DevBuf<qm31> vals((size_t)C * n, st), coeffs((size_t)C * n, st), cw((size_t)C * N, st);
   upload_columns(cols, vals.p, n, st);
   lde_qm31(vals.p, n, coeffs.p, n, cw.p, N, C, small, big, offset_pows.p, st);
-  OwnedTree tree(lN, st);
-  for (uint32_t j = 0; j < C; ++j) {
-    build_qm31_tree(cw.p + (size_t)j * N, tree.t, st);
-    out.digest(root_of(tree.t, st));
+  // trees of up to 1 GiB in all are built together, then their roots read back
+  const size_t tree_bytes = DeviceTree::words_for(lN) * sizeof(uint32_t);
+  const uint32_t per = (uint32_t)std::max<size_t>(1, std::min<size_t>(kTreeBatch, ((size_t)1 << 30) / tree_bytes));
+  std::vector<std::unique_ptr<OwnedTree>> trees;
+  for (uint32_t j = 0; j < std::min(per, C); ++j) trees.push_back(std::make_unique<OwnedTree>(lN, st));
+  for (uint32_t c0 = 0; c0 < C; c0 += per) {
+    const uint32_t c = std::min(per, C - c0);
+    build_qm31_trees(cw.p + (size_t)c0 * N, N, tree_ptrs(trees, 0, c).data(), c, st);
+    for (uint32_t j = 0; j < c; ++j) out.digest(root_of(trees[j]->t, st));
   }
   return out.out;
 }
