@@ -13,6 +13,7 @@
 // All device arithmetic is exact, so every root, layer and proof byte equals the
 // reference's.
 #include <algorithm>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <vector>
@@ -237,6 +238,64 @@ struct OwnedTree {
   ~OwnedTree() { cudaFreeAsync(t.words, st); }
 };
 
+// Size-only tables (NTT twiddles, powers of FRI_OFFSET, fold tables) of sizes up to
+// 2^kCacheLog are built once per device and shared by every later proof: the first
+// use builds them on a private stream and waits for it, after which they are
+// read-only and visible to every stream. The cache is never freed (it would outlive
+// the CUDA context at process exit). Larger tables are built per proof on its stream.
+constexpr unsigned kCacheLog = 20;
+
+template <typename T, typename Make>
+const T& cached_table(unsigned log_n, Make&& make) {
+  static std::mutex mu;
+  static auto* cache = new std::map<std::pair<int, unsigned>, T*>();
+  int dev = 0;
+  ZS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache->find({dev, log_n});
+  if (it != cache->end()) return *it->second;
+  cudaStream_t s = nullptr;
+  ZS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  T* t = make(s);
+  ZS_CUDA(cudaStreamSynchronize(s));
+  ZS_CUDA(cudaStreamDestroy(s));
+  (*cache)[{dev, log_n}] = t;
+  return *t;
+}
+
+const NttTables& ntt_tables(unsigned log_n, cudaStream_t st, std::unique_ptr<NttTables>& own) {
+  if (log_n > kCacheLog) {
+    own = std::make_unique<NttTables>(log_n, st);
+    return *own;
+  }
+  return cached_table<NttTables>(log_n, [&](cudaStream_t s) { return new NttTables(log_n, s); });
+}
+
+const FoldTables& fold_tables(unsigned dlog, cudaStream_t st, std::unique_ptr<FoldTables>& own) {
+  if (dlog > kCacheLog) {
+    own = std::make_unique<FoldTables>(dlog, st);
+    return *own;
+  }
+  return cached_table<FoldTables>(dlog, [&](cudaStream_t s) { return new FoldTables(dlog, s); });
+}
+
+// FRI_OFFSET^k for k < 2^log_n.
+struct OffsetPowers {
+  qm31* p = nullptr;
+  OffsetPowers(unsigned log_n, cudaStream_t s) {
+    ZS_CUDA(cudaMallocAsync(&p, sizeof(qm31) << log_n, s));
+    qm31_powers(q_fri_offset(), p, 1u << log_n, s);
+  }
+};
+const qm31* offset_powers(unsigned log_n, cudaStream_t st, std::unique_ptr<DevBuf<qm31>>& own) {
+  if (log_n > kCacheLog) {
+    own = std::make_unique<DevBuf<qm31>>((size_t)1 << log_n, st);
+    qm31_powers(q_fri_offset(), own->p, 1u << log_n, st);
+    return own->p;
+  }
+  return cached_table<OffsetPowers>(log_n, [&](cudaStream_t s) { return new OffsetPowers(log_n, s); }).p;
+}
+
 // The DeviceTree pointers of trees[a, b).
 std::vector<DeviceTree*> tree_ptrs(const std::vector<std::unique_ptr<OwnedTree>>& trees, uint32_t a, uint32_t b) {
   std::vector<DeviceTree*> v;
@@ -435,9 +494,11 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
 
   // ---- LDE of preprocessed and main columns ------------------------------------
   const uint32_t ncol = n_pre + m_total;  // [pre | main | acc]
-  NttTables small(tl, st), big(lN, st);
-  DevBuf<qm31> offset_pows(n, st);
-  qm31_powers(offset, offset_pows.p, n, st);
+  std::unique_ptr<NttTables> small_own, big_own;
+  std::unique_ptr<DevBuf<qm31>> pows_own;
+  const NttTables& small = ntt_tables(tl, st, small_own);
+  const NttTables& big = ntt_tables(lN, st, big_own);
+  const qm31* offset_pows = offset_powers(tl, st, pows_own);
   DevBuf<qm31> vals((size_t)ncol * n, st), coeffs((size_t)ncol * n, st), cw((size_t)ncol * N, st);
   std::vector<std::unique_ptr<OwnedTree>> trees;
   for (uint32_t j = 0; j < ncol; ++j) trees.push_back(std::make_unique<OwnedTree>(lN, st));
@@ -461,7 +522,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
       upload_columns(gt, vals.p + (size_t)std::max(c0, n_pre) * n, n, up);
       if (cs) cs->join();  // `st` waits for this group's columns only
       lde_qm31(vals.p + (size_t)c0 * n, n, coeffs.p + (size_t)c0 * n, n, cw.p + (size_t)c0 * N, N, c1 - c0, small,
-               big, offset_pows.p, st);
+               big, offset_pows, st);
       build_qm31_trees(cw.p + (size_t)c0 * N, N, tree_ptrs(trees, c0, c1).data(), c1 - c0, st);
     }
   }
@@ -515,7 +576,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     }
     ZS_CUDA(cudaGetLastError());
     lde_qm31(vals.p + (size_t)(n_pre + m) * n, n, coeffs.p + (size_t)(n_pre + m) * n, n,
-             cw.p + (size_t)(n_pre + m) * N, N, n_rel, small, big, offset_pows.p, st);
+             cw.p + (size_t)(n_pre + m) * N, N, n_rel, small, big, offset_pows, st);
     build_qm31_trees(cw.p + (size_t)(n_pre + m) * N, N, tree_ptrs(trees, n_pre + m, n_pre + m + n_rel).data(), n_rel,
                      st);
     for (uint32_t r = 0; r < n_rel; ++r) {
@@ -625,7 +686,8 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   k_deep<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_dc.p, layers[0]->p);
   ZS_CUDA(cudaGetLastError());
 
-  FoldTables ftabs(lN, st);
+  std::unique_ptr<FoldTables> ftabs_own;
+  const FoldTables& ftabs = fold_tables(lN, st, ftabs_own);
   std::vector<std::unique_ptr<OwnedTree>> ftrees;
   for (unsigned i = 0; i < L; ++i) ftrees.push_back(std::make_unique<OwnedTree>(lN - i, st));
   // The commit phase (fri.zig:195-227) runs without host round trips: per layer a
@@ -821,12 +883,14 @@ std::vector<uint8_t> commit_columns(const uint8_t* cols_b, size_t cols_len, unsi
   WireWriter out;
   out.u64(C);
   if (C == 0) return out.out;
-  NttTables small(trace_log, st), big(lN, st);
-  DevBuf<qm31> offset_pows(n, st);
-  qm31_powers(q_fri_offset(), offset_pows.p, n, st);
+  std::unique_ptr<NttTables> small_own, big_own;
+  std::unique_ptr<DevBuf<qm31>> pows_own;
+  const NttTables& small = ntt_tables(trace_log, st, small_own);
+  const NttTables& big = ntt_tables(lN, st, big_own);
+  const qm31* offset_pows = offset_powers(trace_log, st, pows_own);
   DevBuf<qm31> vals((size_t)C * n, st), coeffs((size_t)C * n, st), cw((size_t)C * N, st);
   upload_columns(cols, vals.p, n, st);
-  lde_qm31(vals.p, n, coeffs.p, n, cw.p, N, C, small, big, offset_pows.p, st);
+  lde_qm31(vals.p, n, coeffs.p, n, cw.p, N, C, small, big, offset_pows, st);
   // trees of up to 1 GiB in all are built together, then their roots read back
   const size_t tree_bytes = DeviceTree::words_for(lN) * sizeof(uint32_t);
   const uint32_t per = (uint32_t)std::max<size_t>(1, std::min<size_t>(kTreeBatch, ((size_t)1 << 30) / tree_bytes));
