@@ -3,6 +3,7 @@
 // FRI commitment, then the fold chain with one fused fold+commit launch per layer.
 #include <algorithm>
 #include <cstdlib>
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -19,7 +20,15 @@ CommitPlan::CommitPlan(uint32_t C_, unsigned L_, unsigned B_, unsigned F_) : C(C
   ZS_CUDA(cudaStreamCreateWithFlags(&setup, cudaStreamNonBlocking));
   ZS_CUDA(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
   for (auto& s : sides) ZS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  up_events.resize(kUploadGroups + 1);
+  // Group sizes grow by about 4/3 from 2 columns at the end, so each group's LDE is
+  // done before the next group's copy (the LDE of a column takes about 0.6 of its
+  // copy over PCIe) and the step waits for a small group's LDE after the last copy.
+  for (uint32_t g = 2, used = 0; used < C; g = std::max(g + 1, (g * 4 + 2) / 3)) {
+    upload_groups.push_back(std::min(g, C - used));
+    used += upload_groups.back();
+  }
+  std::sort(upload_groups.begin(), upload_groups.end(), std::greater<uint32_t>());
+  up_events.resize(upload_groups.size() + 1);
   for (auto& e : up_events) ZS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   events.resize(F + 2 + kSides);
   for (auto& e : events) ZS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -112,19 +121,17 @@ void CommitPlan::run_direct(const uint32_t* d_trace, cudaStream_t st) {
 // LDEs run in order on `st` and share the scratch buffer (sized for all C columns).
 void CommitPlan::run_host_direct(const uint32_t* h_trace, cudaStream_t st) {
   const size_t n = (size_t)1 << L, N = (size_t)1 << (L + B);
-  const uint32_t per = (C + kUploadGroups - 1) / kUploadGroups;
-  ZS_CUDA(cudaEventRecord(up_events[kUploadGroups], st));  // the previous step is done with `trace`
-  ZS_CUDA(cudaStreamWaitEvent(copy, up_events[kUploadGroups], 0));
-  for (uint32_t g = 0, c0 = 0; c0 < C; ++g, c0 += per) {
-    const uint32_t cols = std::min(per, C - c0);
-    ZS_CUDA(cudaMemcpyAsync(trace + c0 * n, h_trace + c0 * n, (size_t)cols * n * sizeof(uint32_t),
+  const size_t G = upload_groups.size();
+  ZS_CUDA(cudaEventRecord(up_events[G], st));  // the previous step is done with `trace`
+  ZS_CUDA(cudaStreamWaitEvent(copy, up_events[G], 0));
+  for (size_t g = 0, c0 = 0; g < G; c0 += upload_groups[g++]) {
+    ZS_CUDA(cudaMemcpyAsync(trace + c0 * n, h_trace + c0 * n, (size_t)upload_groups[g] * n * sizeof(uint32_t),
                             cudaMemcpyHostToDevice, copy));
     ZS_CUDA(cudaEventRecord(up_events[g], copy));
   }
-  for (uint32_t g = 0, c0 = 0; c0 < C; ++g, c0 += per) {
-    const uint32_t cols = std::min(per, C - c0);
+  for (size_t g = 0, c0 = 0; g < G; c0 += upload_groups[g++]) {
     ZS_CUDA(cudaStreamWaitEvent(st, up_events[g], 0));
-    circle_lde(trace + c0 * n, n, lde + c0 * N, N, cols, L, B, *small, *big, scratch, st);
+    circle_lde(trace + c0 * n, n, lde + c0 * N, N, upload_groups[g], L, B, *small, *big, scratch, st);
   }
   after_lde(st);
 }

@@ -43,7 +43,9 @@ struct CommitPlan {
   // the step; replayed as one captured graph per host pointer.
   void run_host(const uint32_t* h_trace, cudaStream_t st);
   void run_host_direct(const uint32_t* h_trace, cudaStream_t st);
-  static constexpr unsigned kUploadGroups = 8;
+  // Column counts of the upload groups, largest first: after the last copy only the
+  // last (smallest) group's LDE precedes the rest of the step.
+  std::vector<uint32_t> upload_groups;
 
  private:
   static constexpr unsigned kSides = 3;
@@ -54,7 +56,7 @@ struct CommitPlan {
   cudaGraphExec_t graph_exec = nullptr;
   const uint32_t* graph_trace = nullptr;
   cudaStream_t copy = nullptr;
-  std::vector<cudaEvent_t> up_events;  // kUploadGroups + 1
+  std::vector<cudaEvent_t> up_events;  // one per upload group, plus one
   cudaGraphExec_t host_exec = nullptr;
   const uint32_t* host_trace = nullptr;
   void drop_graph();
