@@ -166,3 +166,24 @@ def test_context_rejects_bad_device():
     with pytest.raises(native.ZsError) as e:
         native.Context(1 << 20)
     assert e.value.code == -5
+
+
+def test_maximum_size_proof_verifies():
+    """The largest domain the prover takes: 2^24 rows at blowup 4 (2^26 points). Too
+    large for the oracle prover in test time, so the proof is checked by the library's
+    verifier, a flipped byte must make it fail, and one size more is refused up front."""
+    from zs_b200 import native
+    tr, pi = wl.seeded_fib(24)
+    params = wire.StarkParams(24, 2, 16, 3)
+    proof = native.prove(wl.AIR_SEEDED_FIB, params, pi, tr, b"", b"max")
+    assert native.verify(wl.AIR_SEEDED_FIB, params, pi, proof, b"max")
+    bad = bytearray(proof)
+    bad[len(bad) // 2] ^= 1
+    try:
+        ok = native.verify(wl.AIR_SEEDED_FIB, params, pi, bytes(bad), b"max")
+    except native.ZsError:
+        ok = False
+    assert not ok
+    with pytest.raises(native.ZsError) as e:
+        native.prove(wl.AIR_SEEDED_FIB, wire.StarkParams(25, 2, 16, 3), pi, tr, b"", b"max")
+    assert e.value.code == -2
