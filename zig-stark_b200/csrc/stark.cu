@@ -110,31 +110,46 @@ __global__ void k_scan_add(qm31* out, uint32_t n, const qm31* block_prefix) {
   if (i < n && blockIdx.x > 0) stq(out + i, qadd(ldq(out + i), ldq(block_prefix + blockIdx.x)));
 }
 
-// partial[pt][col][blk] = sum over the block's j of coeffs[col][j] * zpow[pt][bitrev(j)]
-// (the coefficients are stored in bit-reversed order, log_n = log2 n).
-__global__ void __launch_bounds__(kT) k_eval_partial(const qm31* __restrict__ coeffs, uint32_t n, unsigned log_n,
-                                                     const qm31* __restrict__ zpow, uint32_t npt, qm31* partial) {
-  __shared__ qm31 s[kT];
-  const uint32_t col = blockIdx.y, pt = blockIdx.z;
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  qm31 v = qzero();
-  if (j < n) v = qmul(ldq(coeffs + (size_t)col * n + j), ldq(zpow + (size_t)pt * n + bitrev(j, log_n)));
+// A block's kT threads sum kT * kEvalPer terms; QM31 addition is exact, so the order
+// of the sums does not change the result.
+constexpr uint32_t kEvalPer = 8;
+
+__device__ __forceinline__ qm31 block_sum(qm31 v, qm31* s) {
   s[threadIdx.x] = v;
   __syncthreads();
   for (uint32_t d = blockDim.x / 2; d > 0; d >>= 1) {
     if (threadIdx.x < d) s[threadIdx.x] = qadd(s[threadIdx.x], s[threadIdx.x + d]);
     __syncthreads();
   }
-  if (threadIdx.x == 0) stq(partial + ((size_t)pt * gridDim.y + col) * gridDim.x + blockIdx.x, s[0]);
+  return s[0];
 }
 
-// Sums `nblk` partials per (pt, col) sequentially (nblk is small).
-__global__ void k_eval_sum(const qm31* partial, uint32_t nblk, uint32_t count, qm31* out) {
-  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= count) return;
+// partial[pt][col][blk] = sum over the block's j of coeffs[col][j] * zpow[pt][bitrev(j)]
+// (the coefficients are stored in bit-reversed order, log_n = log2 n).
+__global__ void __launch_bounds__(kT) k_eval_partial(const qm31* __restrict__ coeffs, uint32_t n, unsigned log_n,
+                                                     const qm31* __restrict__ zpow, uint32_t npt, qm31* partial) {
+  __shared__ qm31 s[kT];
+  const uint32_t col = blockIdx.y, pt = blockIdx.z;
+  const qm31* c = coeffs + (size_t)col * n;
+  const qm31* zp = zpow + (size_t)pt * n;
   qm31 acc = qzero();
-  for (uint32_t b = 0; b < nblk; ++b) acc = qadd(acc, ldq(partial + (size_t)idx * nblk + b));
-  stq(out + idx, acc);
+#pragma unroll
+  for (uint32_t k = 0; k < kEvalPer; ++k) {
+    const uint32_t j = (blockIdx.x * kEvalPer + k) * blockDim.x + threadIdx.x;
+    if (j < n) acc = qadd(acc, qmul(ldq(c + j), ldq(zp + bitrev(j, log_n))));
+  }
+  const qm31 sum = block_sum(acc, s);
+  if (threadIdx.x == 0) stq(partial + ((size_t)pt * gridDim.y + col) * gridDim.x + blockIdx.x, sum);
+}
+
+// out[idx] = the sum of the `nblk` partials of (pt, col) = idx, one CTA each.
+__global__ void __launch_bounds__(kT) k_eval_sum(const qm31* partial, uint32_t nblk, qm31* out) {
+  __shared__ qm31 s[kT];
+  const qm31* p = partial + (size_t)blockIdx.x * nblk;
+  qm31 acc = qzero();
+  for (uint32_t b = threadIdx.x; b < nblk; b += blockDim.x) acc = qadd(acc, ldq(p + b));
+  const qm31 sum = block_sum(acc, s);
+  if (threadIdx.x == 0) stq(out + blockIdx.x, sum);
 }
 
 // DEEP codeword (stark.zig:577-588), with 1/(d_i - z) factored out of the sum.
@@ -653,10 +668,10 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     DevBuf<qm31> zpow((size_t)2 * n, st);
     qm31_powers(z, zpow.p, n, st);
     qm31_powers(wz, zpow.p + n, n, st);
-    const uint32_t nblk = (n + kT - 1) / kT;
+    const uint32_t nblk = (n + kT * kEvalPer - 1) / (kT * kEvalPer);
     DevBuf<qm31> partial((size_t)2 * ncol * nblk, st), sums((size_t)2 * ncol, st);
     k_eval_partial<<<dim3(nblk, ncol, 2), kT, 0, st>>>(coeffs.p, n, tl, zpow.p, 2, partial.p);
-    k_eval_sum<<<(2 * ncol + 63) / 64, 64, 0, st>>>(partial.p, nblk, 2 * ncol, sums.p);
+    k_eval_sum<<<2 * ncol, kT, 0, st>>>(partial.p, nblk, sums.p);
     ZS_CUDA(cudaGetLastError());
     std::vector<qm31> hs(2 * ncol);
     d2h_small(hs.data(), sums.p, hs.size() * sizeof(qm31), st);
