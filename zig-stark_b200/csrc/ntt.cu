@@ -37,7 +37,7 @@ __device__ __forceinline__ void stq(qm31* p, const qm31& v) {
 }
 __device__ __forceinline__ cm31 cshl(cm31 x, unsigned k) { return {mshl(x.a, k), mshl(x.b, k)}; }
 // The CRT image (u, v) of a QM31 value, held in the a (u) and b (v) slots of a qm31.
-__device__ __forceinline__ qm31 to_crt(const qm31& x) {
+ZS_HD qm31 to_crt(const qm31& x) {
   // b s = 2^15 (1 - i)(c + d i) = 2^15 ((c + d) + (d - c) i)
   const cm31 bs = {mshl(madd(x.b.a, x.b.b), 15), mshl(msub(x.b.b, x.b.a), 15)};
   return {cadd(x.a, bs), csub(x.a, bs)};
@@ -52,6 +52,12 @@ __device__ __forceinline__ qm31 from_crt(const qm31& y) {
 __device__ __forceinline__ qm31 crt_mul(const qm31& x, const qm31& y) { return {cmul(x.a, y.a), cmul(x.b, y.b)}; }
 __device__ __forceinline__ qm31 crt_add(const qm31& x, const qm31& y) { return {cadd(x.a, y.a), cadd(x.b, y.b)}; }
 __device__ __forceinline__ qm31 crt_sub(const qm31& x, const qm31& y) { return {csub(x.a, y.a), csub(x.b, y.b)}; }
+__device__ __forceinline__ qm31 crt_neg(const qm31& x) { return {{mneg(x.a.a), mneg(x.a.b)}, {mneg(x.b.a), mneg(x.b.b)}}; }
+// Products with the 4th root of unity. w_N^(N/4) = w_4 for every N (the roots are
+// powers of one 2-adic root), and its CRT image is J = (i, -i), so J^-1 = (-i, i);
+// NttTables checks both. (a + b i) i = -b + a i.
+__device__ __forceinline__ qm31 crt_mul_j(const qm31& x) { return {{mneg(x.a.b), x.a.a}, {x.b.b, mneg(x.b.a)}}; }
+__device__ __forceinline__ qm31 crt_mul_jinv(const qm31& x) { return {{x.a.b, mneg(x.a.a)}, {mneg(x.b.b), x.b.a}}; }
 }  // namespace
 
 // pows[k] = x^k: each thread raises x to its first index, then multiplies along a
@@ -81,6 +87,12 @@ __global__ void k_to_crt(const qm31* in, qm31* out, uint32_t count) {
 
 NttTables::NttTables(unsigned l, cudaStream_t s) : log_n(l), st(s) {
   if (log_n > 30) throw Error(ZS_EMALFORMED, "NTT size above 2^30");
+  {  // the radix-4 passes multiply by J = phi(w_4) = (i, -i) as a rotation of the components
+    const qm31 j = to_crt(q_root_of_unity(2)), ji = to_crt(qinv(q_root_of_unity(2)));
+    if (!(j.a.a == 0 && j.a.b == 1 && j.b.a == 0 && j.b.b == P - 1 && ji.a.a == 0 && ji.a.b == P - 1 &&
+          ji.b.a == 0 && ji.b.b == 1))
+      throw Error(ZS_EGENERIC, "unexpected CRT image of the 4th root of unity");
+  }
   const uint32_t half = log_n == 0 ? 1 : (1u << (log_n - 1));
   ZS_CUDA(cudaMallocAsync(&fwd, half * sizeof(qm31), st));
   ZS_CUDA(cudaMallocAsync(&inv_crt, half * sizeof(qm31), st));
@@ -100,40 +112,47 @@ NttTables::~NttTables() {
 
 // Two stages (b, b + 1) on the four elements m0 + {0, 1, 2, 3} * 2^b of each group in
 // shared memory (see k_ntt_pass), one quadruple per thread iteration, then a barrier.
+// As a radix-4 step: with t1 = tw[2 i], t2 = tw[i] (i = k 2^(logN - st - 1)) the upper
+// pair's twiddle of stage b + 1 is tw[i + N/4] = t2 J (J^-1 in the inverse table), so
+// the two stages need three products, by t1, t2 and t3 = t1 t2 = tw[3 i]
+// (= -tw[3 i - N/2] past the table's end, w^(N/2) = -1), and one rotation by J:
+//   DIT: P = t1 e1, A = t2 e2, B = t3 e3:
+//        e0 + P + (A + B), e0 - P + J (A - B), e0 + P - (A + B), e0 - P - J (A - B)
+//   DIF: S0 = e0 + e2, S1 = e1 + e3, A = e0 - e2, C = J^-1 (e1 - e3):
+//        S0 + S1, t1 (S0 - S1), t2 (A + C), t3 (A - C)
+// the same values as the two radix-2 stages, by distributivity.
 template <bool DIF>
 __device__ __forceinline__ void ntt_radix4(qm31* s, unsigned M, uint32_t G, unsigned lo, unsigned logN, uint32_t l0,
                                            unsigned b, const qm31* __restrict__ tw) {
   const uint32_t hb = 1u << b, total = G << M;
   const unsigned st = lo + 1 + b;
+  const size_t half = (size_t)1 << (logN - 1);
   for (uint32_t q = threadIdx.x; q < (total >> 2); q += blockDim.x) {
     const uint32_t t = q >> (M - 2), r = q & ((1u << (M - 2)) - 1);
     const uint32_t m0 = ((r >> b) << (b + 2)) | (r & (hb - 1));
     const uint32_t k = ((m0 & (hb - 1)) << lo) | (l0 + t);
-    const qm31 t1 = ldq(tw + ((size_t)k << (logN - st)));
-    const qm31 t2a = ldq(tw + ((size_t)k << (logN - st - 1)));
-    const qm31 t2b = ldq(tw + ((size_t)(k + (hb << lo)) << (logN - st - 1)));
+    const size_t i2 = (size_t)k << (logN - st - 1), i3 = 3 * i2;
+    const qm31 t1 = ldq(tw + 2 * i2);
+    const qm31 t2 = ldq(tw + i2);
+    const qm31 t3 = i3 < half ? ldq(tw + i3) : crt_neg(ldq(tw + (i3 - half)));
     qm31* p = s + (t << M) + m0;
-    qm31 e0 = p[0], e1 = p[hb], e2 = p[2 * hb], e3 = p[3 * hb];
+    const qm31 e0 = p[0], e1 = p[hb], e2 = p[2 * hb], e3 = p[3 * hb];
     if (!DIF) {
-      qm31 u = crt_mul(t1, e1);
-      e1 = crt_sub(e0, u), e0 = crt_add(e0, u);
-      u = crt_mul(t1, e3);
-      e3 = crt_sub(e2, u), e2 = crt_add(e2, u);
-      u = crt_mul(t2a, e2);
-      e2 = crt_sub(e0, u), e0 = crt_add(e0, u);
-      u = crt_mul(t2b, e3);
-      e3 = crt_sub(e1, u), e1 = crt_add(e1, u);
+      const qm31 P1 = crt_mul(t1, e1), A = crt_mul(t2, e2), B = crt_mul(t3, e3);
+      const qm31 s0 = crt_add(e0, P1), d0 = crt_sub(e0, P1);
+      const qm31 sab = crt_add(A, B), jd = crt_mul_j(crt_sub(A, B));
+      p[0] = crt_add(s0, sab);
+      p[hb] = crt_add(d0, jd);
+      p[2 * hb] = crt_sub(s0, sab);
+      p[3 * hb] = crt_sub(d0, jd);
     } else {
-      qm31 d = crt_sub(e0, e2);
-      e0 = crt_add(e0, e2), e2 = crt_mul(d, t2a);
-      d = crt_sub(e1, e3);
-      e1 = crt_add(e1, e3), e3 = crt_mul(d, t2b);
-      d = crt_sub(e0, e1);
-      e0 = crt_add(e0, e1), e1 = crt_mul(d, t1);
-      d = crt_sub(e2, e3);
-      e2 = crt_add(e2, e3), e3 = crt_mul(d, t1);
+      const qm31 s0 = crt_add(e0, e2), s1 = crt_add(e1, e3);
+      const qm31 a = crt_sub(e0, e2), c = crt_mul_jinv(crt_sub(e1, e3));
+      p[0] = crt_add(s0, s1);
+      p[hb] = crt_mul(crt_sub(s0, s1), t1);
+      p[2 * hb] = crt_mul(crt_add(a, c), t2);
+      p[3 * hb] = crt_mul(crt_sub(a, c), t3);
     }
-    p[0] = e0, p[hb] = e1, p[2 * hb] = e2, p[3 * hb] = e3;
   }
   __syncthreads();
 }
