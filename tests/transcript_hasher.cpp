@@ -3,9 +3,9 @@
 //   B <n> <hex>        absorb n bytes
 //   W <n> <w0> ...     absorb n little-endian words (hex)
 //   F                  print finalize()
-//   S <n> <w0> ...     print the digest of the state extended by n words (a sample:
-//                      a snapshot of the state absorbs them and is finalized), state
-//                      unchanged
+//   S <n> <w0> ...     print the digest of the state extended by n words twice: from a
+//                      snapshot that absorbs them and is finalized, and from
+//                      finalize_suffix (no snapshot); state unchanged
 #include <cstdio>
 #include <vector>
 
@@ -41,6 +41,11 @@ int main() {
         uint8_t o[32];
         snap.finalize(o);
         for (int i = 0; i < 32; ++i) std::printf("%02x", o[i]);
+        std::printf("\n");
+        uint32_t f[8];  // the same digest without a snapshot
+        h.finalize_suffix(b.data(), (unsigned)b.size(), f);
+        for (int i = 0; i < 8; ++i)
+          for (int k = 0; k < 4; ++k) std::printf("%02x", (f[i] >> (8 * k)) & 0xff);
         std::printf("\n");
       }
     } else if (op == 'F') {

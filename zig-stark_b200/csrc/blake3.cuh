@@ -127,6 +127,44 @@ ZS_HD void compress_full(const uint32_t cv[8], const uint32_t m[16], uint64_t co
   out[15] = v15 ^ cv[7];
 }
 
+#ifdef __CUDA_ARCH__
+// compress_full with the rounds in a loop and the message permuted between rounds
+// (m'[i] = m[PERM[i]], PERM = 2 6 3 10 7 0 4 13 1 11 12 5 9 14 15 8), not inlined:
+// a few hundred bytes of code instead of several kilobytes per inlined copy. The
+// device transcript runs in one thread per kernel, often with cold caches, where
+// fetching unrolled code costs more than the rounds.
+static __device__ __noinline__ void compress_rolled(const uint32_t cv[8], const uint32_t m_in[16],
+                                                    uint64_t counter, uint32_t block_len, uint32_t flags,
+                                                    uint32_t out[16]) {
+  uint32_t m[16];
+  for (int i = 0; i < 16; ++i) m[i] = m_in[i];
+  uint32_t v0 = cv[0], v1 = cv[1], v2 = cv[2], v3 = cv[3], v4 = cv[4], v5 = cv[5], v6 = cv[6], v7 = cv[7];
+  uint32_t v8 = IV0, v9 = IV1, v10 = IV2, v11 = IV3;
+  uint32_t v12 = (uint32_t)counter, v13 = (uint32_t)(counter >> 32), v14 = block_len, v15 = flags;
+#pragma unroll 1
+  for (int r = 0; r < 7; ++r) {
+    ZS_B3_ROUND(m, 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15)
+    const uint32_t t0 = m[2], t1 = m[6], t2 = m[3], t3 = m[10], t4 = m[7], t5 = m[0], t6 = m[4], t7 = m[13];
+    const uint32_t t8 = m[1], t9 = m[11], t10 = m[12], t11 = m[5], t12 = m[9], t13 = m[14], t14 = m[15], t15 = m[8];
+    m[0] = t0, m[1] = t1, m[2] = t2, m[3] = t3, m[4] = t4, m[5] = t5, m[6] = t6, m[7] = t7;
+    m[8] = t8, m[9] = t9, m[10] = t10, m[11] = t11, m[12] = t12, m[13] = t13, m[14] = t14, m[15] = t15;
+  }
+  out[0] = v0 ^ v8, out[1] = v1 ^ v9, out[2] = v2 ^ v10, out[3] = v3 ^ v11;
+  out[4] = v4 ^ v12, out[5] = v5 ^ v13, out[6] = v6 ^ v14, out[7] = v7 ^ v15;
+  out[8] = v8 ^ cv[0], out[9] = v9 ^ cv[1], out[10] = v10 ^ cv[2], out[11] = v11 ^ cv[3];
+  out[12] = v12 ^ cv[4], out[13] = v13 ^ cv[5], out[14] = v14 ^ cv[6], out[15] = v15 ^ cv[7];
+}
+#endif
+// The transcript's compression: unrolled on the host, compress_rolled on the device.
+ZS_HD void compress_tx(const uint32_t cv[8], const uint32_t m[16], uint64_t counter, uint32_t block_len,
+                       uint32_t flags, uint32_t out[16]) {
+#ifdef __CUDA_ARCH__
+  compress_rolled(cv, m, counter, block_len, flags, out);
+#else
+  compress_full(cv, m, counter, block_len, flags, out);
+#endif
+}
+
 ZS_HD void iv(uint32_t cv[8]) {
   cv[0] = IV0; cv[1] = IV1; cv[2] = IV2; cv[3] = IV3;
   cv[4] = IV4; cv[5] = IV5; cv[6] = IV6; cv[7] = IV7;
@@ -240,7 +278,7 @@ struct Hasher {
       copy_bytes(m + 8, c, 32);
       uint32_t k[8];
       b3::iv(k);
-      b3::compress_full(k, m, 0, 64, b3::PARENT, out);
+      b3::compress_tx(k, m, 0, 64, b3::PARENT, out);
       copy_bytes(c, out, 32);
       total >>= 1;
     }
@@ -252,7 +290,7 @@ struct Hasher {
       if (blocks_done * 64 + block_len == 1024) {
         uint32_t m[16], out[16];
         words(block, m);
-        b3::compress_full(cv, m, chunk_counter, block_len, start() | b3::CHUNK_END, out);
+        b3::compress_tx(cv, m, chunk_counter, block_len, start() | b3::CHUNK_END, out);
         ++chunk_counter;
         push(out, chunk_counter);
         b3::iv(cv);
@@ -262,7 +300,7 @@ struct Hasher {
       if (block_len == 64) {
         uint32_t m[16], out[16];
         words(block, m);
-        b3::compress_full(cv, m, chunk_counter, 64, start(), out);
+        b3::compress_tx(cv, m, chunk_counter, 64, start(), out);
         copy_bytes(cv, out, 32);
         ++blocks_done;
         for (int i = 0; i < 64; ++i) block[i] = 0;
@@ -281,15 +319,15 @@ struct Hasher {
     words(block, m);
     uint32_t flags = start() | b3::CHUNK_END;
     if (depth == 0) {
-      b3::compress_full(cv, m, chunk_counter, block_len, flags | b3::ROOT, out);
+      b3::compress_tx(cv, m, chunk_counter, block_len, flags | b3::ROOT, out);
     } else {
-      b3::compress_full(cv, m, chunk_counter, block_len, flags, out);
+      b3::compress_tx(cv, m, chunk_counter, block_len, flags, out);
       for (unsigned k = depth; k-- > 0;) {
         uint32_t pm[16], key[8];
         copy_bytes(pm, stack[k], 32);
         copy_bytes(pm + 8, out, 32);
         b3::iv(key);
-        b3::compress_full(key, pm, 0, 64, b3::PARENT | (k == 0 ? b3::ROOT : 0), out);
+        b3::compress_tx(key, pm, 0, 64, b3::PARENT | (k == 0 ? b3::ROOT : 0), out);
       }
     }
     for (int i = 0; i < 8; ++i) {
@@ -297,6 +335,57 @@ struct Hasher {
       out32[4 * i + 1] = (uint8_t)(out[i] >> 8);
       out32[4 * i + 2] = (uint8_t)(out[i] >> 16);
       out32[4 * i + 3] = (uint8_t)(out[i] >> 24);
+    }
+  }
+  // finalize() of the state followed by `n` <= 64 more bytes, state unchanged, without
+  // a snapshot: the chunk state is copied into words, the stack read in place, and a
+  // chunk finished by the suffix (at most one) becomes a virtual top of the stack.
+  ZS_HD void finalize_suffix(const uint8_t* suf, unsigned n, uint32_t o[8]) const {
+    uint32_t c[8], m[16], out[16], top[8];
+    for (int i = 0; i < 8; ++i) c[i] = cv[i];
+    words(block, m);
+    uint32_t len = block_len, blocks = blocks_done;
+    uint64_t counter = chunk_counter;
+    unsigned d = depth;
+    bool has_top = false;
+    for (unsigned i = 0; i < n; ++i) {
+      if (blocks * 64 + len == 1024) {  // chunk full: its chaining value goes on the stack
+        b3::compress_tx(c, m, counter, len, (blocks == 0 ? b3::CHUNK_START : 0) | b3::CHUNK_END, out);
+        for (int w = 0; w < 8; ++w) top[w] = out[w];
+        for (uint64_t total = counter + 1; (total & 1) == 0; total >>= 1) {
+          uint32_t pm[16], key[8];
+          for (int w = 0; w < 8; ++w) pm[w] = stack[d - 1][w], pm[8 + w] = top[w];
+          b3::iv(key);
+          b3::compress_tx(key, pm, 0, 64, b3::PARENT, out);
+          for (int w = 0; w < 8; ++w) top[w] = out[w];
+          --d;
+        }
+        has_top = true;
+        b3::iv(c);
+        for (int w = 0; w < 16; ++w) m[w] = 0;
+        len = blocks = 0;
+        ++counter;
+      } else if (len == 64) {
+        b3::compress_tx(c, m, counter, 64, blocks == 0 ? b3::CHUNK_START : 0, out);
+        for (int w = 0; w < 8; ++w) c[w] = out[w];
+        for (int w = 0; w < 16; ++w) m[w] = 0;
+        len = 0;
+        ++blocks;
+      }
+      m[len >> 2] |= (uint32_t)suf[i] << (8 * (len & 3));
+      ++len;
+    }
+    const unsigned total = d + (has_top ? 1u : 0u);
+    const uint32_t flags = (blocks == 0 ? b3::CHUNK_START : 0) | b3::CHUNK_END;
+    b3::compress_tx(c, m, counter, len, flags | (total == 0 ? b3::ROOT : 0), out);
+    for (int w = 0; w < 8; ++w) o[w] = out[w];
+    for (unsigned k = total; k-- > 0;) {
+      uint32_t pm[16], key[8];
+      const uint32_t* l = has_top && k == d ? top : stack[k];
+      for (int w = 0; w < 8; ++w) pm[w] = l[w], pm[8 + w] = o[w];
+      b3::iv(key);
+      b3::compress_tx(key, pm, 0, 64, b3::PARENT | (k == 0 ? b3::ROOT : 0), out);
+      for (int w = 0; w < 8; ++w) o[w] = out[w];
     }
   }
 };

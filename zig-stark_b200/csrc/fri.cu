@@ -102,7 +102,6 @@ __global__ void __launch_bounds__(kTailMax / 4) k_fri_tail(const FriTail* __rest
   const FriTail& ft = *ftp;
   __shared__ qm31 alpha_s;
   __shared__ __align__(16) unsigned char ch_raw[sizeof(Channel)];    // the transcript, for the CTA's life
-  __shared__ __align__(16) unsigned char snap_raw[sizeof(Hasher)];  // filled by snapshot_from
   copy_state(ch_raw, ch, sizeof(Channel));
   Channel* chs = reinterpret_cast<Channel*>(ch_raw);
   __syncthreads();
@@ -141,7 +140,7 @@ __global__ void __launch_bounds__(kTailMax / 4) k_fri_tail(const FriTail* __rest
         for (int k = 0; k < 4; ++k) b[4 * w + k] = (uint8_t)(root[w] >> (8 * k));
       }
       chs->absorb_bytes(b, 32);
-      alpha_s = chs->sample_q(reinterpret_cast<Hasher*>(snap_raw));
+      alpha_s = chs->sample_q();
       ft.alphas[c] = alpha_s;
     }
     __syncthreads();

@@ -116,10 +116,22 @@ struct Channel {
       for (int k = 0; k < 4; ++k) b[4 * i + k] = (uint8_t)(w[i] >> (8 * k));
     h.update(b, 16);
   }
-  // `scratch` holds the snapshot of the state (a local copy when null).
+  // On the host a sample is drawn from a snapshot of the state (`scratch`, a local
+  // copy when null); on the device, in one thread, from the state itself extended by
+  // the suffix (Hasher::finalize_suffix), which copies no stack.
   ZS_HD void sample_bytes(uint8_t* out, size_t len, Hasher* scratch = nullptr) {
     uint64_t counter = 0;
     while (len) {
+      uint8_t blk[32];
+#ifdef __CUDA_ARCH__
+      (void)scratch;
+      uint8_t suf[24];
+      copy_bytes(suf, "zig-stark:sample", 16);
+      for (int i = 0; i < 8; ++i) suf[16 + i] = (uint8_t)(counter >> (8 * i));
+      uint32_t o[8];
+      h.finalize_suffix(suf, 24, o);
+      for (int i = 0; i < 32; ++i) blk[i] = (uint8_t)(o[i / 4] >> (8 * (i % 4)));
+#else
       Hasher local;
       Hasher& snap = scratch ? *scratch : local;
       snap.snapshot_from(h);
@@ -127,8 +139,8 @@ struct Channel {
       uint8_t cb[8];
       for (int i = 0; i < 8; ++i) cb[i] = (uint8_t)(counter >> (8 * i));
       snap.update(cb, 8);
-      uint8_t blk[32];
       snap.finalize(blk);
+#endif
       h.update(blk, 32);
       const size_t k = len < 32 ? len : 32;
       copy_bytes(out, blk, k);

@@ -196,7 +196,6 @@ struct GatherReq {
 __global__ void k_fri_transcript(Channel* ch, const uint32_t* __restrict__ root, uint32_t* __restrict__ root_out,
                                  qm31* __restrict__ alpha) {
   __shared__ __align__(16) unsigned char ch_raw[sizeof(Channel)];
-  __shared__ __align__(16) unsigned char snap_raw[sizeof(Hasher)];  // filled by snapshot_from
   copy_state(ch_raw, ch, sizeof(Channel));
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -208,7 +207,7 @@ __global__ void k_fri_transcript(Channel* ch, const uint32_t* __restrict__ root,
       for (int k = 0; k < 4; ++k) b[4 * w + k] = (uint8_t)(v >> (8 * k));
     }
     c->absorb_bytes(b, 32);
-    *alpha = c->sample_q(reinterpret_cast<Hasher*>(snap_raw));
+    *alpha = c->sample_q();
   }
   __syncthreads();
   copy_state(ch, ch_raw, sizeof(Channel));
