@@ -222,6 +222,25 @@ void d2h_small(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   std::memcpy(dst, r, bytes);
 }
 
+void d2h_many(const D2H* c, size_t count, cudaStream_t st) {
+  if (count == 0) return;
+  if (!t_slot) {
+    for (size_t k = 0; k < count; ++k)
+      if (c[k].bytes) ZS_CUDA(cudaMemcpyAsync(c[k].dst, c[k].src, c[k].bytes, cudaMemcpyDeviceToHost, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  std::vector<uint8_t*> r(count);
+  for (size_t k = 0; k < count; ++k) {
+    if (!c[k].bytes) continue;
+    r[k] = t_slot->arena.take(c[k].bytes);
+    ZS_CUDA(cudaMemcpyAsync(r[k], c[k].src, c[k].bytes, cudaMemcpyDeviceToHost, st));
+  }
+  ZS_CUDA(cudaStreamSynchronize(st));
+  for (size_t k = 0; k < count; ++k)
+    if (c[k].bytes) std::memcpy(c[k].dst, r[k], c[k].bytes);
+}
+
 void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   if (bytes == 0) return;
   Stager* sg = (bytes < kSmall || !t_slot) ? nullptr : &t_slot->stager;

@@ -65,5 +65,12 @@ class PinnedScope {
 void h2d_small(void* dst, const void* src, size_t bytes, cudaStream_t st);
 // Device -> host through a fresh pinned region; synchronizes `st`.
 void d2h_small(void* dst, const void* src, size_t bytes, cudaStream_t st);
+// Several device -> host copies with one wait on `st`.
+struct D2H {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+void d2h_many(const D2H* copies, size_t count, cudaStream_t st);
 
 }  // namespace zs

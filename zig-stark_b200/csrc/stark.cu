@@ -310,6 +310,16 @@ const qm31* offset_powers(unsigned log_n, cudaStream_t st, std::unique_ptr<DevBu
   return cached_table<OffsetPowers>(log_n, [&](cudaStream_t s) { return new OffsetPowers(log_n, s); }).p;
 }
 
+// The roots of trees[a, b), read back with one wait.
+std::vector<Digest> roots_of(const std::vector<std::unique_ptr<OwnedTree>>& trees, uint32_t a, uint32_t b,
+                             cudaStream_t st) {
+  std::vector<Digest> out(b - a);
+  std::vector<D2H> c;
+  for (uint32_t j = a; j < b; ++j) c.push_back({out[j - a].data(), trees[j]->t.root(), 32});
+  d2h_many(c.data(), c.size(), st);
+  return out;
+}
+
 // The DeviceTree pointers of trees[a, b).
 std::vector<DeviceTree*> tree_ptrs(const std::vector<std::unique_ptr<OwnedTree>>& trees, uint32_t a, uint32_t b) {
   std::vector<DeviceTree*> v;
@@ -548,14 +558,13 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   proof.u64(sp.num_queries);
   proof.u8(sp.remainder_log);
   std::vector<Digest> pre_roots, trace_roots, acc_roots;
-  for (uint32_t j = 0; j < n_pre; ++j) {
-    pre_roots.push_back(root_of(trees[j]->t, st));
-    ch.absorb(pre_roots.back());
+  {
+    const std::vector<Digest> roots = roots_of(trees, 0, n_pre + m, st);
+    pre_roots.assign(roots.begin(), roots.begin() + n_pre);
+    trace_roots.assign(roots.begin() + n_pre, roots.end());
   }
-  for (uint32_t j = 0; j < m; ++j) {
-    trace_roots.push_back(root_of(trees[n_pre + j]->t, st));
-    ch.absorb(trace_roots.back());
-  }
+  for (const Digest& d : pre_roots) ch.absorb(d);
+  for (const Digest& d : trace_roots) ch.absorb(d);
 
   // ---- LogUp challenges and accumulators ---------------------------------------
   QuotConsts kc{};
@@ -593,8 +602,9 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
              cw.p + (size_t)(n_pre + m) * N, N, n_rel, small, big, offset_pows, st);
     build_qm31_trees(cw.p + (size_t)(n_pre + m) * N, N, tree_ptrs(trees, n_pre + m, n_pre + m + n_rel).data(), n_rel,
                      st);
+    const std::vector<Digest> aroots = roots_of(trees, n_pre + m, n_pre + m + n_rel, st);
     for (uint32_t r = 0; r < n_rel; ++r) {
-      acc_roots.push_back(root_of(trees[n_pre + m + r]->t, st));
+      acc_roots.push_back(aroots[r]);
       ch.absorb(acc_roots.back());
     }
   }
@@ -717,6 +727,11 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   if (L - tail > kTailLayers) tail = L - kTailLayers;
   if (tail > 0) build_qm31_tree(layers[0]->p, ftrees[0]->t, st);
   std::vector<Digest> froots(L);
+  // remainder (fri.zig:228-233): interpolate the first 2^(remainder_log - log_blowup)
+  // points of layer L on the host (at most a few dozen values); they come back with
+  // the transcript state and the layer roots, in one wait.
+  const uint32_t rem = 1u << (fp.remainder_log - fp.log_blowup);
+  std::vector<qm31> last(rem);
   if (L > 0) {
     DevBuf<Channel> d_ch(1, st);
     h2d_small(d_ch.p, &ch, sizeof(Channel), st);
@@ -745,17 +760,16 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
       h2d_small(d_tail.p, &ft, sizeof(ft), st);
       fri_tail(d_tail.p, d_ch.p, st);
     }
-    d2h_small(&ch, d_ch.p, sizeof(Channel), st);  // the transcript continues on the host
     std::vector<uint32_t> words((size_t)8 * L);
-    d2h_small(words.data(), d_roots.p, words.size() * sizeof(uint32_t), st);
+    const D2H back[3] = {{&ch, d_ch.p, sizeof(Channel)},  // the transcript continues on the host
+                         {words.data(), d_roots.p, words.size() * sizeof(uint32_t)},
+                         {last.data(), layers[L]->p, rem * sizeof(qm31)}};
+    d2h_many(back, 3, st);
     for (unsigned i = 0; i < L; ++i)
       for (int b = 0; b < 32; ++b) froots[i][b] = (uint8_t)(words[8 * i + b / 4] >> (8 * (b % 4)));
+  } else {
+    d2h_small(last.data(), layers[L]->p, rem * sizeof(qm31), st);
   }
-  // remainder (fri.zig:228-233): interpolate the first 2^(remainder_log - log_blowup)
-  // points of layer L on the host (at most a few dozen values).
-  const uint32_t rem = 1u << (fp.remainder_log - fp.log_blowup);
-  std::vector<qm31> last(rem);
-  d2h_small(last.data(), layers[L]->p, rem * sizeof(qm31), st);
   std::vector<qm31> xs(rem);
   {
     const qm31 wl = q_root_of_unity(lN - L);
@@ -913,7 +927,7 @@ std::vector<uint8_t> commit_columns(const uint8_t* cols_b, size_t cols_len, unsi
   for (uint32_t c0 = 0; c0 < C; c0 += per) {
     const uint32_t c = std::min(per, C - c0);
     build_qm31_trees(cw.p + (size_t)c0 * N, N, tree_ptrs(trees, 0, c).data(), c, st);
-    for (uint32_t j = 0; j < c; ++j) out.digest(root_of(trees[j]->t, st));
+    for (const Digest& d : roots_of(trees, 0, c, st)) out.digest(d);
   }
   return out.out;
 }
