@@ -274,31 +274,41 @@ void upload_low_words(uint32_t* dst, const uint8_t* const* cols, uint32_t C, siz
   HostPool& pool = HostPool::get();
   const size_t parts = pool.width();
   const size_t per_chunk = kChunk / 4;  // elements per staging buffer
-  std::vector<uint8_t> part_high(parts);
-  for (uint32_t j = 0; j < C; ++j) {
-    high[j] = 0;
-    for (size_t off = 0; off < n; off += per_chunk) {
-      const size_t len = std::min(per_chunk, n - off);
-      const int b = (int)(sg->next++ & 1);
-      ZS_CUDA(cudaEventSynchronize(sg->ev[b]));
-      uint32_t* pin = static_cast<uint32_t*>(sg->buf[b]);
-      const uint8_t* src = cols[j] + 16 * off;
-      const size_t piece = (len + parts - 1) / parts;
-      pool.run(parts, [&](size_t i) {
-        const size_t a = std::min(len, i * piece), e = std::min(len, a + piece);
+  // Element g of the upload is element g mod n of column g / n, and the columns are
+  // adjacent in `dst`, so a staging buffer is filled across column boundaries: one
+  // pool run and one copy per buffer, however short the columns.
+  const size_t total = (size_t)C * n;
+  std::vector<uint8_t> part_high(parts * C, 0);
+  for (size_t g0 = 0; g0 < total; g0 += per_chunk) {
+    const size_t len = std::min(per_chunk, total - g0);
+    const int b = (int)(sg->next++ & 1);
+    ZS_CUDA(cudaEventSynchronize(sg->ev[b]));
+    uint32_t* pin = static_cast<uint32_t*>(sg->buf[b]);
+    const size_t piece = (len + parts - 1) / parts;
+    pool.run(parts, [&](size_t i) {
+      size_t a = std::min(len, i * piece);
+      const size_t e = std::min(len, a + piece);
+      while (a < e) {
+        const size_t g = g0 + a, j = g / n, off = g % n;
+        const size_t run = std::min(e - a, n - off);
+        const uint8_t* src = cols[j] + 16 * off;
         uint32_t acc = 0;
-        for (size_t k = a; k < e; ++k) {
+        for (size_t k = 0; k < run; ++k) {
           uint32_t w[4];
           std::memcpy(w, src + 16 * k, 16);
-          pin[k] = w[0];
+          pin[a + k] = w[0];
           acc |= w[1] | w[2] | w[3];
         }
-        part_high[i] = acc != 0;
-      });
-      for (size_t i = 0; i < parts; ++i) high[j] |= part_high[i];
-      ZS_CUDA(cudaMemcpyAsync(dst + (size_t)j * n + off, pin, len * 4, cudaMemcpyHostToDevice, st));
-      ZS_CUDA(cudaEventRecord(sg->ev[b], st));
-    }
+        if (acc) part_high[i * C + j] = 1;
+        a += run;
+      }
+    });
+    ZS_CUDA(cudaMemcpyAsync(dst + g0, pin, len * 4, cudaMemcpyHostToDevice, st));
+    ZS_CUDA(cudaEventRecord(sg->ev[b], st));
+  }
+  for (uint32_t j = 0; j < C; ++j) {
+    high[j] = 0;
+    for (size_t i = 0; i < parts; ++i) high[j] |= part_high[i * C + j];
   }
 }
 
