@@ -18,7 +18,9 @@ struct WireWriter {
   std::vector<uint8_t> out;
   void u8(uint8_t v) { out.push_back(v); }
   void u64(uint64_t v) {
-    for (int i = 0; i < 8; ++i) out.push_back((uint8_t)(v >> (8 * i)));
+    uint8_t b[8];
+    for (int i = 0; i < 8; ++i) b[i] = (uint8_t)(v >> (8 * i));
+    bytes(b, 8);
   }
   void bytes(const void* p, size_t n) {
     const uint8_t* b = (const uint8_t*)p;

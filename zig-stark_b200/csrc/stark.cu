@@ -783,9 +783,16 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   for (auto& v : remainder) ch.absorb(v);
 
   // ---- queries (fri.zig:236-256, stark.zig:595-625) -----------------------------
+  // Every revealed value and Merkle sibling is gathered by one kernel, in the order the
+  // proof lists them, so serialization copies contiguous runs of the gathered words.
   std::vector<uint64_t> p0s(sp.num_queries);
   for (auto& p : p0s) p = ch.sample_index(N);
   std::vector<GatherReq> reqs;
+  {
+    size_t fri_levels = 0;
+    for (unsigned i = 0; i < L; ++i) fri_levels += lN - i;
+    reqs.reserve((size_t)sp.num_queries * (2 * L + 2 * fri_levels + (size_t)reveal_len * (1 + lN)));
+  }
   uint32_t off = 0;
   auto want_value = [&](const qm31* base, uint64_t idx) {
     reqs.push_back({reinterpret_cast<const uint32_t*>(base), idx, 4, off});
@@ -797,7 +804,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
       off += 8;
     }
   };
-  // FRI pairs
+  // FRI pairs: per layer the two values, then their two paths
   for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
     uint64_t p = p0s[qi];
     for (unsigned i = 0; i < L; ++i) {
@@ -809,22 +816,18 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
       p = pn;
     }
   }
-  // STARK reveals
+  // STARK reveals: per query the values (columns at p0, columns at p0 + shift, the
+  // quotient, preprocessed columns), then their paths in the same order
   for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
     const uint64_t p0 = p0s[qi], pn = (p0 + shift) % N;
-    for (uint32_t j = 0; j < m_total; ++j) {
-      const qm31* c = cw.p + (size_t)(n_pre + j) * N;
-      want_value(c, p0);
-      want_path(trees[n_pre + j]->t, p0);
-      want_value(c, pn);
-      want_path(trees[n_pre + j]->t, pn);
-    }
+    for (uint32_t j = 0; j < m_total; ++j) want_value(cw.p + (size_t)(n_pre + j) * N, p0);
+    for (uint32_t j = 0; j < m_total; ++j) want_value(cw.p + (size_t)(n_pre + j) * N, pn);
     want_value(q.p, p0);
+    for (uint32_t j = 0; j < n_pre; ++j) want_value(cw.p + (size_t)j * N, p0);
+    for (uint32_t j = 0; j < m_total; ++j) want_path(trees[n_pre + j]->t, p0);
+    for (uint32_t j = 0; j < m_total; ++j) want_path(trees[n_pre + j]->t, pn);
     want_path(qtree.t, p0);
-    for (uint32_t j = 0; j < n_pre; ++j) {
-      want_value(cw.p + (size_t)j * N, p0);
-      want_path(trees[j]->t, p0);
-    }
+    for (uint32_t j = 0; j < n_pre; ++j) want_path(trees[j]->t, p0);
   }
   std::vector<uint32_t> gathered(off);
   if (!reqs.empty()) {
@@ -836,21 +839,19 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     d2h_small(gathered.data(), d_out.p, off * sizeof(uint32_t), st);
   }
   size_t cursor = 0;
-  auto next_value = [&]() {
-    const uint32_t* w4 = gathered.data() + cursor;
-    cursor += 4;
-    return qmake(w4[0], w4[1], w4[2], w4[3]);
+  auto put_values = [&](size_t count) {  // QM31 values: 4 words each, as on the wire
+    proof.bytes(gathered.data() + cursor, 16 * count);
+    cursor += 4 * count;
   };
-  auto next_path = [&](unsigned log_n) {
-    std::vector<Digest> path(log_n);
-    for (auto& d : path) {
-      std::memcpy(d.data(), gathered.data() + cursor, 32);
-      cursor += 8;
-    }
-    return path;
+  auto put_path = [&](unsigned log_n) {  // []Digest: u64 length, 32 bytes per digest
+    proof.u64(log_n);
+    proof.bytes(gathered.data() + cursor, (size_t)32 * log_n);
+    cursor += (size_t)8 * log_n;
   };
 
   // ---- serialization (stark.zig:107-122, fri.zig:72-79) --------------------------
+  proof.out.reserve(proof.out.size() + (size_t)off * 4 + (size_t)sp.num_queries * (L + reveal_len) * 16 +
+                    (size_t)32 * (L + 64) + 1024);
   proof.u8(fp.log_size);  // Fri.Proof.params
   proof.u8(fp.log_blowup);
   proof.u64(fp.num_queries);
@@ -862,34 +863,18 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     proof.u64(p0s[qi]);
     proof.u64(L);
     for (unsigned i = 0; i < L; ++i) {
-      const qm31 v0 = next_value(), v1 = next_value();
-      const auto path0 = next_path(lN - i), path1 = next_path(lN - i);
-      proof.q(v0);
-      proof.q(v1);
-      proof.digests(path0);
-      proof.digests(path1);
+      put_values(2);
+      put_path(lN - i);
+      put_path(lN - i);
     }
   }
   proof.u64(sp.num_queries);
   for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
-    std::vector<qm31> values(reveal_len);
-    std::vector<std::vector<Digest>> paths(reveal_len);
-    for (uint32_t j = 0; j < m_total; ++j) {
-      values[j] = next_value();
-      paths[j] = next_path(lN);
-      values[m_total + j] = next_value();
-      paths[m_total + j] = next_path(lN);
-    }
-    values[2 * m_total] = next_value();
-    paths[2 * m_total] = next_path(lN);
-    for (uint32_t j = 0; j < n_pre; ++j) {
-      values[2 * m_total + 1 + j] = next_value();
-      paths[2 * m_total + 1 + j] = next_path(lN);
-    }
     proof.u64(p0s[qi]);
-    proof.qs(values);
     proof.u64(reveal_len);
-    for (auto& p : paths) proof.digests(p);
+    put_values(reveal_len);
+    proof.u64(reveal_len);
+    for (uint32_t k = 0; k < reveal_len; ++k) put_path(lN);
   }
   ZS_CUDA(cudaStreamSynchronize(st));
   return proof.out;
