@@ -54,3 +54,20 @@ def test_context_without_device_is_a_device_error():
     with pytest.raises(native.ZsError) as e:
         native.Context(0)
     assert e.value.code == -5
+
+
+def test_context_entry_points_check_arguments_first():
+    """zs_m31_prove_ctx rejects a null context with -2 before touching a device,
+    zs_m31_ctx_destroy(NULL) is a no-op and zs_m31_ctx_device(NULL) is -2."""
+    import ctypes
+    from zs_b200 import native
+    L = native._bind_prove()
+    L.zs_m31_prove_ctx.argtypes = [ctypes.c_void_p] + L.zs_m31_prove.argtypes
+    L.zs_m31_ctx_destroy.argtypes = [ctypes.c_void_p]
+    L.zs_m31_ctx_destroy.restype = None
+    L.zs_m31_ctx_device.argtypes = [ctypes.c_void_p]
+    out, n = ctypes.c_void_p(), ctypes.c_size_t()
+    args = [native.HOST, 1] + [b"", 0] * 5
+    assert L.zs_m31_prove_ctx(None, *args, ctypes.byref(out), ctypes.byref(n)) == -2
+    L.zs_m31_ctx_destroy(None)
+    assert L.zs_m31_ctx_device(None) == -2
