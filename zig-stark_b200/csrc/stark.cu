@@ -270,9 +270,16 @@ const T& cached_table(unsigned log_n, Make&& make) {
   if (it != cache->end()) return *it->second;
   cudaStream_t s = nullptr;
   ZS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-  T* t = make(s);
-  ZS_CUDA(cudaStreamSynchronize(s));
-  ZS_CUDA(cudaStreamDestroy(s));
+  T* t = nullptr;
+  try {
+    t = make(s);
+    ZS_CUDA(cudaStreamSynchronize(s));
+  } catch (...) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    throw;
+  }
+  cudaStreamDestroy(s);
   (*cache)[{dev, log_n}] = t;
   return *t;
 }
