@@ -131,7 +131,10 @@ def dist_setup(args, backend="nccl"):
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
+        if backend == "nccl":
+            torch.cuda.set_device(local)  # each rank's NCCL communicator on its own GPU
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
@@ -404,10 +407,14 @@ def run_serve(args, world, rank, local):
 
 def main():
     args = parse()
-    world, rank, local = dist_setup(args)
+    # the reference arm runs on the host cores only: its ranks meet over gloo
+    world, rank, local = dist_setup(args, backend="gloo" if args.impl == "reference" else "nccl")
     if args.impl == "reference":
         run_reference(args, world, rank)
         barrier(world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     if args.workload in ("prove", "batch", "serve"):
         {"prove": run_prove, "batch": run_batch, "serve": run_serve}[args.workload](args, world, rank, local)
