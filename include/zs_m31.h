@@ -250,9 +250,14 @@ int32_t zs_m31_circle_commit(const uint32_t *trace, uint32_t n_columns, uint32_t
  * every other word it needs in one fixed 16 MiB device array inside the library.
  * It allocates nothing. Limit: 2*2^L + 2*2^(L+B) + n_columns*(2^L + 2^(L+B)) words
  * <= 2^22 (L = log_rows, B = log_blowup); larger requests return -2. All calls share
- * the array, so calls whose GPU work overlaps race; the first call on a device looks
- * up the array's address and should come before any stream capture. Asynchronous on
- * `stream` (a cudaStream_t; NULL = default stream). */
+ * the array, so calls whose GPU work overlaps race. The first call on a device looks
+ * up the array's address and, under CUDA's default lazy module loading, is also when
+ * the driver loads this library's device code and backs the array with device memory:
+ * make one small call on each device before reserving an arena of all free memory and
+ * before any stream capture (or run with CUDA_MODULE_LOADING=EAGER); later calls
+ * allocate nothing. The address is kept for the life of the process, so the entry
+ * point must not be used after a cudaDeviceReset. Asynchronous on `stream` (a
+ * cudaStream_t; NULL = default stream). */
 int32_t zs_m31_circle_lde_noalloc(const uint32_t *d_in, uint32_t *d_out, uint32_t n_columns, uint32_t log_rows,
                                   uint32_t log_blowup, void *stream);
 

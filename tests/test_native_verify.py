@@ -120,3 +120,19 @@ def test_verify_batch_matches_single(orc, threads):
     assert got == want
     assert got[:5] == [True] * 5 and got[5] is False and got[6] is False and got[7] == -2 and got[8] is False
     assert native.verify_batch([]) == []
+
+
+def test_rejects_missing_reveals_the_reference_accepts(orc):
+    """The reference verifier (stark.zig:713) checks only the reveals a proof carries,
+    so a proof with its reveal list cut short, or emptied, passes there on FRI alone.
+    The library requires one reveal per FRI query; the oracle (the reference's
+    behaviour) still accepts, which pins that this is a deliberate difference."""
+    params = wire.StarkParams(5, 2, 16, 3)
+    tr, pi = wl.seeded_fib(5)
+    proof = _proof(orc, wl.AIR_SEEDED_FIB, params, pi, tr)
+    for keep in (0, 7, 15):
+        s = wire.StarkProof.decode(proof)
+        s.queries = s.queries[:keep]
+        cut = s.encode()
+        assert not native.verify(wl.AIR_SEEDED_FIB, params, pi, cut, b"v")
+        assert orc.verify(wl.AIR_SEEDED_FIB, params.encode(), pi, cut, b"v")

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/zs_m31.h"
+#include "airs.cuh"
 #include "host.cuh"
 #include "stark.cuh"
 
@@ -32,19 +33,27 @@ namespace zs {
 namespace {
 
 // Device bytes a proof of this shape holds at its peak: codewords, coefficients and
-// values (16 B per element), one Merkle tree per committed column plus the quotient
-// and FRI layers (64 B per leaf), NTT tables and temporaries.
-uint64_t estimate_footprint(const uint8_t* params, size_t params_len, const uint8_t* trace, size_t trace_len,
-                            const uint8_t* pre, size_t pre_len) {
-  if (!params || params_len < 2) return 64u << 20;  // malformed: the job fails on its own status
-  const unsigned tl = params[0], lb = params[1];
+// values (16 B per element) of every committed column -- preprocessed, main and one
+// LogUp accumulator per relation, counted from the AIR itself -- one Merkle tree per
+// committed column plus the quotient and FRI layers (64 B per leaf), NTT tables and
+// temporaries.
+uint64_t estimate_footprint(const zs_m31_job& j) {
+  if (!j.params || j.params_len < 2) return 64u << 20;  // malformed: the job fails on its own status
+  const unsigned tl = j.params[0], lb = j.params[1];
   if (tl + lb > 40) return 64u << 20;
   const uint64_t n = (uint64_t)1 << tl, N = (uint64_t)1 << (tl + lb);
-  uint64_t cols = 0;
-  if (trace_len >= 8) std::memcpy(&cols, trace, 8);
-  uint64_t pcols = 0;
-  if (pre_len >= 8) std::memcpy(&pcols, pre, 8);
-  const uint64_t c = cols + pcols + 1;  // + one accumulator at most for the compiled-in AIRs
+  uint64_t c = 0;
+  try {
+    const AirInfo air = make_air(j.air_id, j.public_inputs, j.public_inputs_len);
+    c = (uint64_t)air.m + air.n_rel + air.n_pre;
+  } catch (...) {
+    // unknown AIR or malformed public inputs: the job fails on its own status; size it
+    // from the column headers of its buffers
+    uint64_t cols = 0, pcols = 0;
+    if (j.trace_len >= 8) std::memcpy(&cols, j.trace, 8);
+    if (j.preprocessed_len >= 8) std::memcpy(&pcols, j.preprocessed, 8);
+    c = std::min<uint64_t>(cols + pcols + 1, 1u << 10);
+  }
   return c * (N * 16 + 2 * n * 16) + (c + 2) * N * 64 + N * 16 * 3 + (64u << 20);
 }
 
@@ -209,8 +218,7 @@ struct Server {
   // Queues a job; `copy` makes the server's own copy of the caller's buffers.
   uint64_t submit(const zs_m31_job& j, bool copy) {
     Job job = copy ? copy_job(j) : view_job(j);
-    job.footprint = estimate_footprint(j.params, j.params_len, j.trace, j.trace_len, j.preprocessed,
-                                       j.preprocessed_len);
+    job.footprint = estimate_footprint(j);
     auto e = std::make_unique<Entry>();
     e->job = std::move(job);
     e->t_submit = std::chrono::steady_clock::now();
@@ -267,8 +275,7 @@ int32_t zs_m31_prove_batch(zs_host_allocator host, size_t n_jobs, const zs_m31_j
     // largest proofs first, so the long ones overlap with the many short ones
     std::vector<uint64_t> fp(n_jobs);
     for (size_t i = 0; i < n_jobs; ++i)
-      fp[i] = estimate_footprint(jobs[i].params, jobs[i].params_len, jobs[i].trace, jobs[i].trace_len,
-                                 jobs[i].preprocessed, jobs[i].preprocessed_len);
+      fp[i] = estimate_footprint(jobs[i]);
     std::vector<size_t> order(n_jobs);
     for (size_t i = 0; i < n_jobs; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return fp[a] > fp[b]; });

@@ -9,7 +9,11 @@
 // array of fixed size, so it never allocates.
 //
 // Costs and limits, stated for users of this entry point:
-//   - every GPU that loads this library holds the array (16 MiB) until the process exits;
+//   - every GPU on which this library's device code is loaded holds the array (16 MiB)
+//     until the process exits. Under CUDA's default lazy module loading that happens
+//     on the first call on the device (the address lookup below), not when the library
+//     is opened, so a caller that later reserves all free device memory makes one small
+//     call first (or sets CUDA_MODULE_LOADING=EAGER);
 //   - a call needs 2*2^L + 2*2^(L+B) + C*(2^L + 2^(L+B)) words of it, at most
 //     kNoallocWords (2^22 words); larger requests are rejected with -2;
 //   - all calls share the array and it keeps the last call's contents, so calls
@@ -18,7 +22,9 @@
 //     at zero: every word a call reads was written earlier in the same call;
 //   - the first call on a device looks up the array's device address (once per
 //     device, with that device current); make that first call before any stream
-//     capture begins.
+//     capture begins. The address is kept for the life of the process: after a
+//     cudaDeviceReset the module is reloaded elsewhere, so the entry point must not be
+//     used across a device reset.
 #include <mutex>
 
 #include "../../include/zs_m31.h"

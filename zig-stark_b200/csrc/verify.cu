@@ -249,8 +249,11 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
   std::vector<qm31> gammas(n_deep);
   for (auto& g : gammas) g = ch.sample_q();
   if (!fri_verify(fp, p, ch)) return false;
-  // stark.zig:713-714: one reveal per FRI query is read; more would index past the end.
-  if (p.reveals.size() > p.fq.size()) return false;
+  // stark.zig:713-714 reads one reveal per FRI query and checks only the reveals the
+  // proof carries, so the reference accepts a proof with fewer reveals than queries
+  // (none at all skips every DEEP and constraint check). This verifier requires exactly
+  // one reveal per FRI query; honest proofs always carry that many.
+  if (p.reveals.size() != p.fq.size()) return false;
   for (size_t qi = 0; qi < p.reveals.size(); ++qi) {
     const Reveal& rv = p.reveals[qi];
     if (rv.index != p.fq[qi].index) return false;
