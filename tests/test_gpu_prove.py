@@ -187,3 +187,52 @@ def test_maximum_size_proof_verifies():
     with pytest.raises(native.ZsError) as e:
         native.prove(wl.AIR_SEEDED_FIB, wire.StarkParams(25, 2, 16, 3), pi, tr, b"", b"max")
     assert e.value.code == -2
+
+
+@pytest.mark.parametrize("air,trace_log", [(wl.AIR_RESCUE_STACKED, 16), (wl.AIR_RESCUE_STACKED, 18),
+                                           (wl.AIR_AND_TABLE, 16), (wl.AIR_SEEDED_FIB, 18)])
+def test_prover_is_deterministic(orc, air, trace_log):
+    """The same job proven three times, on fresh buffers each time and with other
+    proofs in between, gives the same bytes (the quotient kernel reads per-thread
+    column arrays at indices taken from device memory; the host checks every such
+    index before the launch). The first proof is also checked against the oracle."""
+    from zs_b200 import native
+    if air == wl.AIR_AND_TABLE:
+        tr, pre = wl.and_table_trace(1 << trace_log)
+        pi = b""
+        pre_b = wire.columns(list(pre))
+    else:
+        tr, pi = wl.rescue_stacked(trace_log) if air == wl.AIR_RESCUE_STACKED else wl.seeded_fib(trace_log)
+        pre_b = b""
+    params = wire.StarkParams(trace_log, 2 if air != wl.AIR_AND_TABLE else 1, 16, 3)
+    first = native.prove(air, params, pi, tr, pre_b, b"det")
+    other_tr, other_pi = wl.seeded_fib(12)
+    for _ in range(2):
+        native.prove(wl.AIR_SEEDED_FIB, wire.StarkParams(12, 2, 16, 3), other_pi, other_tr, b"", b"other")
+        assert native.prove(air, params, pi, tr, pre_b, b"det") == first
+    if trace_log <= 16:
+        assert first == orc.prove(air, params.encode(), pi, pre_b, wire.columns(tr), b"det", mode=1)
+
+
+@pytest.mark.parametrize("air,trace_log,log_blowup,rem", [(wl.AIR_FIB, 8, 4, 4), (wl.AIR_FIB, 6, 5, 5),
+                                                          (wl.AIR_SEEDED_FIB, 12, 4, 5), (wl.AIR_RESCUE_STACKED, 10, 4, 5),
+                                                          (wl.AIR_RESCUE_STACKED, 8, 6, 7), (wl.AIR_RANGE_CHECK, 8, 5, 6),
+                                                          (wl.AIR_FIB, 2, 12, 12)])
+def test_blowups_above_8(orc, air, trace_log, log_blowup, rem):
+    """StarkParams.log_blowup is any u8 in the reference (stark.zig:75-90): blowups of
+    16 to 4096 prove byte-equal to the oracle and verify."""
+    from zs_b200 import native
+    pre = ()
+    if air == wl.AIR_FIB:
+        tr = wl.fib_trace(1 << trace_log)
+        pi = wl.fib_public(tr)
+    elif air == wl.AIR_SEEDED_FIB:
+        tr, pi = wl.seeded_fib(trace_log)
+    elif air == wl.AIR_RESCUE_STACKED:
+        tr, pi = wl.rescue_stacked(trace_log)
+    else:
+        tr, pre = wl.range_check_trace(1 << trace_log)
+        pi = b""
+    params = wire.StarkParams(trace_log, log_blowup, 16, rem)
+    proof = _check(orc, air, params, pi, tr, pre, sep=b"blowup")
+    assert native.verify(air, params, pi, proof, b"blowup")

@@ -13,7 +13,9 @@
 // Device layout of a domain's twiddles (flat, n - 1 words used): the twiddle of
 // block b at layer i is TW[n - (n >> i) + b]; layer 0 (the circle layer) occupies
 // [0, n/2), layer i >= 1 the 2^(lg-1-i) words after it. The inverse table holds the
-// elementwise M31 inverses. Tables are generated on the device once per domain.
+// elementwise M31 inverses. Both tables store each twiddle doubled (2t < 2^32), the
+// form the butterflies' multiply takes (mmul2). Tables are generated on the device
+// once per domain.
 //
 // Each transform is split into HBM passes over groups held in shared memory: the
 // butterflies of layers [0, K) connect elements inside aligned runs of 2^K
@@ -73,9 +75,16 @@ __global__ void k_tw_small(unsigned lg, cpoint p0, uint32_t* TW) {
   }
 }
 
+// Inverse table, stored doubled like the forward one (see mmul2).
 __global__ void k_invert(const uint32_t* in, uint32_t* out, uint32_t n) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) out[k] = minv(in[k]);
+  if (k < n) out[k] = minv(in[k]) << 1;
+}
+
+// Forward table doubled in place, after k_invert has read it.
+__global__ void k_double(uint32_t* tw, uint32_t n) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) tw[k] <<= 1;
 }
 
 // canonicHalf(lg) (src/m31/circle/coset.zig:59-65): B = generator().neg(),
@@ -111,12 +120,53 @@ void CircleDomain::init(cpoint offset, cpoint step, cudaStream_t st) {
     k_tw_circle_layer<<<(k + 255) / 256, 256, 0, st>>>(lg, tw);
   }
   k_invert<<<(n + 255) / 256, 256, 0, st>>>(tw, itw, n);
+  k_double<<<(n + 255) / 256, 256, 0, st>>>(tw, n);
   ZS_CUDA(cudaGetLastError());
 }
 
 CircleDomain::~CircleDomain() {
   cudaFree(tw);
   cudaFree(itw);
+}
+
+// ---------------------------------------------------------------------------
+// Butterfly arithmetic
+// ---------------------------------------------------------------------------
+
+// The transforms are bound by integer issue. The plain M31 operations (field.cuh) put
+// all their additions, shifts and minima on the ALU pipe, which accepts an instruction
+// every other cycle, while the FMA pipe beside it, which runs integer multiply-adds,
+// idles. These variants move part of each operation to multiply-adds: a + b as
+// a * 1 + b, a - b as b * (2^32 - 1) + a, and the Mersenne fold of a product as a
+// multiply-high. The multipliers come from constant memory so that the compiler
+// keeps the multiply-adds. Results are the canonical values of madd / msub / mmul.
+__constant__ uint32_t c_pipe[3] = {1u, 0xffffffffu, 0x80000000u};
+
+__device__ __forceinline__ uint32_t imad_lo(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+__device__ __forceinline__ uint32_t imad_hi(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t r;
+  asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+// a + b mod p, a, b < p.
+__device__ __forceinline__ uint32_t madd2(uint32_t a, uint32_t b) {
+  return umin32(imad_lo(a, c_pipe[0], b), a + b - P);
+}
+// a - b mod p, a, b < p.
+__device__ __forceinline__ uint32_t msub2(uint32_t a, uint32_t b) {
+  return umin32(imad_lo(b, c_pipe[1], a), a - b + P);
+}
+// a * t mod p for a < p and a twiddle stored doubled, t2 = 2t (every twiddle table
+// of this file holds doubled values). a * t2 = 2at, so its high word is at >> 31 and
+// its low word is 2 (at & p); hi + (lo >> 1) <= 2p - 2 is the Mersenne fold of at.
+__device__ __forceinline__ uint32_t mmul2(uint32_t a, uint32_t t2) {
+  const uint32_t lo = a * t2, hi = __umulhi(a, t2);
+  const uint32_t s = imad_hi(lo, c_pipe[2], hi);
+  return umin32(s, imad_lo(s, c_pipe[0], 0x80000001u));  // s - p
 }
 
 // ---------------------------------------------------------------------------
@@ -163,9 +213,9 @@ __device__ __forceinline__ void chunk(uint32_t* s, uint32_t gstride, unsigned G,
           if (m0 & (1 << l)) continue;
           const int m1 = m0 | (1 << l);
           const uint32_t t = tws[m0 >> (l + 1)];
-          const uint32_t x1 = mmul(v[m1], t), x0 = v[m0];
-          v[m1] = msub(x0, x1);
-          v[m0] = madd(x0, x1);
+          const uint32_t x1 = mmul2(v[m1], t), x0 = v[m0];
+          v[m1] = msub2(x0, x1);
+          v[m0] = madd2(x0, x1);
         }
       }
     } else {
@@ -183,8 +233,8 @@ __device__ __forceinline__ void chunk(uint32_t* s, uint32_t gstride, unsigned G,
           const int m1 = m0 | (1 << l);
           const uint32_t t = tws[m0 >> (l + 1)];
           const uint32_t x0 = v[m0], x1 = v[m1];
-          v[m0] = madd(x0, x1);
-          v[m1] = mmul(msub(x0, x1), t);
+          v[m0] = madd2(x0, x1);
+          v[m1] = mmul2(msub2(x0, x1), t);
         }
       }
     }
@@ -237,13 +287,13 @@ __device__ __forceinline__ void chunk_ct(uint32_t* s, uint32_t gstride, unsigned
         const int m1 = m0 | (1 << l);
         const uint32_t t = tws[m0 >> (l + 1)];
         if (!INV) {
-          const uint32_t x1 = mmul(v[m1], t), x0 = v[m0];
-          v[m1] = msub(x0, x1);
-          v[m0] = madd(x0, x1);
+          const uint32_t x1 = mmul2(v[m1], t), x0 = v[m0];
+          v[m1] = msub2(x0, x1);
+          v[m0] = madd2(x0, x1);
         } else {
           const uint32_t x0 = v[m0], x1 = v[m1];
-          v[m0] = madd(x0, x1);
-          v[m1] = mmul(msub(x0, x1), t);
+          v[m0] = madd2(x0, x1);
+          v[m1] = mmul2(msub2(x0, x1), t);
         }
       }
     }
@@ -590,6 +640,7 @@ void circle_twiddles_into(unsigned lg, uint32_t* tw, uint32_t* itw, cudaStream_t
     k_tw_circle_layer<<<(k + 255) / 256, 256, 0, st>>>(lg, tw);
   }
   k_invert<<<(n + 255) / 256, 256, 0, st>>>(tw, itw, n);
+  k_double<<<(n + 255) / 256, 256, 0, st>>>(tw, n);
   ZS_CUDA(cudaGetLastError());
 }
 

@@ -8,8 +8,8 @@ namespace zs {
 // canonicHalf(lg) plus its conjugate), forward and inverse, resident on the device.
 struct CircleDomain {
   unsigned lg;
-  uint32_t* tw = nullptr;   // flat forward table, n words
-  uint32_t* itw = nullptr;  // elementwise inverses
+  uint32_t* tw = nullptr;   // flat forward table, n words, each twiddle doubled (circle.cu)
+  uint32_t* itw = nullptr;  // elementwise inverses, doubled
   // The canonic domain canonicHalf(lg) ++ conjugate.
   CircleDomain(unsigned lg, cudaStream_t st);
   // The domain half_coset ++ conjugate of the half coset {offset + k * step, k < 2^(lg-1)}.

@@ -5,8 +5,6 @@
 
 namespace zs {
 
-constexpr uint32_t kPerRows = 64;  // 8 rows per permutation x blowup <= 8
-
 // Everything the quotient and DEEP kernels need beyond the codewords.
 struct QuotConsts {
   AirConsts air;
@@ -22,9 +20,11 @@ struct QuotConsts {
   uint32_t n_bpts;         // distinct boundary points, bpts[g], and b_grp[b] = g with bpts[g] = b_pt[b]
   uint32_t b_grp[kMaxBound];
   qm31 bpts[kMaxBound];
-  uint32_t per_mask;                 // stacked Rescue: per_tab[i & per_mask] holds the
-  qm31 per_tab[kPerRows][5];         // periodic values of domain point i (airs.cuh)
-  qm31 zh[8], zh_inv[8];  // Z_H(d_i) depends on i mod 2^log_blowup
+  uint32_t per_mask;  // stacked Rescue: row i & per_mask of the periodic table (a device
+                      // buffer of 8 * 2^log_blowup rows of 5 values, airs.cuh) holds the
+                      // periodic values of domain point i
+  qm31 on;            // FRI_OFFSET^n: Z_H(d_i) = on * w_(2^log_blowup)^(i mod 2^log_blowup) - 1,
+                      // kept in a device table of 2^log_blowup (Z_H, Z_H^-1) pairs
   qm31 ac[kMaxKey], ar[kMaxRel];
   uint32_t sel[kMaxRel], mult[kMaxRel], n_keys[kMaxRel], keys[kMaxRel][kMaxKey], tabs[kMaxRel][kMaxKey];
 };
@@ -46,6 +46,47 @@ __device__ __host__ __forceinline__ qm31 lookup_constraint(const QuotConsts& k, 
   const qm31 lb = qsub(qmul(dacc, qsub(k.ar[r], key)), mult);
   const qm31 tb = qadd(qmul(dacc, qsub(k.ar[r], tkey)), qone());
   return qadd(qmul(sel, lb), qmul(qsub(qone(), sel), tb));
+}
+
+// Columns an AIR's transition constraints read from `current` / `next` (air_eval).
+inline uint32_t air_columns_read(uint32_t id) {
+  switch (id) {
+    case AIR_FIB:
+    case AIR_SEEDED_FIB: return 2;
+    case AIR_RESCUE_EXAMPLE: return 4;
+    case AIR_RESCUE_STACKED: return 12;
+    case AIR_LINEAR_EXAMPLE: return 1;
+    default: return 0;
+  }
+}
+
+// Host-side check, before every launch that reads `k`, that each index the quotient,
+// LogUp and DEEP kernels take from it stays inside the arrays it selects from: the
+// per-thread column arrays (m_total main + accumulator columns, n_pre preprocessed),
+// the boundary groups, the periodic table and the Z_H table (`zh_entries` pairs; 0 for
+// the host-side evaluation, which reads no table). `lookups_only`: the accumulator
+// phase, before the boundaries are filled in. Returns a message naming the first index
+// out of range, or nullptr.
+inline const char* quot_consts_out_of_range(const QuotConsts& k, uint32_t zh_entries, bool lookups_only = false) {
+  if (k.m_total > kMaxCols || k.n_pre > kMaxPre || k.m + k.n_rel != k.m_total) return "column counts";
+  if (k.num_trans > kMaxTrans || k.n_rel > kMaxRel || k.total_bound > kMaxBound) return "constraint counts";
+  if (air_columns_read(k.air.id) > k.m) return "transition columns";
+  for (uint32_t r = 0; r < k.n_rel; ++r) {
+    if (k.sel[r] >= k.m || k.mult[r] >= k.m) return "lookup selector or multiplicity column";
+    if (k.n_keys[r] > kMaxKey) return "lookup key count";
+    for (uint32_t j = 0; j < k.n_keys[r]; ++j)
+      if (k.keys[r][j] >= k.m || k.tabs[r][j] >= k.n_pre) return "lookup key or table column";
+  }
+  if (lookups_only) return nullptr;
+  if (k.n_bpts > k.total_bound) return "boundary groups";
+  for (uint32_t b = 0; b < k.total_bound; ++b) {
+    if (k.b_col[b] >= k.m_total) return "boundary column";
+    if (k.b_grp[b] >= k.n_bpts) return "boundary group";
+  }
+  if (zh_entries == 0) return nullptr;  // host-side evaluation: no tables
+  if (k.air.id == AIR_RESCUE_STACKED && (uint64_t)k.per_mask + 1 != (8ull << k.log_blowup)) return "periodic table";
+  if (((uint64_t)1 << k.log_blowup) != zh_entries) return "vanishing-polynomial table";
+  return nullptr;
 }
 
 // Groups the boundary assertions by their point (host side, after b_pt is filled).

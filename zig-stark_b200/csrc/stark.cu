@@ -48,9 +48,31 @@ __device__ __forceinline__ qm31 domain_point(const QuotConsts& k, const qm31* __
   return qmul(k.offset, w);
 }
 
+// The quotient's per-point tables: zh[2t] = Z_H(d_i), zh[2t + 1] = Z_H(d_i)^-1 for
+// t = i mod 2^log_blowup (stark.zig:520-533 evaluates Z_H at every point; it takes only
+// 2^log_blowup values on D), and for the stacked Rescue AIR the periodic values
+// {y - w8^7, P_0(y), .., P_3(y)} of y = d_r^(n/8), which repeat with period 8 * 2^log_blowup.
+__global__ void k_quot_tables(qm31* __restrict__ zh, qm31* __restrict__ per, const QuotConsts* __restrict__ kp,
+                              qm31 wb, qm31 wN, uint32_t period) {
+  const QuotConsts& k = *kp;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (1u << k.log_blowup)) {
+    const qm31 z = qsub(qmul(k.on, qpow(wb, t)), qone());
+    stq(zh + 2 * (size_t)t, z);
+    stq(zh + 2 * (size_t)t + 1, qinv(z));
+  }
+  if (per && t < period) {
+    const qm31 y = qpow(qmul(k.offset, qpow(wN, t)), k.air.n_div8);
+    qm31* row = per + (size_t)5 * t;
+    stq(row, qsub(y, k.air.w8_7));
+    for (int j = 0; j < 4; ++j) stq(row + 1 + j, horner(k.air.poly[j], 8, y));
+  }
+}
+
 // cw: codewords of all columns ([pre | main | acc]), N each.
 __global__ void __launch_bounds__(kT) k_quotient(const qm31* __restrict__ cw, qm31* __restrict__ q,
-                                                 const qm31* __restrict__ wpow, const QuotConsts* __restrict__ kp) {
+                                                 const qm31* __restrict__ wpow, const QuotConsts* __restrict__ kp,
+                                                 const qm31* __restrict__ zh_tab, const qm31* __restrict__ per_tab) {
   const QuotConsts& k = *kp;
   const uint32_t N = 1u << k.log_N;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -65,9 +87,12 @@ __global__ void __launch_bounds__(kT) k_quotient(const qm31* __restrict__ cw, qm
   }
   const qm31 x = domain_point(k, wpow, i);
   const uint32_t zi = i & ((1u << k.log_blowup) - 1);
-  const qm31* per = k.air.id == AIR_RESCUE_STACKED ? k.per_tab[i & k.per_mask] : nullptr;
-  const qm31 h = composition(k, x, cur, next, pre, k.zh[zi], per, true);
-  stq(q + i, qmul(h, k.zh_inv[zi]));
+  qm31 per[5];
+  const bool stacked = k.air.id == AIR_RESCUE_STACKED;
+  if (stacked)
+    for (int j = 0; j < 5; ++j) per[j] = ldq(per_tab + (size_t)5 * (i & k.per_mask) + j);
+  const qm31 h = composition(k, x, cur, next, pre, ldq(zh_tab + 2 * (size_t)zi), stacked ? per : nullptr, true);
+  stq(q + i, qmul(h, ldq(zh_tab + 2 * (size_t)zi + 1)));
 }
 
 // LogUp row contributions (stark.zig:283-297) on H: out[i] = contribution of row i.
@@ -486,7 +511,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   const WireColumns pre = locate_columns(pre_b, pre_len);
   const WireColumns trace = locate_columns(trace_b, trace_len);
   const unsigned tl = sp.trace_log, lb = sp.log_blowup, lN = tl + lb;
-  if (lN > 26 || lb > 3) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 26 or log_blowup above 3");
+  if (lN > 26) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 26");
   const uint32_t n = 1u << tl, N = 1u << lN, shift = 1u << lb;
   if (air.fixed_n && n != air.fixed_n) throw Error(ZS_EMALFORMED, "the AIR is defined for a fixed trace length");
   if (air.id == AIR_RESCUE_STACKED && n < 8) throw Error(ZS_EMALFORMED, "stacked rescue needs at least 8 rows");
@@ -588,6 +613,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     for (uint32_t j = 0; j < air.n_keys[r]; ++j) kc.keys[r][j] = air.keys[r][j], kc.tabs[r][j] = air.tabs[r][j];
   }
   DevBuf<QuotConsts> d_kc(1, st);
+  if (const char* bad = quot_consts_out_of_range(kc, shift, true)) throw Error(ZS_EGENERIC, bad);
   h2d_small(d_kc.p, &kc, sizeof(kc), st);
   if (n_rel > 0) {
     DevBuf<qm31> contrib(n, st);
@@ -641,33 +667,21 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     kc.b_pt[b] = qpow(w, bnd[b].step);
   }
   group_boundaries(kc);
-  if (air.id == AIR_RESCUE_STACKED) {
-    // y_i = d_i^(n/8) = offset^(n/8) (w_N^(n/8))^i repeats with period 8 * 2^lb
-    const uint32_t period = 8u << lb;
-    if (period > kPerRows) throw Error(ZS_EGENERIC, "blowup too large for the periodic table");
-    kc.per_mask = period - 1;
-    const qm31 wN = q_root_of_unity(lN);
-    qm31 wr = qone();
-    for (uint32_t r = 0; r < period; ++r) {
-      const qm31 y = qpow(qmul(offset, wr), n / 8);
-      kc.per_tab[r][0] = qsub(y, kc.air.w8_7);
-      for (int j = 0; j < 4; ++j) kc.per_tab[r][1 + j] = horner(kc.air.poly[j], 8, y);
-      wr = qmul(wr, wN);
-    }
-  }
-  {
-    // Z_H(d_i) = offset^n * (w_N^n)^(i mod 2^lb) - 1
-    const qm31 on = qpow(offset, n), wb = q_root_of_unity(lb);
-    qm31 acc = on;
-    for (uint32_t t = 0; t < shift; ++t) {
-      kc.zh[t] = qsub(acc, qone());
-      kc.zh_inv[t] = qinv(kc.zh[t]);
-      acc = qmul(acc, wb);
-    }
-  }
+  // Z_H(d_i) = offset^n * (w_N^n)^(i mod 2^lb) - 1, and the stacked Rescue AIR's
+  // y_i = d_i^(n/8) = offset^(n/8) (w_N^(n/8))^i, which repeats with period 8 * 2^lb
+  const uint32_t period = air.id == AIR_RESCUE_STACKED ? 8u << lb : 0;
+  kc.per_mask = period ? period - 1 : 0;
+  kc.on = qpow(offset, n);
+  if (const char* bad = quot_consts_out_of_range(kc, shift)) throw Error(ZS_EGENERIC, bad);
   h2d_small(d_kc.p, &kc, sizeof(kc), st);
+  DevBuf<qm31> zh_tab((size_t)2 * shift, st), per_tab(period ? (size_t)5 * period : 1, st);
+  {
+    const uint32_t cnt = std::max<uint32_t>(shift, period);
+    k_quot_tables<<<(cnt + kT - 1) / kT, kT, 0, st>>>(zh_tab.p, period ? per_tab.p : nullptr, d_kc.p,
+                                                      q_root_of_unity(lb), q_root_of_unity(lN), period);
+  }
   DevBuf<qm31> q(N, st);
-  k_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_kc.p);
+  k_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_kc.p, zh_tab.p, per_tab.p);
   ZS_CUDA(cudaGetLastError());
   OwnedTree qtree(lN, st);
   build_qm31_tree(q.p, qtree.t, st);

@@ -188,7 +188,7 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
   const AirInfo air = make_air(air_id, pi, pi_len);
   const Proof p = parse(proof_b, proof_len);
   const unsigned tl = sp.trace_log, lb = sp.log_blowup, lN = tl + lb;
-  if (lN > 30 || lb > 3) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 30 or log_blowup above 3");
+  if (lN > 30) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 30");
   const uint64_t n = (uint64_t)1 << tl, N = (uint64_t)1 << lN, shift = (uint64_t)1 << lb;
   const uint32_t m = air.m, n_pre = air.n_pre, n_rel = air.n_rel, m_total = m + n_rel;
   const uint32_t n_deep = 2 * m_total + 1, reveal_len = 2 * m_total + 1 + n_pre;
@@ -243,6 +243,7 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
     kc.b_pt[b] = qpow(w, bnd[b].step);
   }
   group_boundaries(kc);
+  if (const char* bad = quot_consts_out_of_range(kc, 0)) throw Error(ZS_EGENERIC, bad);
   ch.absorb(p.qroot);
   const qm31 z = ch.sample_q();
   for (auto& v : p.deep) ch.absorb(v);
