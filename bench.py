@@ -38,6 +38,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--log-rows", type=int, default=LOG_ROWS, help="smaller cases for profiling")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-proofs", action="store_true",
+                    help="skip the proof workloads and the reference-kernel bar after the commit step")
     ap.add_argument("--workload", default="commit", choices=["commit", "prove", "batch", "serve"],
                     help="commit: the circle commit step (default); prove: single proofs (Fibonacci 2^12, "
                          "stacked Rescue 2^18); batch: mixed-size proof batch, batched vs one at a time; "
@@ -211,8 +213,7 @@ def _proof_jobs(shapes, cache_variants=None):
         key = (air, lg, i % cache_variants) if cache_variants else i
         if key not in cache:
             cache[key] = wl.proof_job(air, lg, seed, sep)
-        air_, params, pi, trace, _ = cache[key]
-        jobs.append((air_, params, pi, trace, sep))
+        jobs.append(cache[key]._replace(sep=sep))
     return jobs
 
 
@@ -223,8 +224,8 @@ def _cpu_prove_sample(jobs, max_log, count):
     import oracle
     pick = [j for j in jobs if j[1][0] <= max_log][:count]
     t0 = time.perf_counter()
-    for air, params, pi, trace, sep in pick:
-        oracle.prove(air, params, pi, b"", trace, sep, mode=1)
+    for air, params, pi, trace, sep, pre in pick:
+        oracle.prove(air, params, pi, pre, trace, sep, mode=1)
     dt = time.perf_counter() - t0
     return {"value": len(pick) / dt, "unit": "proofs/s", "cores": os.cpu_count() or 1, "kind": "port",
             "sample": f"{len(pick)} jobs of the stream with <= 2^{max_log} rows, oracle NTT prover, {dt:.2f} s"}
@@ -233,27 +234,30 @@ def _cpu_prove_sample(jobs, max_log, count):
 def run_prove(args, world, rank, local):
     """Single proofs through zs_m31_prove from host buffers, one at a time: the
     2^12-row Fibonacci AIR (a_1 seeded, blowup 4, 16 queries, separator
-    "zig-stark:fibonacci:example") and stacked Rescue at 2^18 rows (blowup 4)."""
+    "zig-stark:fibonacci:example"), stacked Rescue at 2^18 rows and the linear layer
+    (W 128 x 128, 2^14 input vectors, 2^15 rows), all at blowup 4."""
     import torch
     from zs_b200 import native, wire
     from zs_b200 import workload as wl
     torch.cuda.set_device(local)
     fib_tr, fib_pi = wl.seeded_fib(12)
-    fib = (wl.AIR_SEEDED_FIB, wire.StarkParams(12, 2, 16, 3).encode(), fib_pi, wire.columns(fib_tr),
-           b"zig-stark:fibonacci:example")
+    fib = wl.ProofJob(wl.AIR_SEEDED_FIB, wire.StarkParams(12, 2, 16, 3).encode(), fib_pi, wire.columns(fib_tr),
+                      b"zig-stark:fibonacci:example", b"")
     cases = {"seeded_fib_2^12": fib,
-             "rescue_stacked_2^18": wl.proof_job(wl.AIR_RESCUE_STACKED, 18, wl.SEED_RESCUE, b"zig-stark:rescue:stacked")}
+             "rescue_stacked_2^18": wl.proof_job(wl.AIR_RESCUE_STACKED, 18, wl.SEED_RESCUE, b"zig-stark:rescue:stacked"),
+             "ml_linear_2^14_vectors": wl.proof_job(wl.AIR_ML_LINEAR, 15, wl.SEED_ML_LINEAR,
+                                                    b"zig-stark:ml_linear:layer")}
     out = {}
     with ClockSampler(local) as clocks:
-        for name, (air, params, pi, trace, sep) in cases.items():
+        for name, (air, params, pi, trace, sep, pre) in cases.items():
             proof = None
             for _ in range(args.warmup):
-                proof = native.prove(air, params, pi, trace, b"", sep)
+                proof = native.prove(air, params, pi, trace, pre, sep)
             barrier(world)
             ts = []
             for _ in range(args.steps):
                 t0 = time.perf_counter()
-                p = native.prove(air, params, pi, trace, b"", sep)
+                p = native.prove(air, params, pi, trace, pre, sep)
                 ts.append(time.perf_counter() - t0)
             assert p == proof, "proof changed between runs"
             ms = max_over_ranks(sorted(ts)[len(ts) // 2], world) * 1e3
@@ -265,8 +269,9 @@ def run_prove(args, world, rank, local):
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": out["rescue_stacked_2^18"]["ms_per_proof_median"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 (M31 / QM31 exact)", "data": "synthetic (seeded)",
-        "config": {"workload": "stacked Rescue 2^18 rows (value); SeededFib 2^12 rows also timed; blowup 4, "
-                               "16 queries", "parallelism": f"replicas x{world}"},
+        "config": {"workload": "stacked Rescue 2^18 rows (value); SeededFib 2^12 rows and the linear layer "
+                               "(W 128 x 128, 2^14 input vectors) also timed; blowup 4, 16 queries",
+                   "parallelism": f"replicas x{world}"},
         "cases": out,
         "e2e": {"value": out["rescue_stacked_2^18"]["proofs_per_s"], "unit": "proofs/s",
                 "h2d_bytes_per_step": out["rescue_stacked_2^18"]["trace_bytes"],
@@ -276,7 +281,7 @@ def run_prove(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
-        air, params, pi, trace, sep = fib
+        air, params, pi, trace, sep, _ = fib
         t0 = time.perf_counter()
         want = oracle.prove(air, params, pi, b"", trace, sep, mode=1)
         dt = time.perf_counter() - t0
@@ -299,7 +304,8 @@ def run_batch(args, world, rank, local):
     lo, hi = args.log_min or 10, args.log_max or 20
     shapes = wl.batch_shapes(args.jobs, log_min=lo, log_max=hi)[rank::world]
     jobs = _proof_jobs(shapes)
-    kw = [dict(air_id=a, params=p, public_inputs=pi, trace=t, channel_sep=sp) for a, p, pi, t, sp in jobs]
+    kw = [dict(air_id=a, params=p, public_inputs=pi, trace=t, preprocessed=pre, channel_sep=sp)
+          for a, p, pi, t, sp, pre in jobs]
     h2d = sum(len(j[3]) + len(j[1]) + len(j[2]) for j in jobs)
 
     def batched():
@@ -357,8 +363,9 @@ def run_batch(args, world, rank, local):
 
 def run_serve(args, world, rank, local):
     """Poisson arrivals at --rate per second for --duration seconds; each request a
-    Fibonacci or stacked Rescue proof (50/50) with log2 rows from a geometric
-    distribution (p = 0.5) truncated to 12..22. Served with continuous batching
+    Fibonacci, stacked Rescue or linear-layer proof (50/30/20) with log2 rows from a
+    geometric distribution (p = 0.5) truncated to 12..22 (the linear layer capped at
+    2^15 rows). Served with continuous batching
     (--concurrency workers) and, on the same arrivals, one request at a time."""
     import torch
     from zs_b200 import serving
@@ -388,7 +395,8 @@ def run_serve(args, world, rank, local):
         "dtype": "u32 (M31 / QM31 exact)", "data": "synthetic (SplitMix64 seeded; traces repeat over 2 seeds "
                                                    "per shape, every request has its own channel separator)",
         "config": {"workload": f"Poisson {args.rate:g} req/s for {args.duration:g} s per GPU, SeededFib / "
-                               f"stacked Rescue 50/50, log2 rows geometric(0.5) truncated to {lo}..{hi}, "
+                               f"stacked Rescue / linear layer 50/30/20, log2 rows geometric(0.5) truncated "
+                               f"to {lo}..{hi} (linear layer at most 2^15), "
                                "blowup 4, 16 queries", "requests": n_total, "concurrency": args.concurrency,
                    "parallelism": f"replicas x{world}"},
         "latency_ms": {"p50": serving.percentile(lat, 50), "p99": serving.percentile(lat, 99),
@@ -403,6 +411,129 @@ def run_serve(args, world, rank, local):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def proof_metrics(args, local, budget_s=90.0):
+    """The proof configurations, bounded for the default run (about a minute), on one
+    GPU: single-proof latency of the 2^12-row SeededFib proof (bytes checked against
+    the oracle), of the 2^18-row stacked Rescue proof and of the linear layer (W 128 x
+    128, 2^14 input vectors); the 512-trace mixed batch (SeededFib / stacked Rescue
+    50/50, log2 rows 10..20), batched against one at a time; and the served stream
+    (SeededFib / stacked Rescue / linear layer 50/30/20, log2 rows geometric over
+    12..22) at three arrival rates, with p50/p99 latency, against one request at a time
+    at the middle rate. Traces repeat per (AIR, size) over two seeds; every job has its
+    own channel separator, so every proof differs."""
+    import torch
+    from zs_b200 import native, serving, wire
+    from zs_b200 import workload as wl
+    t_start = time.perf_counter()
+    out = {}
+    fib_tr, fib_pi = wl.seeded_fib(12)
+    singles = {"seeded_fib_2^12": wl.ProofJob(wl.AIR_SEEDED_FIB, wire.StarkParams(12, 2, 16, 3).encode(), fib_pi,
+                                              wire.columns(fib_tr), b"zig-stark:fibonacci:example", b""),
+               "rescue_stacked_2^18": wl.proof_job(wl.AIR_RESCUE_STACKED, 18, wl.SEED_RESCUE,
+                                                   b"zig-stark:rescue:stacked"),
+               "ml_linear_2^14_vectors": wl.proof_job(wl.AIR_ML_LINEAR, 15, wl.SEED_ML_LINEAR,
+                                                      b"zig-stark:ml_linear:layer")}
+    for name, (air, params, pi, trace, sep, pre) in singles.items():
+        proof = native.prove(air, params, pi, trace, pre, sep)
+        for _ in range(3):
+            native.prove(air, params, pi, trace, pre, sep)
+        ts = []
+        for _ in range(15):
+            t0 = time.perf_counter()
+            p = native.prove(air, params, pi, trace, pre, sep)
+            ts.append(time.perf_counter() - t0)
+        assert p == proof, "proof changed between runs"
+        out[name] = {"ms_median": sorted(ts)[len(ts) // 2] * 1e3, "ms_min": min(ts) * 1e3,
+                     "proof_bytes": len(proof), "trace_bytes": len(trace) + len(pre)}
+        if name.startswith("seeded_fib"):
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            out[name]["bytes_equal_oracle"] = proof == oracle.prove(air, params, pi, pre, trace, sep, mode=1)
+    # 512 mixed-size traces, batched vs one at a time
+    jobs = _proof_jobs(wl.batch_shapes(512), cache_variants=2)
+    kw = [dict(air_id=a, params=p, public_inputs=pi, trace=t, preprocessed=pre, channel_sep=sp)
+          for a, p, pi, t, sp, pre in jobs]
+    ref = native.prove_batch(kw, concurrency=8)
+    assert all(isinstance(p, bytes) for p in ref), "a batch job failed"
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    got = native.prove_batch(kw, concurrency=8)
+    t_b = time.perf_counter() - t0
+    assert got == ref, "batched proofs changed between runs"
+    t0 = time.perf_counter()
+    got_p = [native.prove(**k) for k in kw]
+    t_p = time.perf_counter() - t0
+    assert got_p == ref, "one-at-a-time proofs differ from the batched ones"
+    out["batch_512"] = {"batched_proofs_per_s": len(kw) / t_b, "plain_proofs_per_s": len(kw) / t_p,
+                        "batched_over_plain": t_p / t_b, "batched_s": t_b, "plain_s": t_p,
+                        "workload": "512 traces, SeededFib / stacked Rescue 50/50, log2 rows uniform 10..20, "
+                                    "blowup 4, 16 queries, concurrency 8"}
+    # served stream at three rates, and one at a time at the middle rate
+    serve = {}
+    for rate in (100.0, 400.0, 1200.0):
+        if time.perf_counter() - t_start > budget_s:
+            serve[f"{rate:g}"] = {"skipped": "time budget of the default run"}
+            continue
+        arrivals = serving.poisson_arrivals(rate, 4.0, wl.SEED_SERVE)
+        sjobs = _proof_jobs(wl.serve_shapes(len(arrivals)), cache_variants=2)
+        if rate == 100.0:  # warm the pool with the largest shapes
+            warm = sorted(set((j[0], j[1][0]) for j in sjobs), key=lambda x: -x[1])[:4]
+            wjobs = [next(j for j in sjobs if (j[0], j[1][0]) == w) for w in warm]
+            serving.replay(wjobs * 2, [0.0] * (2 * len(wjobs)), 8)
+        r = serving.replay(sjobs, arrivals, 8)
+        lat = r["latency_ms"]
+        row = {"requests": len(sjobs), "proofs_per_s": len(sjobs) / r["wall_s"],
+               "p50_ms": serving.percentile(lat, 50), "p99_ms": serving.percentile(lat, 99), "failed": r["failed"]}
+        if rate == 400.0:
+            rp = serving.replay(sjobs, arrivals, 1)
+            row["plain"] = {"proofs_per_s": len(sjobs) / rp["wall_s"],
+                            "p50_ms": serving.percentile(rp["latency_ms"], 50),
+                            "p99_ms": serving.percentile(rp["latency_ms"], 99)}
+        serve[f"{rate:g}"] = row
+    out["serve"] = {"workload": "Poisson arrivals for 4 s per rate, SeededFib / stacked Rescue / linear layer "
+                                "50/30/20, log2 rows geometric(0.5) truncated to 12..22 (linear layer capped at "
+                                "2^15 rows), blowup 4, 16 queries, 8 workers",
+                    "rates": serve}
+    out["wall_s"] = time.perf_counter() - t_start
+    return out
+
+
+def reference_gpu_bar(n_cols=64):
+    """The reference's own GPU circle FFT (its kernels built from its source for sm_100a,
+    driven as src/cuda/circlefft_gpu.zig does: one launch per layer), timed on this
+    GPU for the commit workload's transforms: the circleIFFT of 2^20 points and the
+    circleFFT of 2^22 points per column. Device time of its launches per column (host
+    twiddles by the coset walk, which gives the same values faster), scaled to the 64
+    columns, and one whole reference call at 2^16 points with its per-call host twiddles."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref not built (the reference tree was absent at build time)"}
+    from zs_b200 import workload as wl
+    x20 = wl.uniform_m31(0x5EED00F0, 1 << 20)
+    x22 = wl.uniform_m31(0x5EED00F1, 1 << 22)
+    ref_gpu.set_fast_twiddles(True)
+    for _ in range(2):
+        ref_gpu.ifft(x20)
+        ref_gpu.fft(x22)
+    dev_i, dev_f = [], []
+    for _ in range(3):
+        dev_i.append(ref_gpu.ifft(x20)[2])
+        dev_f.append(ref_gpu.fft(x22)[2])
+    ref_gpu.set_fast_twiddles(False)
+    x16 = wl.uniform_m31(0x5EED00F2, 1 << 16)
+    ref_gpu.fft(x16)
+    _, wall16, dev16 = ref_gpu.fft(x16)
+    ref_gpu.set_fast_twiddles(True)
+    di, df = min(dev_i), min(dev_f)
+    return {"ifft_2^20_device_ms_per_column": di, "fft_2^22_device_ms_per_column": df,
+            "lde_device_ms_64_columns": n_cols * (di + df),
+            "fft_2^16_call_ms": wall16, "fft_2^16_call_device_ms": dev16,
+            "note": "reference kernels src/cuda/kernels/circlefft.cu compiled for sm_100a, one launch per layer; "
+                    "device ms are CUDA events around its launches; the call at 2^16 includes its host "
+                    "twiddles, allocations and copies"}
 
 
 def main():
@@ -531,7 +662,9 @@ def main():
     int_peak = n_sm * 128 * sm_mhz * 1e6 / 1e12
     lg_n, lg_N = log_rows, log_rows + LOG_BLOWUP
     ops = {
-        "lde": 13 * N_COLS * (lg_n * (n >> 1) + lg_N * (N >> 1)),
+        # inverse: lg_n layers of n/2; forward: the top B layers of the 2^(lg_n+B) transform
+        # only copy (the padded half is zero), so lg_n layers of N/2
+        "lde": 13 * N_COLS * (lg_n * (n >> 1) + lg_n * (N >> 1)),
         "row_tree": 700 * (N * ((N_COLS * 4 + 63) // 64) + 2 * (N - 1)) + 36 * N * N_COLS,
         "folds": sum(700 * ((N >> i) + 2 * ((N >> i) - 1)) + 60 * (N >> (i + 1)) for i in range(N_FOLDS)),
     }
@@ -563,9 +696,15 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and log_rows == LOG_ROWS:
         line["cpu_baseline"] = cpu_baseline_sample(os.cpu_count() or 1)
+    plan.close()
+    if world == 1 and log_rows == LOG_ROWS and not args.no_proofs:
+        try:
+            line["reference_gpu_circle_fft"] = reference_gpu_bar()
+        except Exception as e:  # the bar is reported, never required
+            line["reference_gpu_circle_fft"] = {"unavailable": f"{type(e).__name__}: {e}"}
+        line["proofs"] = proof_metrics(args, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    plan.close()
     barrier(world)
     if world > 1:
         import torch.distributed as dist

@@ -12,6 +12,9 @@
 //   LinearAir (n=8)   examples/ml_linear/src/main.zig:21-116
 // AIRs for workloads the reference has no AIR for, written in the same shape:
 //   SeededFibAir      FibAir with public a_0, a_1 (boundaries from public inputs)
+//   RescueStackedAir  independent Rescue permutations stacked 8 rows each
+//   MlLinearAir       y = W x for a batch of input vectors bound by LogUp to a
+//                     preprocessed input table (examples/ml_linear widened)
 #pragma once
 #include <memory>
 #include <stdexcept>
@@ -38,6 +41,7 @@ enum AirId : uint32_t {
   AIR_RESCUE_EXAMPLE = 5,
   AIR_LINEAR_EXAMPLE = 6,
   AIR_RESCUE_STACKED = 7,
+  AIR_ML_LINEAR = 8,
 };
 
 struct Air {
@@ -279,6 +283,63 @@ struct RescueStackedAir : Air {
   }
 };
 
+// One linear layer y = W x over M31 (examples/ml_linear/src/main.zig:21-116 proves one
+// dot product of public weights with public inputs; this is the same kind of statement
+// for a 128 x 128 weight matrix and a batch of input vectors that stay private and
+// are bound to a committed input table instead).
+// Columns: x_0..x_127 (0..127), y_0..y_127 (128..255), sel (256), mult (257).
+// Preprocessed: P_0..P_127, the input table (one input vector per table row).
+// Rows with sel = 1 hold an input vector x and its output y = W x; rows with sel = 0
+// are table rows (x = y = 0 there, P = a table vector).
+//   C_k = y_k - sum_l W[k][l] x_l, k < 128 (every row; degree 1)
+//   one LogUp relation: key (x_0..x_127) on rows with sel = 1, multiplicity `mult`,
+//   against table key (P_0..P_127) on rows with sel = 0: every input vector is a row
+//   of the committed input table (combined with 128 per-column challenges).
+//   boundary: sel = 0 on the last row (the one row the transitions leave unchecked,
+//   stark.zig:505-533 multiplies them by x - w^(n-1), must not carry an input).
+// PublicInputs {w: []QM31, 128 x 128 row-major, each an M31 value}.
+struct MlLinearAir : Air {
+  static constexpr size_t D = 128;
+  std::vector<M31> W;  // row-major D x D
+  explicit MlLinearAir(const std::vector<QM31>& w) {
+    if (w.size() != D * D) throw WireError("ml linear AIR takes a 128 x 128 weight matrix", -2);
+    W.resize(D * D);
+    for (size_t k = 0; k < D * D; ++k) {
+      if (w[k].a.c1.v != 0 || w[k].b.c0.v != 0 || w[k].b.c1.v != 0)
+        throw WireError("ml linear weights are M31 values", -2);
+      W[k] = w[k].a.c0;
+    }
+    num_columns = 2 * D + 2;
+    num_transitions = D;
+    num_boundary = 1;
+    num_preprocessed = D;
+    num_lookup_columns = D;
+    num_lookup_relations = 1;
+    selector_cols = {2 * D};
+    mult_cols = {2 * D + 1};
+    std::vector<size_t> cols(D);
+    for (size_t l = 0; l < D; ++l) cols[l] = l;
+    key_cols = {cols};
+    table_cols = {cols};
+  }
+  // v * w for an M31 weight w: each M31 component scaled (QM31.mul by fromM31(w)).
+  static QM31 scale(const QM31& v, M31 w) {
+    return QM31(CM31(v.a.c0.mul(w), v.a.c1.mul(w)), CM31(v.b.c0.mul(w), v.b.c1.mul(w)));
+  }
+  void evalTransition(const QM31&, const QM31* cur, const QM31*, QM31* out) const override {
+    for (size_t k = 0; k < D; ++k) {
+      QM31 acc = QM31::zero();
+      for (size_t l = 0; l < D; ++l) acc = acc.add(scale(cur[l], W[k * D + l]));
+      out[k] = cur[D + k].sub(acc);
+    }
+  }
+  size_t maxConstraintDegree(size_t n) const override { return n - 1; }
+  void boundaryAssertions(size_t n, BoundaryAssertion* out) const override { out[0] = {2 * D, n - 1, QM31::zero()}; }
+  void checkTraceLen(size_t n) const override {
+    if (n < 2) throw WireError("ml linear AIR needs at least 2 rows", -2);
+  }
+};
+
 // Builds the AIR for `air_id` from the wire encoding of its PublicInputs.
 inline std::unique_ptr<Air> makeAir(uint32_t air_id, const uint8_t* pi, size_t pi_len) {
   Reader r(pi, pi_len);
@@ -321,6 +382,11 @@ inline std::unique_ptr<Air> makeAir(uint32_t air_id, const uint8_t* pi, size_t p
       for (auto& v : init) v = r.qm31();
       for (auto& v : fin) v = r.qm31();
       air = std::make_unique<RescueStackedAir>(init, fin);
+      break;
+    }
+    case AIR_ML_LINEAR: {
+      std::vector<QM31> w = r.qm31s();
+      air = std::make_unique<MlLinearAir>(w);
       break;
     }
     default:

@@ -168,20 +168,30 @@ struct Stark {
 
     std::vector<std::vector<QM31>> coeffs(m_total), codewords(m_total);
     std::vector<std::vector<QM31>> pre_coeffs(n_pre), pre_cw(n_pre);
-    for (size_t j = 0; j < m; ++j) lde(trace[j], params, h_points, d_points, mode, coeffs[j], codewords[j]);
-    for (size_t j = 0; j < n_pre; ++j) lde(pre[j], params, h_points, d_points, mode, pre_coeffs[j], pre_cw[j]);
+    // columns are independent until their roots are absorbed: LDE and tree per column in
+    // parallel, then the roots in the reference's order
+    std::vector<MerkleTree> pre_trees(n_pre), trace_trees(m), acc_trees(n_rel);
+#pragma omp parallel for schedule(dynamic)
+    for (long jj = 0; jj < (long)(m + n_pre); ++jj) {
+      const size_t j = (size_t)jj;
+      if (j < m) {
+        lde(trace[j], params, h_points, d_points, mode, coeffs[j], codewords[j]);
+        trace_trees[j].init(hashCodeword(codewords[j]));
+      } else {
+        const size_t k = j - m;
+        lde(pre[k], params, h_points, d_points, mode, pre_coeffs[k], pre_cw[k]);
+        pre_trees[k].init(hashCodeword(pre_cw[k]));
+      }
+    }
 
     StarkProof proof;
     proof.params = params;
-    std::vector<MerkleTree> pre_trees(n_pre), trace_trees(m), acc_trees(n_rel);
     if (n_pre > 0) proof.preprocessed_roots = std::vector<Digest>();
     for (size_t j = 0; j < n_pre; ++j) {
-      pre_trees[j].init(hashCodeword(pre_cw[j]));
       proof.preprocessed_roots->push_back(pre_trees[j].root());
       ch.absorbDigest(pre_trees[j].root());
     }
     for (size_t j = 0; j < m; ++j) {
-      trace_trees[j].init(hashCodeword(codewords[j]));
       proof.trace_roots.push_back(trace_trees[j].root());
       ch.absorbDigest(trace_trees[j].root());
     }

@@ -14,7 +14,8 @@ def _mixed_jobs():
     jobs = []
     for i, (air, lg) in enumerate([(wl.AIR_SEEDED_FIB, 10), (wl.AIR_RESCUE_STACKED, 6), (wl.AIR_SEEDED_FIB, 4),
                                    (wl.AIR_RESCUE_STACKED, 11), (wl.AIR_SEEDED_FIB, 13), (wl.AIR_RESCUE_STACKED, 3),
-                                   (wl.AIR_SEEDED_FIB, 7), (wl.AIR_RESCUE_STACKED, 9)]):
+                                   (wl.AIR_SEEDED_FIB, 7), (wl.AIR_RESCUE_STACKED, 9), (wl.AIR_ML_LINEAR, 5),
+                                   (wl.AIR_ML_LINEAR, 8)]):
         jobs.append(wl.proof_job(air, lg, 1000 + i, b"zig-stark:test:" + bytes([i])))
     tr, table = wl.range_check_trace(64)
     jobs.append((wl.AIR_RANGE_CHECK, wire.StarkParams(6, 2, 16, 3).encode(), b"", wire.columns(tr),
@@ -44,9 +45,9 @@ def test_batch_matches_alone(orc, concurrency):
         assert isinstance(g, bytes)
         assert g == _alone(j)
     # two of them against the oracle as well
-    for j, g in [(jobs[0], got[0]), (jobs[1], got[1])]:
-        air, params, pi, trace, sep = j
-        assert g == orc.prove(air, params, pi, b"", trace, sep, mode=1)
+    for j, g in [(jobs[0], got[0]), (jobs[1], got[1]), (jobs[8], got[8])]:
+        air, params, pi, trace, sep, pre = j
+        assert g == orc.prove(air, params, pi, pre, trace, sep, mode=1)
         assert orc.verify(air, params, pi, g, sep)
 
 

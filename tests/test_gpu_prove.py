@@ -236,3 +236,41 @@ def test_blowups_above_8(orc, air, trace_log, log_blowup, rem):
     params = wire.StarkParams(trace_log, log_blowup, 16, rem)
     proof = _check(orc, air, params, pi, tr, pre, sep=b"blowup")
     assert native.verify(air, params, pi, proof, b"blowup")
+
+
+@pytest.mark.parametrize("trace_log", [1, 5, 8, 12])
+def test_ml_linear(orc, trace_log):
+    """The linear layer y = W x (W 128 x 128, inputs bound to the preprocessed input
+    table by LogUp) at growing batch sizes, against the oracle."""
+    from zs_b200 import native
+    tr, pre, pi = wl.ml_linear(trace_log)
+    params = wire.StarkParams(trace_log, 2, 16, 3)
+    proof = _check(orc, wl.AIR_ML_LINEAR, params, pi, tr, pre, sep=b"zig-stark:ml_linear:layer")
+    assert native.verify(wl.AIR_ML_LINEAR, params, pi, proof, b"zig-stark:ml_linear:layer")
+
+
+def test_ml_linear_full_size(orc):
+    """The full layer: W 128 x 128 with entries in [0, 2^16), 2^14 input vectors with
+    entries in [0, 2^16) (2^15 rows: the vectors and the input table), blowup 4;
+    byte-equal to the oracle, accepted by the oracle and the library verifiers."""
+    from zs_b200 import native
+    tr, pre, pi = wl.ml_linear(15)
+    params = wire.StarkParams(15, 2, 16, 3)
+    proof = _check(orc, wl.AIR_ML_LINEAR, params, pi, tr, pre, sep=b"zig-stark:ml_linear:layer")
+    assert native.verify(wl.AIR_ML_LINEAR, params, pi, proof, b"zig-stark:ml_linear:layer")
+
+
+def test_ml_linear_false_statements_fail(orc):
+    """A wrong output, or an input vector missing from the input table, still proves
+    (the prover does not check the statement) but the proof is rejected, with the same
+    bytes as the oracle's."""
+    from zs_b200 import native
+    tr, pre, pi = wl.ml_linear(6)
+    params = wire.StarkParams(6, 2, 16, 3)
+    bad_y = [c.copy() for c in tr]
+    bad_y[wl.ML_DIM + 3][2, 0] = (int(bad_y[wl.ML_DIM + 3][2, 0]) + 1) % wl.P
+    bad_x = [c.copy() for c in pre]
+    bad_x[7][-1, 0] = (int(bad_x[7][-1, 0]) + 1) % wl.P  # the table no longer holds the last input vector
+    for t, p_ in ((bad_y, pre), (tr, bad_x)):
+        proof = _check(orc, wl.AIR_ML_LINEAR, params, pi, t, p_, sep=b"ml", valid=False)
+        assert not native.verify(wl.AIR_ML_LINEAR, params, pi, proof, b"ml")

@@ -136,3 +136,19 @@ def test_rejects_missing_reveals_the_reference_accepts(orc):
         cut = s.encode()
         assert not native.verify(wl.AIR_SEEDED_FIB, params, pi, cut, b"v")
         assert orc.verify(wl.AIR_SEEDED_FIB, params.encode(), pi, cut, b"v")
+
+
+@pytest.mark.parametrize("trace_log", [2, 6])
+def test_ml_linear(orc, trace_log):
+    """The library verifier's linear-layer composition (ml_composition) accepts the
+    oracle's proofs and rejects a changed quotient root or public weight."""
+    tr, pre, pi = wl.ml_linear(trace_log)
+    params = wire.StarkParams(trace_log, 2, 16, 3)
+    proof = _proof(orc, wl.AIR_ML_LINEAR, params, pi, tr, pre)
+    assert native.verify(wl.AIR_ML_LINEAR, params, pi, proof, b"v")
+    s = wire.StarkProof.decode(proof)
+    s.quotient_root = bytes(32)
+    assert not native.verify(wl.AIR_ML_LINEAR, params, pi, s.encode(), b"v")
+    bad = bytearray(pi)
+    bad[8] ^= 1  # W[0][0]
+    assert not native.verify(wl.AIR_ML_LINEAR, params, bytes(bad), proof, b"v")

@@ -271,3 +271,35 @@ def test_rescue_stacked_first_permutation_matches_example():
     ex, _ = wl.rescue_example(init)
     for j in range(4):
         assert np.array_equal(tr[j][:8], ex[j])
+
+
+def test_ml_linear_oracle_roundtrip_and_tamper(orc):
+    """The linear-layer AIR in the oracle: an honest batch verifies; an output that is
+    not W x, and an input vector that is not in the preprocessed input table, do not."""
+    import numpy as np
+    from zs_b200 import wire
+    from zs_b200 import workload as wl
+    lg = 5
+    tr, pre, pi = wl.ml_linear(lg)
+    params = wire.StarkParams(lg, 2, 16, 3).encode()
+    good = orc.prove(wl.AIR_ML_LINEAR, params, pi, wire.columns(pre), wire.columns(tr), b"ml", mode=1)
+    assert orc.verify(wl.AIR_ML_LINEAR, params, pi, good, b"ml")
+    bad = [c.copy() for c in tr]
+    bad[wl.ML_DIM][0, 0] = (int(bad[wl.ML_DIM][0, 0]) + 1) % wl.P
+    proof = orc.prove(wl.AIR_ML_LINEAR, params, pi, wire.columns(pre), wire.columns(bad), b"ml", mode=1)
+    assert not orc.verify(wl.AIR_ML_LINEAR, params, pi, proof, b"ml")
+    # an input vector changed together with its outputs (consistent y = W x) but absent
+    # from the input table
+    W = wl.uniform_below(wl.SEED_ML_LINEAR, wl.ML_DIM ** 2, 1 << 16).reshape(wl.ML_DIM, wl.ML_DIM)
+    bad = [c.copy() for c in tr]
+    bad[0][1, 0] = (int(bad[0][1, 0]) + 1) % wl.P
+    x = np.array([int(bad[l][1, 0]) for l in range(wl.ML_DIM)], dtype=np.uint64)
+    y = (W.astype(np.uint64) @ x) % wl.P
+    for k in range(wl.ML_DIM):
+        bad[wl.ML_DIM + k][1, 0] = int(y[k])
+    proof = orc.prove(wl.AIR_ML_LINEAR, params, pi, wire.columns(pre), wire.columns(bad), b"ml", mode=1)
+    assert not orc.verify(wl.AIR_ML_LINEAR, params, pi, proof, b"ml")
+    # the last row must be a table row
+    bad_w = bytearray(pi)
+    bad_w[8 + 4] = 1  # an entry with a non-zero second component: not an M31 weight
+    assert not orc.verify(wl.AIR_ML_LINEAR, params, bytes(bad_w), good, b"ml")

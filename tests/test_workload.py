@@ -85,3 +85,30 @@ def test_percentile():
     assert serving.percentile(v, 50) == pytest.approx(50.5)
     assert serving.percentile(v, 99) == pytest.approx(99.01)
     assert serving.percentile([3.0], 99) == 3.0
+
+
+def test_ml_linear_workload():
+    """The linear-layer trace: W and inputs in [0, 2^16), y = W x mod p on the input
+    rows, the input table on the other rows, the last row a table row."""
+    tr, pre, pi = wl.ml_linear(6)
+    D, n = wl.ML_DIM, 64
+    X = np.stack([tr[l][:, 0] for l in range(D)], axis=1)
+    Y = np.stack([tr[D + k][:, 0] for k in range(D)], axis=1)
+    Pm = np.stack([pre[l][:, 0] for l in range(D)], axis=1)
+    sel = tr[2 * D][:, 0]
+    W = wl.uniform_below(wl.SEED_ML_LINEAR, D * D, 1 << 16).reshape(D, D)
+    assert W.max() < (1 << 16) and X.max() < (1 << 16)
+    assert (sel[: n // 2] == 1).all() and (sel[n // 2:] == 0).all() and sel[-1] == 0
+    assert np.array_equal(Y, (X.astype(np.uint64) @ W.T.astype(np.uint64)) % wl.P)
+    assert np.array_equal(Pm[n // 2:], X[: n // 2]) and not Pm[: n // 2].any() and not X[n // 2:].any()
+    assert len(pi) == 8 + 16 * D * D
+    for c in tr + pre:
+        assert c.shape == (n, 4) and not c[:, 1:].any()
+
+
+def test_serve_mix_includes_the_linear_layer():
+    shapes = wl.serve_shapes(4000)
+    airs = np.array([s[0] for s in shapes])
+    assert 0.25 < np.mean(airs == wl.AIR_RESCUE_STACKED) < 0.35
+    assert 0.15 < np.mean(airs == wl.AIR_ML_LINEAR) < 0.25
+    assert max(s[1] for s in shapes if s[0] == wl.AIR_ML_LINEAR) <= wl.ML_LINEAR_MAX_LOG

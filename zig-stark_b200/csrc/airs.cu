@@ -53,6 +53,9 @@ void AirInfo::boundary(uint64_t n, std::vector<Boundary>& out) const {
       out.push_back({0, 0, qmul_m(x_inputs[0], 1)});
       out.push_back({0, n - 1, pi[0]});
       break;
+    case AIR_ML_LINEAR:  // the last row, which the transitions leave unchecked, is a table row
+      out.push_back({kMlSel, n - 1, qzero()});
+      break;
     default:
       break;
   }
@@ -125,6 +128,19 @@ AirInfo make_air(uint32_t air_id, const uint8_t* pi_bytes, size_t pi_len) {
       const std::vector<qm31> c = interpolate_small(h, ys);
       a.consts.poly_len = 8;
       for (int k = 0; k < 8; ++k) a.consts.poly[0][k] = c[k];
+      break;
+    }
+    case AIR_ML_LINEAR: {
+      a.m = kMlCols, a.n_pre = kMlDim, a.n_lc = kMlDim, a.n_rel = 1, a.num_trans = kMlDim, a.num_bound = 1;
+      a.sel[0] = kMlSel, a.mult[0] = kMlMult;  // keys x_l and table columns P_l, l < kMlDim (implicit)
+      const uint64_t nw = r.len(16);
+      if (nw != (uint64_t)kMlDim * kMlDim) throw Error(ZS_EMALFORMED, "linear layer AIR takes a 128 x 128 matrix");
+      a.w.resize(nw);
+      for (uint64_t k = 0; k < nw; ++k) {
+        const qm31 v = r.q();
+        if (v.a.b || v.b.a || v.b.b) throw Error(ZS_EMALFORMED, "linear layer weights are M31 values");
+        a.w[k] = v.a.a;
+      }
       break;
     }
     default:

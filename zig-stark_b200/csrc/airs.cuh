@@ -23,15 +23,25 @@ enum AirIdInternal : uint32_t {
   AIR_RESCUE_EXAMPLE = 5,
   AIR_LINEAR_EXAMPLE = 6,
   AIR_RESCUE_STACKED = 7,
-  AIR_COUNT = 8,
+  AIR_ML_LINEAR = 8,
+  AIR_COUNT = 9,
 };
 
+// Limits of the generic quotient path, which keeps a row's columns in per-thread
+// arrays. The linear-layer AIR (AIR_ML_LINEAR) is wider and has kernels of its own
+// that stream its columns (constraints.cuh, stark.cu).
 constexpr unsigned kMaxCols = 16;      // main + accumulator columns
 constexpr unsigned kMaxTrans = 16;     // AIR transition constraints
 constexpr unsigned kMaxBound = 16;     // boundary assertions incl. synthesized ones
 constexpr unsigned kMaxPre = 4;
 constexpr unsigned kMaxRel = 2;
 constexpr unsigned kMaxKey = 4;
+
+// The linear-layer AIR: y = W x with W 128 x 128 (public input), input vectors bound
+// by one LogUp relation to a preprocessed input table. Columns x_0..x_127, y_0..y_127,
+// sel, mult; preprocessed P_0..P_127.
+constexpr uint32_t kMlDim = 128;
+constexpr uint32_t kMlSel = 2 * kMlDim, kMlMult = 2 * kMlDim + 1, kMlCols = 2 * kMlDim + 2;
 
 // Constants an AIR's evalTransition needs (row-dependent polynomials of the examples).
 struct AirConsts {
@@ -133,6 +143,7 @@ struct AirInfo {
   bool dc_plus_n8 = false;
   std::vector<qm31> pi;  // public inputs (QM31 fields in declaration order)
   std::vector<qm31> x_inputs;  // linear example: public x
+  std::vector<uint32_t> w;     // linear layer: W, row-major kMlDim x kMlDim M31 values
   AirConsts consts{};
 
   uint64_t max_constraint_degree(uint64_t n) const {  // stark.zig:217-221 incl. LogUp padding

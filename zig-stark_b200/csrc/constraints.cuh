@@ -48,6 +48,76 @@ __device__ __host__ __forceinline__ qm31 lookup_constraint(const QuotConsts& k, 
   return qadd(qmul(sel, lb), qmul(qsub(qone(), sel), tb));
 }
 
+// Composition constants of the linear-layer AIR (AIR_ML_LINEAR, airs.cuh), whose 259
+// committed columns are streamed by its own kernels instead of held per thread.
+// Hc(x) (stark.zig:505-533) for this AIR is
+//   (x - w^(n-1)) sum_k alpha_k (y_k - sum_l W[k][l] x_l)
+//     + alpha_look L(x) + alpha_bin sel (1 - sel)
+//     + Z_H(x) (beta_sel sel / (x - w^(n-1)) + beta_acc acc / (x - 1)),
+// L the denominator-cleared LogUp constraint (stark.zig:259-276) of the key
+// sum_l ac_l x_l against the table key sum_l ac_l P_l. The transition sum is taken as
+// sum_k alpha_k y_k - sum_l beta_l x_l with beta_l = sum_k alpha_k W[k][l]: equal in the
+// ring, and 2 * 128 products per point instead of 128 * 129.
+struct MlConsts {
+  qm31 ac[kMlDim];       // LogUp column challenges
+  qm31 alpha_y[kMlDim];  // transition weights alpha_k
+  qm31 beta_x[kMlDim];   // sum_k alpha_k W[k][l]
+  qm31 ar, alpha_look, alpha_bin, beta_sel, beta_acc;
+  qm31 last_point;  // w^(n-1), also the point of the sel boundary
+  qm31 offset;      // FRI_OFFSET
+  uint32_t log_N, log_blowup, shift;
+};
+
+// The composition at x from the row's values: cur/next index the m_total = kMlCols + 1
+// main and accumulator columns, pre the kMlDim preprocessed ones. `units`: x - w^(n-1)
+// and x - 1 are units (always on the evaluation domain), so both inverses come from one.
+__device__ __host__ inline qm31 ml_composition(const MlConsts& k, const qm31& x, const qm31* cur, const qm31* next,
+                                               const qm31* pre, const qm31& zh, bool units) {
+  qm31 ty = qzero(), tx = qzero(), key = qzero(), tkey = qzero();
+  for (uint32_t l = 0; l < kMlDim; ++l) {
+    ty = qadd(ty, qmul(k.alpha_y[l], cur[kMlDim + l]));
+    tx = qadd(tx, qmul(k.beta_x[l], cur[l]));
+    key = qadd(key, qmul(k.ac[l], cur[l]));
+    tkey = qadd(tkey, qmul(k.ac[l], pre[l]));
+  }
+  const qm31 sel = cur[kMlSel], mult = cur[kMlMult], acc = cur[kMlCols], accn = next[kMlCols];
+  qm31 h = qmul(qsub(ty, tx), qsub(x, k.last_point));
+  const qm31 dacc = qsub(accn, acc);
+  const qm31 lb = qsub(qmul(dacc, qsub(k.ar, key)), mult);
+  const qm31 tb = qadd(qmul(dacc, qsub(k.ar, tkey)), qone());
+  h = qadd(h, qmul(k.alpha_look, qadd(qmul(sel, lb), qmul(qsub(qone(), sel), tb))));
+  h = qadd(h, qmul(k.alpha_bin, qmul(sel, qsub(qone(), sel))));
+  const qm31 d_sel = qsub(x, k.last_point), d_acc = qsub(x, qone());
+  qm31 i_sel, i_acc;
+  if (units) {
+    const qm31 inv = qinv(qmul(d_sel, d_acc));
+    i_sel = qmul(inv, d_acc);
+    i_acc = qmul(inv, d_sel);
+  } else {
+    i_sel = qinv(d_sel);
+    i_acc = qinv(d_acc);
+  }
+  const qm31 b = qadd(qmul(k.beta_sel, qmul(sel, i_sel)), qmul(k.beta_acc, qmul(acc, i_acc)));
+  return qadd(h, qmul(b, zh));
+}
+
+// Fills the linear-layer AIR's weights from the sampled transition weights (128
+// transitions, then the LogUp and selector-binarity constraints) and boundary weights
+// (sel at w^(n-1), then acc at 1): beta_l = sum_k alpha_k W[k][l].
+inline void ml_set_weights(MlConsts& k, const AirInfo& air, const std::vector<qm31>& alphas,
+                           const std::vector<qm31>& betas) {
+  for (uint32_t l = 0; l < kMlDim; ++l) {
+    k.alpha_y[l] = alphas[l];
+    k.beta_x[l] = qzero();
+  }
+  for (uint32_t r = 0; r < kMlDim; ++r)
+    for (uint32_t l = 0; l < kMlDim; ++l) k.beta_x[l] = qadd(k.beta_x[l], qmul_m(alphas[r], air.w[(size_t)r * kMlDim + l]));
+  k.alpha_look = alphas[kMlDim];
+  k.alpha_bin = alphas[kMlDim + 1];
+  k.beta_sel = betas[0];
+  k.beta_acc = betas[1];
+}
+
 // Columns an AIR's transition constraints read from `current` / `next` (air_eval).
 inline uint32_t air_columns_read(uint32_t id) {
   switch (id) {

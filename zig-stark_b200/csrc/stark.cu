@@ -112,6 +112,63 @@ __global__ void k_logup_rows(const qm31* __restrict__ vals, uint32_t n, const Qu
   stq(out + i, qsub(lt, tt));
 }
 
+// The linear-layer AIR's LogUp row contributions (stark.zig:283-297) on H, its key and
+// table columns streamed from the column-major values [P_0..P_127 | x, y, sel, mult].
+__global__ void __launch_bounds__(kT) k_ml_logup_rows(const qm31* __restrict__ vals, uint32_t n,
+                                                      const MlConsts* __restrict__ kp, qm31* __restrict__ out) {
+  const MlConsts& k = *kp;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const qm31* main = vals + (size_t)kMlDim * n;
+  qm31 key = qzero(), tkey = qzero();
+  for (uint32_t l = 0; l < kMlDim; ++l) {
+    key = qadd(key, qmul(k.ac[l], ldq(main + (size_t)l * n + i)));
+    tkey = qadd(tkey, qmul(k.ac[l], ldq(vals + (size_t)l * n + i)));
+  }
+  const qm31 sel = ldq(main + (size_t)kMlSel * n + i), mult = ldq(main + (size_t)kMlMult * n + i);
+  const qm31 lt = qmul(sel, qmul(mult, qinv(qsub(k.ar, key))));
+  const qm31 tt = qmul(qsub(qone(), sel), qinv(qsub(k.ar, tkey)));
+  stq(out + i, qsub(lt, tt));
+}
+
+// The linear-layer AIR's quotient Hc(d_i) / Z_H(d_i) on D: ml_composition
+// (constraints.cuh) with the row's 387 values streamed from the codewords
+// [P_0..P_127 | x, y, sel, mult | acc] instead of held per thread.
+__global__ void __launch_bounds__(kT) k_ml_quotient(const qm31* __restrict__ cw, qm31* __restrict__ q,
+                                                    const qm31* __restrict__ wpow, const MlConsts* __restrict__ kp,
+                                                    const qm31* __restrict__ zh_tab) {
+  const MlConsts& k = *kp;
+  const uint32_t N = 1u << k.log_N;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t half = N >> 1;
+  const qm31 x = qmul(k.offset, i < half ? ldq(wpow + i) : qneg(ldq(wpow + (i - half))));
+  const qm31* main = cw + (size_t)kMlDim * N;
+  qm31 ty = qzero(), tx = qzero(), key = qzero(), tkey = qzero();
+  for (uint32_t l = 0; l < kMlDim; ++l) {
+    const qm31 xl = ldq(main + (size_t)l * N + i);
+    ty = qadd(ty, qmul(k.alpha_y[l], ldq(main + (size_t)(kMlDim + l) * N + i)));
+    tx = qadd(tx, qmul(k.beta_x[l], xl));
+    key = qadd(key, qmul(k.ac[l], xl));
+    tkey = qadd(tkey, qmul(k.ac[l], ldq(cw + (size_t)l * N + i)));
+  }
+  const uint32_t in = (i + k.shift) & (N - 1);
+  const qm31 sel = ldq(main + (size_t)kMlSel * N + i), mult = ldq(main + (size_t)kMlMult * N + i);
+  const qm31 acc = ldq(main + (size_t)kMlCols * N + i), accn = ldq(main + (size_t)kMlCols * N + in);
+  qm31 h = qmul(qsub(ty, tx), qsub(x, k.last_point));
+  const qm31 dacc = qsub(accn, acc);
+  const qm31 lb = qsub(qmul(dacc, qsub(k.ar, key)), mult);
+  const qm31 tb = qadd(qmul(dacc, qsub(k.ar, tkey)), qone());
+  h = qadd(h, qmul(k.alpha_look, qadd(qmul(sel, lb), qmul(qsub(qone(), sel), tb))));
+  h = qadd(h, qmul(k.alpha_bin, qmul(sel, qsub(qone(), sel))));
+  const qm31 d_sel = qsub(x, k.last_point), d_acc = qsub(x, qone());
+  const qm31 inv = qinv(qmul(d_sel, d_acc));
+  const qm31 b = qadd(qmul(k.beta_sel, qmul(sel, qmul(inv, d_acc))), qmul(k.beta_acc, qmul(acc, qmul(inv, d_sel))));
+  const uint32_t zi = i & ((1u << k.log_blowup) - 1);
+  h = qadd(h, qmul(b, ldq(zh_tab + 2 * (size_t)zi)));
+  stq(q + i, qmul(h, ldq(zh_tab + 2 * (size_t)zi + 1)));
+}
+
 // Exclusive prefix sum of QM31 values in blocks of 1024 (exact, so any association
 // order gives the reference's acc[i] = sum_{k<i} c_k).
 __global__ void __launch_bounds__(1024) k_scan_block(const qm31* in, qm31* out, uint32_t n, qm31* block_sums) {
@@ -178,18 +235,19 @@ __global__ void __launch_bounds__(kT) k_eval_sum(const qm31* partial, uint32_t n
 }
 
 // DEEP codeword (stark.zig:577-588), with 1/(d_i - z) factored out of the sum.
+// ge: the 2 m_total + 1 weights gamma_j, then the 2 m_total evaluations f_j(z), f_j(wz).
 struct DeepConsts {
   uint32_t m_total, n_pre, shift;
   unsigned log_N;
   qm31 offset, z, qz;
-  qm31 gammas[2 * kMaxCols + 1];
-  qm31 evals[2 * kMaxCols];
 };
 
 __global__ void __launch_bounds__(kT) k_deep(const qm31* __restrict__ cw, const qm31* __restrict__ q,
                                              const qm31* __restrict__ wpow, const DeepConsts* __restrict__ kp,
-                                             qm31* __restrict__ g) {
+                                             const qm31* __restrict__ ge, qm31* __restrict__ g) {
   const DeepConsts& k = *kp;
+  const qm31* gammas = ge;
+  const qm31* evals = ge + 2 * k.m_total + 1;
   const uint32_t N = 1u << k.log_N;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
@@ -201,10 +259,10 @@ __global__ void __launch_bounds__(kT) k_deep(const qm31* __restrict__ cw, const 
   qm31 acc = qzero();
   for (uint32_t j = 0; j < k.m_total; ++j) {
     const qm31* c = cw + (size_t)(k.n_pre + j) * N;
-    acc = qadd(acc, qmul(k.gammas[j], qsub(ldq(c + i), k.evals[j])));
-    acc = qadd(acc, qmul(k.gammas[k.m_total + j], qsub(ldq(c + in), k.evals[k.m_total + j])));
+    acc = qadd(acc, qmul(ldq(gammas + j), qsub(ldq(c + i), ldq(evals + j))));
+    acc = qadd(acc, qmul(ldq(gammas + k.m_total + j), qsub(ldq(c + in), ldq(evals + k.m_total + j))));
   }
-  acc = qadd(acc, qmul(k.gammas[2 * k.m_total], qsub(ldq(q + i), k.qz)));
+  acc = qadd(acc, qmul(ldq(gammas + 2 * k.m_total), qsub(ldq(q + i), k.qz)));
   stq(g + i, qmul(acc, inv_dz));
 }
 
@@ -526,7 +584,8 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   const uint32_t m = air.m, n_pre = air.n_pre, n_rel = air.n_rel, m_total = m + n_rel;
   const uint32_t n_trans_total = air.num_trans + 2 * n_rel, total_bound = air.num_bound + n_rel;
   const uint32_t n_deep = 2 * m_total + 1, reveal_len = 2 * m_total + 1 + n_pre;
-  if (m_total > kMaxCols || air.num_trans > kMaxTrans || total_bound > kMaxBound || n_pre > kMaxPre)
+  const bool wide = air.id == AIR_ML_LINEAR;  // streamed by its own kernels
+  if (!wide && (m_total > kMaxCols || air.num_trans > kMaxTrans || total_bound > kMaxBound || n_pre > kMaxPre))
     throw Error(ZS_EGENERIC, "AIR exceeds the compiled-in limits");
   // FRI parameters (stark.zig:197-239)
   FriParamsH fp;
@@ -606,22 +665,40 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   kc.total_bound = total_bound, kc.shift = shift, kc.log_N = lN, kc.log_blowup = lb;
   kc.offset = offset;
   kc.last_point = qpow(w, n - 1);
-  for (uint32_t j = 0; j < air.n_lc; ++j) kc.ac[j] = ch.sample_q();
-  for (uint32_t r = 0; r < n_rel; ++r) kc.ar[r] = ch.sample_q();
-  for (uint32_t r = 0; r < n_rel; ++r) {
-    kc.sel[r] = air.sel[r], kc.mult[r] = air.mult[r], kc.n_keys[r] = air.n_keys[r];
-    for (uint32_t j = 0; j < air.n_keys[r]; ++j) kc.keys[r][j] = air.keys[r][j], kc.tabs[r][j] = air.tabs[r][j];
-  }
+  std::vector<qm31> ac(air.n_lc), ar(n_rel);
+  for (auto& a : ac) a = ch.sample_q();
+  for (auto& a : ar) a = ch.sample_q();
   DevBuf<QuotConsts> d_kc(1, st);
-  if (const char* bad = quot_consts_out_of_range(kc, shift, true)) throw Error(ZS_EGENERIC, bad);
-  h2d_small(d_kc.p, &kc, sizeof(kc), st);
+  std::unique_ptr<MlConsts> ml;
+  std::unique_ptr<DevBuf<MlConsts>> d_ml;
+  if (wide) {
+    ml = std::make_unique<MlConsts>();
+    for (uint32_t l = 0; l < kMlDim; ++l) ml->ac[l] = ac[l];
+    ml->ar = ar[0];
+    ml->last_point = kc.last_point, ml->offset = offset;
+    ml->log_N = lN, ml->log_blowup = lb, ml->shift = shift;
+    d_ml = std::make_unique<DevBuf<MlConsts>>(1, st);
+    h2d_small(d_ml->p, ml.get(), sizeof(MlConsts), st);
+  } else {
+    for (uint32_t j = 0; j < air.n_lc; ++j) kc.ac[j] = ac[j];
+    for (uint32_t r = 0; r < n_rel; ++r) kc.ar[r] = ar[r];
+    for (uint32_t r = 0; r < n_rel; ++r) {
+      kc.sel[r] = air.sel[r], kc.mult[r] = air.mult[r], kc.n_keys[r] = air.n_keys[r];
+      for (uint32_t j = 0; j < air.n_keys[r]; ++j) kc.keys[r][j] = air.keys[r][j], kc.tabs[r][j] = air.tabs[r][j];
+    }
+    if (const char* bad = quot_consts_out_of_range(kc, shift, true)) throw Error(ZS_EGENERIC, bad);
+    h2d_small(d_kc.p, &kc, sizeof(kc), st);
+  }
   if (n_rel > 0) {
     DevBuf<qm31> contrib(n, st);
     const uint32_t nb = (n + 1023) / 1024;
     DevBuf<qm31> sums(nb, st), sums_scan(nb, st);
     for (uint32_t r = 0; r < n_rel; ++r) {
       qm31* acc_vals = vals.p + (size_t)(n_pre + m + r) * n;
-      k_logup_rows<<<(n + kT - 1) / kT, kT, 0, st>>>(vals.p, n, d_kc.p, r, contrib.p);
+      if (wide)
+        k_ml_logup_rows<<<(n + kT - 1) / kT, kT, 0, st>>>(vals.p, n, d_ml->p, contrib.p);
+      else
+        k_logup_rows<<<(n + kT - 1) / kT, kT, 0, st>>>(vals.p, n, d_kc.p, r, contrib.p);
       // acc[i] = sum_{k < i} contrib[k] (stark.zig:438-446)
       k_scan_block<<<nb, 1024, 0, st>>>(contrib.p, acc_vals, n, sums.p);
       if (nb > 1) {
@@ -656,23 +733,32 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   }
 
   // ---- constraint weights and the quotient -------------------------------------
-  for (uint32_t t = 0; t < n_trans_total; ++t) kc.alphas[t] = ch.sample_q();
+  std::vector<qm31> alphas(n_trans_total);
+  for (auto& a : alphas) a = ch.sample_q();
   std::vector<Boundary> bnd;
   air.boundary(n, bnd);
   for (uint32_t r = 0; r < n_rel; ++r) bnd.push_back({m + r, 0, qzero()});
-  for (uint32_t b = 0; b < total_bound; ++b) {
-    kc.betas[b] = ch.sample_q();
-    kc.b_col[b] = bnd[b].column;
-    kc.b_val[b] = bnd[b].value;
-    kc.b_pt[b] = qpow(w, bnd[b].step);
+  std::vector<qm31> betas(total_bound);
+  for (auto& b : betas) b = ch.sample_q();
+  if (wide) {
+    ml_set_weights(*ml, air, alphas, betas);
+  } else {
+    for (uint32_t t = 0; t < n_trans_total; ++t) kc.alphas[t] = alphas[t];
+    for (uint32_t b = 0; b < total_bound; ++b) {
+      kc.betas[b] = betas[b];
+      kc.b_col[b] = bnd[b].column;
+      kc.b_val[b] = bnd[b].value;
+      kc.b_pt[b] = qpow(w, bnd[b].step);
+    }
+    group_boundaries(kc);
   }
-  group_boundaries(kc);
   // Z_H(d_i) = offset^n * (w_N^n)^(i mod 2^lb) - 1, and the stacked Rescue AIR's
   // y_i = d_i^(n/8) = offset^(n/8) (w_N^(n/8))^i, which repeats with period 8 * 2^lb
   const uint32_t period = air.id == AIR_RESCUE_STACKED ? 8u << lb : 0;
   kc.per_mask = period ? period - 1 : 0;
   kc.on = qpow(offset, n);
-  if (const char* bad = quot_consts_out_of_range(kc, shift)) throw Error(ZS_EGENERIC, bad);
+  if (!wide)
+    if (const char* bad = quot_consts_out_of_range(kc, shift)) throw Error(ZS_EGENERIC, bad);
   h2d_small(d_kc.p, &kc, sizeof(kc), st);
   DevBuf<qm31> zh_tab((size_t)2 * shift, st), per_tab(period ? (size_t)5 * period : 1, st);
   {
@@ -681,7 +767,12 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
                                                       q_root_of_unity(lb), q_root_of_unity(lN), period);
   }
   DevBuf<qm31> q(N, st);
-  k_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_kc.p, zh_tab.p, per_tab.p);
+  if (wide) {
+    h2d_small(d_ml->p, ml.get(), sizeof(MlConsts), st);
+    k_ml_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_ml->p, zh_tab.p);
+  } else {
+    k_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_kc.p, zh_tab.p, per_tab.p);
+  }
   ZS_CUDA(cudaGetLastError());
   OwnedTree qtree(lN, st);
   build_qm31_tree(q.p, qtree.t, st);
@@ -712,7 +803,8 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     for (uint32_t j = 0; j < n_pre; ++j) pre_z[j] = hs[j];
     // computeQuotientAt (stark.zig:794-849)
     const qm31 zh = qsub(qpow(z, n), qone());
-    const qm31 h = composition(kc, z, deep.data(), deep.data() + m_total, pre_z.data(), zh);
+    const qm31 h = wide ? ml_composition(*ml, z, deep.data(), deep.data() + m_total, pre_z.data(), zh, false)
+                        : composition(kc, z, deep.data(), deep.data() + m_total, pre_z.data(), zh);
     deep[2 * m_total] = qmul(h, qinv(zh));
   }
   for (auto& v : deep) ch.absorb(v);
@@ -722,13 +814,16 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   DeepConsts dc{};
   dc.m_total = m_total, dc.n_pre = n_pre, dc.shift = shift, dc.log_N = lN;
   dc.offset = offset, dc.z = z, dc.qz = deep[2 * m_total];
-  for (uint32_t j = 0; j < n_deep; ++j) dc.gammas[j] = ch.sample_q();
-  for (uint32_t j = 0; j < 2 * m_total; ++j) dc.evals[j] = deep[j];
+  std::vector<qm31> ge(n_deep + 2 * m_total);  // gammas, then f_j(z), f_j(wz)
+  for (uint32_t j = 0; j < n_deep; ++j) ge[j] = ch.sample_q();
+  for (uint32_t j = 0; j < 2 * m_total; ++j) ge[n_deep + j] = deep[j];
   DevBuf<DeepConsts> d_dc(1, st);
   h2d_small(d_dc.p, &dc, sizeof(dc), st);
+  DevBuf<qm31> d_ge(ge.size(), st);
+  h2d_small(d_ge.p, ge.data(), ge.size() * sizeof(qm31), st);
   std::vector<std::unique_ptr<DevBuf<qm31>>> layers;
   layers.push_back(std::make_unique<DevBuf<qm31>>(N, st));
-  k_deep<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_dc.p, layers[0]->p);
+  k_deep<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_dc.p, d_ge.p, layers[0]->p);
   ZS_CUDA(cudaGetLastError());
 
   std::unique_ptr<FoldTables> ftabs_own;

@@ -2,6 +2,7 @@
 // (src/m31/fri.zig:277-336). Like the reference, verification is a host-side replay
 // of the transcript plus a few hundred hash and field operations per query; it is
 // not on the hot path and runs on the CPU.
+#include <memory>
 #include <vector>
 
 #include "constraints.cuh"
@@ -193,7 +194,8 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
   const uint32_t m = air.m, n_pre = air.n_pre, n_rel = air.n_rel, m_total = m + n_rel;
   const uint32_t n_deep = 2 * m_total + 1, reveal_len = 2 * m_total + 1 + n_pre;
   const uint32_t total_bound = air.num_bound + n_rel;
-  if (m_total > kMaxCols || air.num_trans > kMaxTrans || total_bound > kMaxBound || n_pre > kMaxPre)
+  const bool wide = air.id == AIR_ML_LINEAR;  // composed by ml_composition
+  if (!wide && (m_total > kMaxCols || air.num_trans > kMaxTrans || total_bound > kMaxBound || n_pre > kMaxPre))
     throw Error(ZS_EGENERIC, "AIR exceeds the compiled-in limits");
   if (air.fixed_n && n != air.fixed_n) throw Error(ZS_EMALFORMED, "the AIR is defined for a fixed trace length");
   if (air.id == AIR_RESCUE_STACKED && n < 8) throw Error(ZS_EMALFORMED, "stacked rescue needs at least 8 rows");
@@ -225,25 +227,41 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
   kc.m = m, kc.m_total = m_total, kc.n_pre = n_pre, kc.num_trans = air.num_trans, kc.n_rel = n_rel;
   kc.total_bound = total_bound;
   kc.last_point = qpow(w, n - 1);
-  for (uint32_t j = 0; j < air.n_lc; ++j) kc.ac[j] = ch.sample_q();
-  for (uint32_t r = 0; r < n_rel; ++r) kc.ar[r] = ch.sample_q();
-  for (uint32_t r = 0; r < n_rel; ++r) {
-    kc.sel[r] = air.sel[r], kc.mult[r] = air.mult[r], kc.n_keys[r] = air.n_keys[r];
-    for (uint32_t j = 0; j < air.n_keys[r]; ++j) kc.keys[r][j] = air.keys[r][j], kc.tabs[r][j] = air.tabs[r][j];
-  }
+  std::vector<qm31> ac(air.n_lc), ar(n_rel);
+  for (auto& a : ac) a = ch.sample_q();
+  for (auto& a : ar) a = ch.sample_q();
   for (auto& d : p.acc_roots) ch.absorb(d);
-  for (uint32_t t = 0; t < air.num_trans + 2 * n_rel; ++t) kc.alphas[t] = ch.sample_q();
+  std::vector<qm31> alphas(air.num_trans + 2 * n_rel);
+  for (auto& a : alphas) a = ch.sample_q();
   std::vector<Boundary> bnd;
   air.boundary(n, bnd);
   for (uint32_t r = 0; r < n_rel; ++r) bnd.push_back({m + r, 0, qzero()});
-  for (uint32_t b = 0; b < total_bound; ++b) {
-    kc.betas[b] = ch.sample_q();
-    kc.b_col[b] = bnd[b].column;
-    kc.b_val[b] = bnd[b].value;
-    kc.b_pt[b] = qpow(w, bnd[b].step);
+  std::vector<qm31> betas(total_bound);
+  for (auto& b : betas) b = ch.sample_q();
+  std::unique_ptr<MlConsts> ml;
+  if (wide) {
+    ml = std::make_unique<MlConsts>();
+    for (uint32_t l = 0; l < kMlDim; ++l) ml->ac[l] = ac[l];
+    ml->ar = ar[0];
+    ml->last_point = kc.last_point;
+    ml_set_weights(*ml, air, alphas, betas);
+  } else {
+    for (uint32_t j = 0; j < air.n_lc; ++j) kc.ac[j] = ac[j];
+    for (uint32_t r = 0; r < n_rel; ++r) kc.ar[r] = ar[r];
+    for (uint32_t r = 0; r < n_rel; ++r) {
+      kc.sel[r] = air.sel[r], kc.mult[r] = air.mult[r], kc.n_keys[r] = air.n_keys[r];
+      for (uint32_t j = 0; j < air.n_keys[r]; ++j) kc.keys[r][j] = air.keys[r][j], kc.tabs[r][j] = air.tabs[r][j];
+    }
+    for (uint32_t t = 0; t < alphas.size(); ++t) kc.alphas[t] = alphas[t];
+    for (uint32_t b = 0; b < total_bound; ++b) {
+      kc.betas[b] = betas[b];
+      kc.b_col[b] = bnd[b].column;
+      kc.b_val[b] = bnd[b].value;
+      kc.b_pt[b] = qpow(w, bnd[b].step);
+    }
+    group_boundaries(kc);
+    if (const char* bad = quot_consts_out_of_range(kc, 0)) throw Error(ZS_EGENERIC, bad);
   }
-  group_boundaries(kc);
-  if (const char* bad = quot_consts_out_of_range(kc, 0)) throw Error(ZS_EGENERIC, bad);
   ch.absorb(p.qroot);
   const qm31 z = ch.sample_q();
   for (auto& v : p.deep) ch.absorb(v);
@@ -285,8 +303,9 @@ bool stark_verify(uint32_t air_id, const uint8_t* params_b, size_t params_len, c
     const qm31 leaf = p0 == p1 ? p.fq[qi].pairs[0].v0 : p.fq[qi].pairs[0].v1;
     if (!qeq(g, leaf)) return false;
     const qm31 zh = qsub(qpow(x0, n), qone());
-    const qm31 h = composition(kc, x0, rv.values.data(), rv.values.data() + m_total,
-                               rv.values.data() + 2 * m_total + 1, zh);
+    const qm31* vals = rv.values.data();
+    const qm31 h = wide ? ml_composition(*ml, x0, vals, vals + m_total, vals + 2 * m_total + 1, zh, false)
+                        : composition(kc, x0, vals, vals + m_total, vals + 2 * m_total + 1, zh);
     if (!qeq(h, qmul(zh, rv.values[2 * m_total]))) return false;
   }
   return true;

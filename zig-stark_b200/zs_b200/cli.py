@@ -12,7 +12,7 @@ import time
 from . import native
 from . import workload as wl
 
-AIRS = {"seeded_fib": wl.AIR_SEEDED_FIB, "rescue_stacked": wl.AIR_RESCUE_STACKED}
+AIRS = {"seeded_fib": wl.AIR_SEEDED_FIB, "rescue_stacked": wl.AIR_RESCUE_STACKED, "ml_linear": wl.AIR_ML_LINEAR}
 
 
 def main(argv=None):
@@ -22,10 +22,10 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=2)
     ap.add_argument("--seed", type=int, default=3)
     args = ap.parse_args(argv)
-    air, params, pi, trace, sep = wl.proof_job(AIRS[args.air], args.log_rows, args.seed, b"zig-stark:cli")
+    air, params, pi, trace, sep, pre = wl.proof_job(AIRS[args.air], args.log_rows, args.seed, b"zig-stark:cli")
     for i in range(args.repeat):
         t0 = time.perf_counter()
-        proof = native.prove(air, params, pi, trace, b"", sep)
+        proof = native.prove(air, params, pi, trace, pre, sep)
         print(f"proof {i}: {len(proof)} bytes in {1e3 * (time.perf_counter() - t0):.2f} ms", flush=True)
 
 

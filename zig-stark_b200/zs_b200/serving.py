@@ -1,8 +1,8 @@
 """Request streams over the proof server (zs_m31_server_*): open-loop arrivals,
 continuous batching on the device, per-request latency.
 
-A request is a tuple (air_id, params, public_inputs, trace, channel_sep) of wire
-bytes. `replay` submits each request at its arrival time from one thread while
+A request is a tuple (air_id, params, public_inputs, trace, channel_sep[,
+preprocessed]) of wire bytes (workload.ProofJob). `replay` submits each request at its arrival time from one thread while
 another collects the results, so arrivals never wait for completions (open loop).
 """
 import threading
@@ -52,8 +52,9 @@ def replay(requests, arrivals, workers, hbm_budget=0, keep_proofs=False):
                 delay = t0 + at - time.perf_counter()
                 if delay > 0:
                     time.sleep(delay)
-                air, params, pi, trace, sep = req
-                tickets[i] = srv.submit(air, params, pi, trace, b"", sep)
+                air, params, pi, trace, sep = req[:5]
+                pre = req[5] if len(req) > 5 else b""
+                tickets[i] = srv.submit(air, params, pi, trace, pre, sep)
                 ready[i].set()
 
         th = threading.Thread(target=submitter)

@@ -9,6 +9,8 @@ challenges alpha).
 Trace generators follow the reference AIRs' own ``generateTrace`` functions
 (src/m31/stark.zig:908-925, 999-1030, 1081-1120, 1173-1205).
 """
+from collections import namedtuple
+
 import numpy as np
 
 from . import wire
@@ -304,6 +306,54 @@ def rescue_stacked(trace_log, seed=SEED_RESCUE):
 
 
 # ---------------------------------------------------------------------------
+# One linear layer y = W x over a batch of input vectors (AIR_ML_LINEAR)
+# ---------------------------------------------------------------------------
+
+AIR_ML_LINEAR = 8
+SEED_ML_LINEAR = 0x5EED0006
+ML_DIM = 128
+
+
+def uniform_below(seed, count, bound):
+    """`count` values uniform in [0, bound) for a power-of-two bound (top bits of
+    SplitMix64 outputs)."""
+    shift = 64 - (int(bound).bit_length() - 1)
+    return (splitmix64(seed, count) >> np.uint64(shift)).astype(np.uint32)
+
+
+def ml_linear(trace_log, seed=SEED_ML_LINEAR, vectors=None):
+    """The linear-layer workload: W (128 x 128) and 2^(trace_log - 1) input vectors,
+    entries uniform in [0, 2^16) (W from `seed`, the inputs from seed + 1).
+
+    Rows [0, V) hold the input vectors (sel = 1, mult = 1) with y = W x mod p; rows
+    [V, n) are the input table's rows (sel = 0, x = y = 0), where the preprocessed
+    columns P_0..P_127 hold the same vectors. The LogUp relation then matches every
+    input vector with its table row. Returns (trace, preprocessed, public_inputs) with
+    PublicInputs {w: []QM31}."""
+    n = 1 << trace_log
+    V = vectors if vectors is not None else n // 2
+    if not 0 < V <= n // 2:
+        raise ValueError("at most half the rows hold input vectors")
+    D = ML_DIM
+    W = uniform_below(seed, D * D, 1 << 16).reshape(D, D)
+    X = uniform_below(seed + 1, V * D, 1 << 16).reshape(V, D)
+    Y = (X.astype(np.uint64) @ W.T.astype(np.uint64)) % P  # < 128 * 2^32: exact in u64
+    x_cols = np.zeros((D, n), dtype=np.uint32)
+    y_cols = np.zeros((D, n), dtype=np.uint32)
+    p_cols = np.zeros((D, n), dtype=np.uint32)
+    x_cols[:, :V] = X.T
+    y_cols[:, :V] = Y.T.astype(np.uint32)
+    p_cols[:, n - V:] = X.T
+    sel = np.zeros(n, dtype=np.uint32)
+    sel[:V] = 1
+    trace = [wire.m31_column_as_qm31(c) for c in x_cols] + [wire.m31_column_as_qm31(c) for c in y_cols]
+    trace += [wire.m31_column_as_qm31(sel), wire.m31_column_as_qm31(sel.copy())]
+    pre = [wire.m31_column_as_qm31(c) for c in p_cols]
+    pi = wire.qm31_slice(wire.m31_column_as_qm31(W.reshape(-1)))
+    return trace, pre, pi
+
+
+# ---------------------------------------------------------------------------
 # Mixed-size proof streams (batched and served proving)
 # ---------------------------------------------------------------------------
 
@@ -315,16 +365,25 @@ def _mix(seed, index):
     return int(splitmix64((seed ^ (index * 0xD1B54A32D192ED03)) & MASK64, 1)[0])
 
 
+class ProofJob(namedtuple("ProofJob", "air params pi trace sep pre")):
+    """One proof request in wire form: AIR id, StarkParams, public inputs, trace columns,
+    channel separator and preprocessed columns (b"" when the AIR has none)."""
+
+
 def proof_job(air, trace_log, seed, sep, num_queries=16, remainder_log=3):
-    """One proof request at blowup 4: (air, params bytes, public inputs, trace bytes, sep)."""
+    """One proof request at blowup 4 (a ProofJob)."""
+    pre = b""
     if air == AIR_SEEDED_FIB:
         tr, pi = seeded_fib(trace_log, seed)
     elif air == AIR_RESCUE_STACKED:
         tr, pi = rescue_stacked(trace_log, seed)
+    elif air == AIR_ML_LINEAR:
+        tr, pre_cols, pi = ml_linear(trace_log, seed)
+        pre = wire.columns(pre_cols)
     else:
         raise ValueError(f"no stream generator for AIR {air}")
     params = wire.StarkParams(trace_log, 2, num_queries, remainder_log).encode()
-    return (air, params, pi, wire.columns(tr), sep)
+    return ProofJob(air, params, pi, wire.columns(tr), sep, pre)
 
 
 def batch_shapes(count, seed=SEED_BATCH, log_min=10, log_max=20):
@@ -340,19 +399,29 @@ def batch_shapes(count, seed=SEED_BATCH, log_min=10, log_max=20):
     return out
 
 
-def serve_shapes(count, seed=SEED_SERVE, log_min=12, log_max=22, p_geo=0.5, mix=(0.5, 0.5)):
-    """Served-stream requests: AIR by `mix` (Fibonacci, stacked Rescue), log2 rows from a
-    geometric distribution (success probability p_geo) truncated to [log_min, log_max]."""
+ML_LINEAR_MAX_LOG = 15  # 2^14 input vectors: the linear layer's full size
+
+
+def serve_shapes(count, seed=SEED_SERVE, log_min=12, log_max=22, p_geo=0.5, mix=(0.5, 0.3, 0.2)):
+    """Served-stream requests: AIR by `mix` (Fibonacci, stacked Rescue, linear layer),
+    log2 rows from a geometric distribution (success probability p_geo) truncated to
+    [log_min, log_max]. A linear-layer request holds 2^(rows - 1) input vectors of 387
+    committed columns, so its rows are capped at 2^15 (2^14 vectors, the layer's full
+    size)."""
     out = []
     span = log_max - log_min + 1
     w = np.array([(1 - p_geo) ** k * p_geo for k in range(span)])
     cdf = np.cumsum(w / w.sum())
+    edges = np.cumsum(np.asarray(mix, dtype=np.float64) / sum(mix))
+    airs = (AIR_SEEDED_FIB, AIR_RESCUE_STACKED, AIR_ML_LINEAR)
     for i in range(count):
         r = _mix(seed, i)
         u = ((r >> 11) & ((1 << 53) - 1)) / float(1 << 53)
         lg = log_min + int(np.searchsorted(cdf, u, side="right"))
         lg = min(lg, log_max)
         v = (r & 0x3FF) / 1024.0
-        air = AIR_SEEDED_FIB if v < mix[0] / sum(mix) else AIR_RESCUE_STACKED
+        air = airs[min(int(np.searchsorted(edges, v, side="right")), len(mix) - 1)]
+        if air == AIR_ML_LINEAR:
+            lg = min(lg, ML_LINEAR_MAX_LOG)
         out.append((air, lg, _mix(seed ^ 0xABCDEF, i), b"zs-serve:%d" % i))
     return out
