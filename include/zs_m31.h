@@ -44,7 +44,13 @@ typedef struct {
  *   ZS_AIR_LINEAR_EXAMPLE  examples/ml_linear (8 rows)          PI {x: []QM31, claimed_y: QM31}
  *   ZS_AIR_RESCUE_STACKED  the rescue example's permutation, 8 rows each, stacked to
  *                          any 2^k >= 8 rows with square/cube helper columns (12
- *                          columns, degree 2(n-1) + n/8)    PI {initial: [4]QM31, final: [4]QM31} */
+ *                          columns, degree 2(n-1) + n/8)    PI {initial: [4]QM31, final: [4]QM31}
+ *   ZS_AIR_ML_LINEAR       examples/ml_linear widened to one linear layer y = W x, W
+ *                          128 x 128: columns x_0..x_127, y_0..y_127, sel, mult; 128
+ *                          preprocessed columns holding the input table; one LogUp
+ *                          relation binding every input vector (sel = 1 rows) to a
+ *                          table row (sel = 0 rows); sel = 0 on the last row
+ *                                                           PI {w: []QM31, 16384 M31 values} */
 enum {
     ZS_AIR_FIB = 0,
     ZS_AIR_SEEDED_FIB = 1,
@@ -53,7 +59,8 @@ enum {
     ZS_AIR_MULTIPLICITY = 4,
     ZS_AIR_RESCUE_EXAMPLE = 5,
     ZS_AIR_LINEAR_EXAMPLE = 6,
-    ZS_AIR_RESCUE_STACKED = 7
+    ZS_AIR_RESCUE_STACKED = 7,
+    ZS_AIR_ML_LINEAR = 8
 };
 
 /* ---- prover ------------------------------------------------------------------
@@ -141,7 +148,10 @@ int32_t zs_m31_server_poll(zs_m31_server *server, uint64_t ticket, int32_t wait,
 /* Replaces GenericStark(Air).verify (src/m31/stark.zig:660-784); conventions of
  * zs_binius_verify (zig-capi.h:53-63). Sets *out_ok to 1 when the proof verifies and
  * 0 otherwise; returns 0, or a negative code when the inputs cannot be parsed. Runs
- * on the host (the reference's verifier is a few hundred hashes per query). */
+ * on the host (the reference's verifier is a few hundred hashes per query). One
+ * deliberate difference: the reference checks only the query reveals a proof carries
+ * (stark.zig:713), so it accepts a proof whose reveal list is cut short; this verifier
+ * requires one reveal per FRI query (honest proofs always carry that many). */
 int32_t zs_m31_verify(zs_host_allocator host, uint32_t air_id, const uint8_t *params, size_t params_len,
                       const uint8_t *public_inputs, size_t public_inputs_len, const uint8_t *proof, size_t proof_len,
                       const uint8_t *channel_sep, size_t channel_sep_len, int *out_ok);
