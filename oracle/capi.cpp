@@ -1,6 +1,7 @@
 // ORACLE — test infrastructure only. C entry points over the CPU restatement,
 // loaded by the tests (ctypes) as the checker for the GPU backend. Buffers the
 // oracle returns are malloc'ed and released with orc_free.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
@@ -308,6 +309,26 @@ int orc_commit_columns(const uint8_t* cols, size_t cols_len, unsigned trace_log,
 }
 
 // Re-serializes a proof after a round trip through the wire reader.
+// serialization.zig:220-250 "golden wire layout is stable": the struct
+// {name: [3]u8 = "abc", count: u32 = 0x01020304, rows: []u16 = {0x0102, 0x0304},
+// flag: bool = true, maybe: ?[2]u8 = {0xde, 0xad}} through the oracle's Writer.
+// Writes at most 64 bytes; returns the length.
+size_t orc_wire_golden(uint8_t* out) {
+  Writer w;
+  const uint8_t name[3] = {'a', 'b', 'c'};
+  w.raw(name, 3);
+  w.uint_le(0x01020304u, 4);
+  const uint16_t rows[2] = {0x0102, 0x0304};
+  w.u64(2);
+  for (uint16_t r : rows) w.uint_le(r, 2);
+  w.flag(true);
+  const uint8_t maybe[2] = {0xde, 0xad};
+  w.flag(true);
+  w.raw(maybe, 2);
+  std::memcpy(out, w.out.data(), std::min<size_t>(w.out.size(), 64));
+  return w.out.size();
+}
+
 int orc_proof_roundtrip(const uint8_t* proof, size_t proof_len, uint8_t** out, size_t* out_len) {
   try {
     StarkProof p = StarkProof::deserialize(proof, proof_len);

@@ -44,6 +44,7 @@ def lib():
         L.orc_circle_ifft.argtypes = [u32p, ctypes.c_uint, u32p, ctypes.c_int]
         L.orc_circle_eval_at.argtypes = [u32p, ctypes.c_uint, ctypes.c_uint32, ctypes.c_uint32]
         L.orc_circle_eval_at.restype = ctypes.c_uint32
+        L.orc_wire_golden.restype = ctypes.c_size_t
         L.orc_circle_twiddles.argtypes = [ctypes.c_uint, u32p]
         L.orc_merkle_root.argtypes = [ctypes.c_char_p, ctypes.c_size_t, u8p]
         L.orc_interpolate_subgroup.argtypes = [u32p, ctypes.c_uint, ctypes.c_int, u32p]

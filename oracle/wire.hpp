@@ -21,10 +21,15 @@ struct WireError : std::runtime_error {
 
 struct Writer {
   std::vector<uint8_t> out;
-  void u8(uint8_t v) { out.push_back(v); }
-  void u64(uint64_t v) {
-    for (int i = 0; i < 8; ++i) out.push_back((uint8_t)(v >> (8 * i)));
+  // serialization.zig:58-120: ints little-endian at their own width, usize and slice
+  // lengths as u64, bool and an optional's presence as one byte, arrays raw.
+  void uint_le(uint64_t v, unsigned width) {
+    for (unsigned i = 0; i < width; ++i) out.push_back((uint8_t)(v >> (8 * i)));
   }
+  void u8(uint8_t v) { uint_le(v, 1); }
+  void u64(uint64_t v) { uint_le(v, 8); }
+  void flag(bool present) { u8(present ? 1 : 0); }
+  void raw(const uint8_t* p, size_t n) { out.insert(out.end(), p, p + n); }
   void digest(const Digest& d) { out.insert(out.end(), d.begin(), d.end()); }
   void qm31(const QM31& v) {
     uint8_t b[16];

@@ -16,13 +16,38 @@ P = 2**31 - 1
 rng = np.random.default_rng(44)
 
 
-def test_golden_wire_layout():
-    # serialization.zig:220-250, encoded with the same rules wire.py uses
-    expected = bytes([ord("a"), ord("b"), ord("c"), 0x04, 0x03, 0x02, 0x01,
-                      0x02, 0, 0, 0, 0, 0, 0, 0, 0x02, 0x01, 0x04, 0x03, 0x01, 0x01, 0xDE, 0xAD])
+GOLDEN = bytes([ord("a"), ord("b"), ord("c"), 0x04, 0x03, 0x02, 0x01,
+                0x02, 0, 0, 0, 0, 0, 0, 0, 0x02, 0x01, 0x04, 0x03, 0x01, 0x01, 0xDE, 0xAD])
+
+
+def test_golden_wire_layout_oracle_writer(orc):
+    """serialization.zig:220-250: {name: [3]u8, count: u32, rows: []u16, flag: bool,
+    maybe: ?[2]u8} through the oracle's wire writer (oracle/wire.hpp)."""
+    import ctypes
+    out = (ctypes.c_uint8 * 64)()
+    n = orc.lib().orc_wire_golden(out)
+    assert bytes(out)[:n] == GOLDEN
+
+
+def test_golden_wire_layout_library_writer(tmp_path):
+    """The same struct through the library's wire writer (csrc/host.cuh), the one every
+    proof is serialized with, compiled for the host."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "wire_golden")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I", os.path.join(root, "zig-stark_b200", "csrc"),
+                    "-I", "/usr/local/cuda/include", os.path.join(root, "tests", "wire_golden.cpp"), "-o", exe],
+                   check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.strip()
+    assert bytes.fromhex(out) == GOLDEN
+
+
+def test_golden_wire_layout_python_mirror():
+    # the Python mirror (zs_b200/wire.py) follows the same rules
     enc = b"abc" + struct.pack("<I", 0x01020304) + wire.u64(2) + struct.pack("<2H", 0x0102, 0x0304) \
         + wire.u8(1) + wire.u8(1) + bytes([0xDE, 0xAD])
-    assert enc == expected
+    assert enc == GOLDEN
 
 
 def _fri_coeffs(log_size, seed):

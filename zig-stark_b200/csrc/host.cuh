@@ -16,12 +16,13 @@ using Digest = std::array<uint8_t, 32>;
 
 struct WireWriter {
   std::vector<uint8_t> out;
-  void u8(uint8_t v) { out.push_back(v); }
-  void u64(uint64_t v) {
-    uint8_t b[8];
-    for (int i = 0; i < 8; ++i) b[i] = (uint8_t)(v >> (8 * i));
-    bytes(b, 8);
+  // An unsigned integer of `width` bytes, little-endian (every int on the wire).
+  void uint_le(uint64_t v, unsigned width) {
+    for (unsigned i = 0; i < width; ++i) out.push_back((uint8_t)(v >> (8 * i)));
   }
+  void u8(uint8_t v) { uint_le(v, 1); }
+  void u64(uint64_t v) { uint_le(v, 8); }  // also every usize and slice length
+  void flag(bool present) { u8(present ? 1 : 0); }  // bool, and an optional's presence byte
   void bytes(const void* p, size_t n) {
     const uint8_t* b = (const uint8_t*)p;
     out.insert(out.end(), b, b + n);
