@@ -485,7 +485,8 @@ def proof_metrics(args, local, budget_s=90.0):
         r = serving.replay(sjobs, arrivals, 8)
         lat = r["latency_ms"]
         row = {"requests": len(sjobs), "proofs_per_s": len(sjobs) / r["wall_s"],
-               "p50_ms": serving.percentile(lat, 50), "p99_ms": serving.percentile(lat, 99), "failed": r["failed"]}
+               "p50_ms": serving.percentile(lat, 50), "p99_ms": serving.percentile(lat, 99), "failed": r["failed"],
+               "submit_lag_p99_ms": serving.percentile(r["submit_lag_ms"], 99)}
         if rate == 400.0:
             rp = serving.replay(sjobs, arrivals, 1)
             row["plain"] = {"proofs_per_s": len(sjobs) / rp["wall_s"],

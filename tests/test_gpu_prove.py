@@ -238,7 +238,7 @@ def test_blowups_above_8(orc, air, trace_log, log_blowup, rem):
     assert native.verify(air, params, pi, proof, b"blowup")
 
 
-@pytest.mark.parametrize("trace_log", [1, 5, 8, 12])
+@pytest.mark.parametrize("trace_log", [2, 5, 8, 12])
 def test_ml_linear(orc, trace_log):
     """The linear layer y = W x (W 128 x 128, inputs bound to the preprocessed input
     table by LogUp) at growing batch sizes, against the oracle."""

@@ -217,11 +217,12 @@ struct Server {
 
   // Queues a job; `copy` makes the server's own copy of the caller's buffers.
   uint64_t submit(const zs_m31_job& j, bool copy) {
+    const auto t_submit = std::chrono::steady_clock::now();  // a request's latency includes taking its copy
     Job job = copy ? copy_job(j) : view_job(j);
     job.footprint = estimate_footprint(j);
     auto e = std::make_unique<Entry>();
     e->job = std::move(job);
-    e->t_submit = std::chrono::steady_clock::now();
+    e->t_submit = t_submit;
     uint64_t t;
     {
       std::lock_guard<std::mutex> lk(mu);

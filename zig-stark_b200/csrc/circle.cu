@@ -133,40 +133,15 @@ CircleDomain::~CircleDomain() {
 // Butterfly arithmetic
 // ---------------------------------------------------------------------------
 
-// The transforms are bound by integer issue. The plain M31 operations (field.cuh) put
-// all their additions, shifts and minima on the ALU pipe, which accepts an instruction
-// every other cycle, while the FMA pipe beside it, which runs integer multiply-adds,
-// idles. These variants move part of each operation to multiply-adds: a + b as
-// a * 1 + b, a - b as b * (2^32 - 1) + a, and the Mersenne fold of a product as a
-// multiply-high. The multipliers come from constant memory so that the compiler
-// keeps the multiply-adds. Results are the canonical values of madd / msub / mmul.
-__constant__ uint32_t c_pipe[3] = {1u, 0xffffffffu, 0x80000000u};
-
-__device__ __forceinline__ uint32_t imad_lo(uint32_t a, uint32_t b, uint32_t c) {
-  uint32_t r;
-  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
-  return r;
-}
-__device__ __forceinline__ uint32_t imad_hi(uint32_t a, uint32_t b, uint32_t c) {
-  uint32_t r;
-  asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
-  return r;
-}
-// a + b mod p, a, b < p.
-__device__ __forceinline__ uint32_t madd2(uint32_t a, uint32_t b) {
-  return umin32(imad_lo(a, c_pipe[0], b), a + b - P);
-}
-// a - b mod p, a, b < p.
-__device__ __forceinline__ uint32_t msub2(uint32_t a, uint32_t b) {
-  return umin32(imad_lo(b, c_pipe[1], a), a - b + P);
-}
-// a * t mod p for a < p and a twiddle stored doubled, t2 = 2t (every twiddle table
-// of this file holds doubled values). a * t2 = 2at, so its high word is at >> 31 and
-// its low word is 2 (at & p); hi + (lo >> 1) <= 2p - 2 is the Mersenne fold of at.
+// Every twiddle table of this file holds each twiddle doubled, t2 = 2t < 2^32. Then
+// a * t2 = 2at, whose high word is at >> 31 and whose low word is 2 (at & p), so the
+// Mersenne fold of at is hi + (lo >> 1) <= 2p - 2: one 32 x 32 -> 64 multiply and one
+// shift-add, where a product of undoubled values needs a mask, a 64-bit shift and an
+// add. The result is mmul's canonical value (field.cuh).
 __device__ __forceinline__ uint32_t mmul2(uint32_t a, uint32_t t2) {
-  const uint32_t lo = a * t2, hi = __umulhi(a, t2);
-  const uint32_t s = imad_hi(lo, c_pipe[2], hi);
-  return umin32(s, imad_lo(s, c_pipe[0], 0x80000001u));  // s - p
+  const uint64_t prod = (uint64_t)a * t2;
+  const uint32_t s = (uint32_t)(prod >> 32) + ((uint32_t)prod >> 1);
+  return umin32(s, s - P);
 }
 
 // ---------------------------------------------------------------------------
@@ -214,8 +189,8 @@ __device__ __forceinline__ void chunk(uint32_t* s, uint32_t gstride, unsigned G,
           const int m1 = m0 | (1 << l);
           const uint32_t t = tws[m0 >> (l + 1)];
           const uint32_t x1 = mmul2(v[m1], t), x0 = v[m0];
-          v[m1] = msub2(x0, x1);
-          v[m0] = madd2(x0, x1);
+          v[m1] = msub(x0, x1);
+          v[m0] = madd(x0, x1);
         }
       }
     } else {
@@ -233,8 +208,8 @@ __device__ __forceinline__ void chunk(uint32_t* s, uint32_t gstride, unsigned G,
           const int m1 = m0 | (1 << l);
           const uint32_t t = tws[m0 >> (l + 1)];
           const uint32_t x0 = v[m0], x1 = v[m1];
-          v[m0] = madd2(x0, x1);
-          v[m1] = mmul2(msub2(x0, x1), t);
+          v[m0] = madd(x0, x1);
+          v[m1] = mmul2(msub(x0, x1), t);
         }
       }
     }
@@ -255,67 +230,100 @@ __device__ __forceinline__ void chunk_dispatch(unsigned r, uint32_t* s, uint32_t
   }
 }
 
+// C consecutive twiddles from T into registers, as 16- or 8-byte loads where C allows
+// (a chunk's twiddle run for layer i starts at TW[n - (n >> i) + Vh * C], a multiple of
+// C words from a 256-byte-aligned table, so the vector loads are aligned).
+template <int C>
+__device__ __forceinline__ void load_twiddles(uint32_t* dst, const uint32_t* __restrict__ T) {
+  if constexpr (C >= 4) {
+#pragma unroll
+    for (int q = 0; q < C / 4; ++q) {
+      const uint4 x = __ldg(reinterpret_cast<const uint4*>(T) + q);
+      dst[4 * q] = x.x, dst[4 * q + 1] = x.y, dst[4 * q + 2] = x.z, dst[4 * q + 3] = x.w;
+    }
+  } else if constexpr (C == 2) {
+    const uint2 x = __ldg(reinterpret_cast<const uint2*>(T));
+    dst[0] = x.x, dst[1] = x.y;
+  } else {
+    dst[0] = __ldg(T);
+  }
+}
+
+// The R layers of one chunk on the 2^R values in registers: layer LL of the chunk's
+// order (top-down forward, bottom-up inverse), then the rest. base_i: the global layer
+// of the chunk's lowest layer; Vh: the virtual block index of the slot's lowest
+// element at the chunk's top.
+template <int R, bool INV, int LL>
+__device__ __forceinline__ void chunk_layers(uint32_t* v, const uint32_t* __restrict__ TW, uint32_t n_dom,
+                                             unsigned base_i, uint32_t Vh) {
+  if constexpr (LL < R) {
+    constexpr int l = INV ? LL : R - 1 - LL;
+    const unsigned i = base_i + l;
+    uint32_t tws[1 << (R - 1 - l)];
+    load_twiddles<(1 << (R - 1 - l))>(tws, TW + (n_dom - (n_dom >> i)) + (Vh << (R - l - 1)));
+#pragma unroll
+    for (int m0 = 0; m0 < (1 << R); ++m0) {
+      if (m0 & (1 << l)) continue;
+      const int m1 = m0 | (1 << l);
+      const uint32_t t = tws[m0 >> (l + 1)];
+      if (!INV) {
+        const uint32_t x1 = mmul2(v[m1], t), x0 = v[m0];
+        v[m1] = msub(x0, x1);
+        v[m0] = madd(x0, x1);
+      } else {
+        const uint32_t x0 = v[m0], x1 = v[m1];
+        v[m0] = madd(x0, x1);
+        v[m1] = mmul2(msub(x0, x1), t);
+      }
+    }
+    chunk_layers<R, INV, LL + 1>(v, TW, n_dom, base_i, Vh);
+  }
+}
+
 // Compile-time variant of `chunk` for a known group size 2^M and chunk offset B0.
 // The chunk's index bits never overlap the slot's, so element m sits at
 // padx(e0) + padx(m << B0): one runtime address per slot, immediate offsets after it.
-template <int R, bool INV, unsigned M, unsigned B0>
-__device__ __forceinline__ void chunk_ct(uint32_t* s, uint32_t gstride, unsigned G, unsigned shift,
-                                         const uint32_t* __restrict__ TW, uint32_t n_dom, const uint32_t* vb) {
+// Reads the groups from `src` and writes them to `dst` (the same layout; in place when
+// they are equal); with SCALE, multiplies every output by 2^scale_sh (a rotation).
+template <int R, bool INV, unsigned M, unsigned B0, bool SCALE = false>
+__device__ __forceinline__ void chunk_ct(const uint32_t* src, uint32_t* dst, uint32_t gstride, unsigned G,
+                                         unsigned shift, const uint32_t* __restrict__ TW, uint32_t n_dom,
+                                         const uint32_t* vb, unsigned scale_sh = 0) {
   constexpr unsigned SL = M - R;
   const uint32_t total = G << SL;
   for (uint32_t slot = threadIdx.x; slot < total; slot += blockDim.x) {
     const uint32_t gi = slot >> SL;
     const uint32_t rest = slot & ((1u << SL) - 1);
     const uint32_t e0 = ((rest >> B0) << (B0 + R)) | (rest & ((1u << B0) - 1));
-    uint32_t* base = s + gi * gstride + padx(e0);
+    const uint32_t off = gi * gstride + padx(e0);
     uint32_t v[1 << R];
 #pragma unroll
-    for (int m = 0; m < (1 << R); ++m) v[m] = base[(m << B0) + ((m << B0) >> 5)];
+    for (int m = 0; m < (1 << R); ++m) v[m] = src[off + (m << B0) + ((m << B0) >> 5)];
     const uint32_t Vh = (vb[gi] + e0) >> (B0 + R);
+    chunk_layers<R, INV, 0>(v, TW, n_dom, B0 + shift, Vh);
 #pragma unroll
-    for (int ll = 0; ll < R; ++ll) {
-      const int l = INV ? ll : R - 1 - ll;
-      const unsigned i = B0 + l + shift;
-      const uint32_t* T = TW + (n_dom - (n_dom >> i)) + (Vh << (R - l - 1));
-      uint32_t tws[1 << (R - 1)];
-#pragma unroll
-      for (int hb = 0; hb < (1 << (R - 1)); ++hb)
-        if (hb < (1 << (R - 1 - l))) tws[hb] = __ldg(T + hb);
-#pragma unroll
-      for (int m0 = 0; m0 < (1 << R); ++m0) {
-        if (m0 & (1 << l)) continue;
-        const int m1 = m0 | (1 << l);
-        const uint32_t t = tws[m0 >> (l + 1)];
-        if (!INV) {
-          const uint32_t x1 = mmul2(v[m1], t), x0 = v[m0];
-          v[m1] = msub2(x0, x1);
-          v[m0] = madd2(x0, x1);
-        } else {
-          const uint32_t x0 = v[m0], x1 = v[m1];
-          v[m0] = madd2(x0, x1);
-          v[m1] = mmul2(msub2(x0, x1), t);
-        }
-      }
-    }
-#pragma unroll
-    for (int m = 0; m < (1 << R); ++m) base[(m << B0) + ((m << B0) >> 5)] = v[m];
+    for (int m = 0; m < (1 << R); ++m)
+      dst[off + (m << B0) + ((m << B0) >> 5)] = SCALE ? mshl(v[m], scale_sh) : v[m];
   }
 }
 
 // All M layers with a compile-time chunk schedule (chunks of <= 5 layers, the
-// largest first), DONE layers already applied.
-template <bool INV, unsigned M, unsigned DONE>
-__device__ __forceinline__ void run_layers_ct(uint32_t* s, uint32_t gstride, unsigned G, unsigned shift,
-                                              const uint32_t* TW, uint32_t n_dom, const uint32_t* vb) {
+// largest first), DONE layers already applied. The first chunk reads `src`, every
+// chunk writes `dst`; with SCALE the last chunk multiplies its outputs by 2^scale_sh.
+template <bool INV, unsigned M, unsigned DONE, bool SCALE = false>
+__device__ __forceinline__ void run_layers_ct(const uint32_t* src, uint32_t* dst, uint32_t gstride, unsigned G,
+                                              unsigned shift, const uint32_t* TW, uint32_t n_dom, const uint32_t* vb,
+                                              unsigned scale_sh = 0) {
   if constexpr (DONE < M) {
     constexpr unsigned REM = M - DONE;
     constexpr unsigned NCH = (REM + 4) / 5;
     constexpr unsigned R = (REM + NCH - 1) / NCH;
     // forward: top-down, the chunk covers [M - DONE - R, M - DONE); inverse: bottom-up
     constexpr unsigned B0 = INV ? DONE : M - DONE - R;
-    chunk_ct<R, INV, M, B0>(s, gstride, G, shift, TW, n_dom, vb);
+    constexpr bool LAST = DONE + R == M;
+    chunk_ct<R, INV, M, B0, SCALE && LAST>(src, dst, gstride, G, shift, TW, n_dom, vb, scale_sh);
     __syncthreads();
-    run_layers_ct<INV, M, DONE + R>(s, gstride, G, shift, TW, n_dom, vb);
+    run_layers_ct<INV, M, DONE + R, SCALE>(dst, dst, gstride, G, shift, TW, n_dom, vb, scale_sh);
   }
 }
 
@@ -326,10 +334,10 @@ __device__ __forceinline__ void run_layers(uint32_t* s, uint32_t gstride, unsign
                            const uint32_t* TW, uint32_t n_dom, const uint32_t* vb) {
   if (M == 0) return;
   switch (M) {
-    case 8: return run_layers_ct<INV, 8, 0>(s, gstride, G, shift, TW, n_dom, vb);
-    case 9: return run_layers_ct<INV, 9, 0>(s, gstride, G, shift, TW, n_dom, vb);
-    case 10: return run_layers_ct<INV, 10, 0>(s, gstride, G, shift, TW, n_dom, vb);
-    case 11: return run_layers_ct<INV, 11, 0>(s, gstride, G, shift, TW, n_dom, vb);
+    case 8: return run_layers_ct<INV, 8, 0>(s, s, gstride, G, shift, TW, n_dom, vb);
+    case 9: return run_layers_ct<INV, 9, 0>(s, s, gstride, G, shift, TW, n_dom, vb);
+    case 10: return run_layers_ct<INV, 10, 0>(s, s, gstride, G, shift, TW, n_dom, vb);
+    case 11: return run_layers_ct<INV, 11, 0>(s, s, gstride, G, shift, TW, n_dom, vb);
     default: break;
   }
   const unsigned nch = (M + 3) / 4, base = M / nch, extra = M % nch;
@@ -365,6 +373,75 @@ __device__ __forceinline__ void cp_async4(uint32_t* smem, const uint32_t* gmem) 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
+// Bit reversal of a compile-time value (the unrolled loops' constant offsets).
+__host__ __device__ constexpr uint32_t cbitrev(uint32_t x, unsigned bits) {
+  uint32_t r = 0;
+  for (unsigned b = 0; b < bits; ++b) r |= ((x >> b) & 1u) << (bits - 1 - b);
+  return r;
+}
+
+constexpr unsigned kLowThreads = 256;
+
+// Moves between global memory and a batch of G padded groups in shared memory, for a
+// size-2^LG transform split at K (groups of 2^K), hb = LG - K. Two orders:
+//   contiguous: element e of group t is global word gbase(t) + e;
+//   bit-reversed: element bitrev_K(v) of group t is global word (v << hb) + g0 + t.
+// KC, GC: 0, or K and G known at compile time with 2^K >= kLowThreads >= G and
+// kLowThreads / G = 2^a, K - a >= 5. Then a thread keeps one (t, low bits of v) or
+// one e for the whole batch and every other offset is a constant: in the bit-reversed
+// order, bitrev_K(vlo + (k << a)) = (bitrev_a(vlo) << (K - a)) | bitrev_(K-a)(k), and
+// padx() of a multiple of 32 plus r < 32 is padx of the first plus r.
+template <unsigned KC, unsigned GC>
+struct LowIO {
+  static constexpr bool kFast = KC != 0;
+  static constexpr unsigned A = kFast ? 31 - __builtin_clz(kLowThreads / GC) : 0;  // log2(threads / G)
+  static_assert(!kFast || ((1u << KC) >= kLowThreads && KC >= A + 5), "fast low-pass layout");
+
+  // Calls f(smem offset, global offset) for every element of the bit-reversed order.
+  template <typename F>
+  __device__ __forceinline__ static void bitrev_order(unsigned K, unsigned G, unsigned hb, uint32_t g0, F&& f) {
+    if constexpr (kFast) {
+      const uint32_t t = threadIdx.x & (GC - 1), vlo = threadIdx.x >> (31 - __builtin_clz(GC));
+      const uint32_t s0 = t * group_stride(KC) + padx((vlo ? (__brev(vlo) >> (32 - A)) : 0u) << (KC - A));
+      const size_t g0v = ((size_t)vlo << hb) + g0 + t;
+      const size_t gstep = (size_t)1 << (A + hb);
+#pragma unroll
+      for (uint32_t k = 0; k < (1u << (KC - A)); ++k) f(s0 + cbitrev(k, KC - A), g0v + k * gstep);
+    } else {
+      const unsigned lg_g = 31 - __clz(G);
+      const uint32_t gstride = group_stride(K);
+#pragma unroll 8
+      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+        const uint32_t t = idx & (G - 1), v = idx >> lg_g;
+        f(t * gstride + padx(bitrev(v, K)), ((size_t)v << hb) + g0 + t);
+      }
+    }
+  }
+
+  // Calls f(smem offset, global offset) for every element of the contiguous order;
+  // gbase(t) gives group t's first global word.
+  template <typename B, typename F>
+  __device__ __forceinline__ static void contiguous_order(unsigned K, unsigned G, B&& gbase, F&& f) {
+    if constexpr (kFast) {
+      const uint32_t pt = padx(threadIdx.x);
+#pragma unroll
+      for (uint32_t t = 0; t < GC; ++t) {
+        const size_t gb = gbase(t) + threadIdx.x;
+#pragma unroll
+        for (uint32_t e = 0; e < (1u << KC); e += kLowThreads)
+          f(t * group_stride(KC) + pt + e + (e >> 5), gb + e);
+      }
+    } else {
+      const uint32_t gsz = 1u << K, gstride = group_stride(K);
+#pragma unroll 8
+      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+        const uint32_t t = idx >> K, e = idx & (gsz - 1);
+        f(t * gstride + padx(e), gbase(t) + e);
+      }
+    }
+  }
+};
+
 // The low pass of the inverse (INV) or forward transform over `iters` consecutive
 // batches of G groups of 2^K elements per CTA (blockIdx.y = column), double-buffered:
 // batch j + 1 is copied into shared memory while batch j is transformed and stored.
@@ -373,14 +450,17 @@ __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wai
 //   forward: layers [0, K) of a size-2^LG transform over contiguous groups, then the
 //            reference's final bit reversal on the store (natural-order evaluations).
 // Shared memory: two buffers of G padded groups, then two G-entry arrays of virtual
-// group bases.
-template <bool INV>
-__global__ void __launch_bounds__(256, 3) k_low(const uint32_t* __restrict__ src, size_t src_stride,
-                                             uint32_t* __restrict__ dst, size_t dst_stride, unsigned LG, unsigned K,
-                                             unsigned G, unsigned iters, const uint32_t* __restrict__ TW) {
+// group bases. KC, GC: the compile-time layout of LowIO (0, 0: K and G at run time).
+template <bool INV, unsigned KC = 0, unsigned GC = 0>
+__global__ void __launch_bounds__(kLowThreads, 3) k_low(const uint32_t* __restrict__ src, size_t src_stride,
+                                                     uint32_t* __restrict__ dst, size_t dst_stride, unsigned LG,
+                                                     unsigned K_, unsigned G_, unsigned iters,
+                                                     const uint32_t* __restrict__ TW) {
   extern __shared__ uint32_t sm[];
-  const uint32_t N = 1u << LG, gsz = 1u << K, gstride = group_stride(K);
-  const unsigned hb = LG - K, lg_g = 31 - __clz(G);
+  using IO = LowIO<KC, GC>;
+  const unsigned K = KC ? KC : K_, G = GC ? GC : G_;
+  const uint32_t N = 1u << LG, gstride = group_stride(K);
+  const unsigned hb = LG - K;
   // buffer b at sm + b * G * gstride, its group bases at sm + 2 * G * gstride + b * G
   auto buf = [&](int b) { return sm + (uint32_t)b * G * gstride; };
   auto vbs = [&](int b) { return sm + 2 * G * gstride + (uint32_t)b * G; };
@@ -393,17 +473,11 @@ __global__ void __launch_bounds__(256, 3) k_low(const uint32_t* __restrict__ src
     if (threadIdx.x < G) vbs(b)[threadIdx.x] = bitrev(g0 + threadIdx.x, hb) << K;
     uint32_t* s = buf(b);
     if (INV) {
-      #pragma unroll 8
-      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-        const uint32_t t = idx & (G - 1), v = idx >> lg_g;
-        cp_async4(s + t * gstride + padx(bitrev(v, K)), col + ((size_t)v << hb) + g0 + t);
-      }
+      IO::bitrev_order(K, G, hb, g0, [&](uint32_t so, size_t go) { cp_async4(s + so, col + go); });
     } else {
-      #pragma unroll 8
-      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-        const uint32_t t = idx >> K, e = idx & (gsz - 1);
-        cp_async4(s + t * gstride + padx(e), col + ((size_t)bitrev(g0 + t, hb) << K) + e);
-      }
+      IO::contiguous_order(
+          K, G, [&](uint32_t t) { return (size_t)bitrev(g0 + t, hb) << K; },
+          [&](uint32_t so, size_t go) { cp_async4(s + so, col + go); });
     }
     cp_async_commit();
   };
@@ -420,19 +494,15 @@ __global__ void __launch_bounds__(256, 3) k_low(const uint32_t* __restrict__ src
     uint32_t* s = buf(b);
     const uint32_t* vb = vbs(b);
     const uint32_t g0 = (batch0 + j) * G;
-    run_layers<INV>(s, gstride, G, K, 0, TW, N, vb);  // ends with a barrier
+    if constexpr (KC != 0)
+      run_layers_ct<INV, KC, 0>(s, s, gstride, G, 0, TW, N, vb);  // ends with a barrier
+    else
+      run_layers<INV>(s, gstride, G, K, 0, TW, N, vb);  // ends with a barrier
     if (INV) {
-      #pragma unroll 8
-      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-        const uint32_t t = idx >> K, e = idx & (gsz - 1);
-        out[vb[t] + e] = s[t * gstride + padx(e)];
-      }
+      IO::contiguous_order(
+          K, G, [&](uint32_t t) { return (size_t)vb[t]; }, [&](uint32_t so, size_t go) { out[go] = s[so]; });
     } else {
-      #pragma unroll 8
-      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-        const uint32_t t = idx & (G - 1), v = idx >> lg_g;
-        out[((size_t)v << hb) + g0 + t] = s[t * gstride + padx(bitrev(v, K))];
-      }
+      IO::bitrev_order(K, G, hb, g0, [&](uint32_t so, size_t go) { out[go] = s[so]; });
     }
     __syncthreads();  // buffer b is refilled by the next iteration's issue
   }
@@ -446,13 +516,50 @@ __global__ void __launch_bounds__(256, 3) k_low(const uint32_t* __restrict__ src
 //   mode FFT_ONLY:  load A-then-B coefficients interleaved, forward layers [K, L).
 enum MidMode : int { MID_LDE = 0, MID_IFFT_ONLY = 1, MID_FFT_ONLY = 2 };
 
-__global__ void __launch_bounds__(512, 2) k_mid(const uint32_t* __restrict__ in, size_t in_stride,
-                                             uint32_t* __restrict__ out, size_t out_stride, unsigned L, unsigned K,
-                                             unsigned B, unsigned G, const uint32_t* __restrict__ ITW_small,
-                                             const uint32_t* __restrict__ TW_big, int mode) {
+constexpr unsigned kMidThreads = 256;
+
+// Calls f(smem offset, global offset) for every element of k_mid's groups: element hi
+// of group t (the groups share the low K position bits lo0 + t) is global word
+// (hi << K) + lo0 + t. KC, MC, GC: 0, or K, M and G known at compile time with
+// kMidThreads / G = 2^A and A <= 5 <= M; then hi = hlo + (k << A) for a per-thread hlo,
+// padx(hi) = padx(hlo) + k (2^A + 2^A / 32) and every offset but the first is a constant.
+template <unsigned KC, unsigned MC, unsigned GC, typename F>
+__device__ __forceinline__ void mid_order(unsigned K, unsigned M, unsigned G, uint32_t lo0, F&& f) {
+  if constexpr (KC != 0) {
+    constexpr unsigned LG_G = 31 - __builtin_clz(GC), A = 31 - __builtin_clz(kMidThreads / GC);
+    static_assert(A <= 5 && MC >= A, "fast middle-pass layout");
+    const uint32_t t = threadIdx.x & (GC - 1), hlo = threadIdx.x >> LG_G;
+    const uint32_t s0 = t * group_stride(MC) + padx(hlo);
+    const size_t g0 = ((size_t)hlo << KC) + lo0 + t;
+#pragma unroll
+    for (uint32_t k = 0; k < (1u << (MC - A)); ++k)
+      f(s0 + k * ((1u << A) + (1u << A) / 32), g0 + ((size_t)k << (A + KC)));
+  } else {
+    const unsigned lg_g = 31 - __clz(G);
+    const uint32_t gstride = group_stride(M);
+#pragma unroll 8
+    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
+      f(t * gstride + padx(hi), ((size_t)hi << K) + lo0 + t);
+    }
+  }
+}
+
+// KC, MC, GC: the compile-time layout of mid_order (0, 0, 0: K, M and G at run time).
+// In the LDE mode with a compile-time layout, 1/n is applied by the last inverse chunk
+// and each quarter's first forward chunk reads the inverse result in s_in and writes
+// s_w, so s_in is neither rescaled nor copied in a pass of its own.
+template <unsigned KC = 0, unsigned MC = 0, unsigned GC = 0>
+__global__ void __launch_bounds__(kMidThreads, 3) k_mid(const uint32_t* __restrict__ in, size_t in_stride,
+                                                      uint32_t* __restrict__ out, size_t out_stride, unsigned L,
+                                                      unsigned K_, unsigned B, unsigned G_,
+                                                      const uint32_t* __restrict__ ITW_small,
+                                                      const uint32_t* __restrict__ TW_big, int mode) {
   extern __shared__ uint32_t sm[];
+  constexpr bool FAST = KC != 0;
+  const unsigned K = FAST ? KC : K_, G = FAST ? GC : G_;
   const unsigned M = L - K;
-  const uint32_t n = 1u << L, gsz = 1u << M, gstride = group_stride(M);
+  const uint32_t n = 1u << L, gstride = group_stride(M);
   uint32_t* s_in = sm;
   uint32_t* s_w = sm + G * gstride;
   uint32_t* vb = s_w + G * gstride;
@@ -464,32 +571,24 @@ __global__ void __launch_bounds__(512, 2) k_mid(const uint32_t* __restrict__ in,
   if (mode == MID_FFT_ONLY) {
     // interleaved position p holds A[p/2] (even p) or B[p/2] (odd p)
     #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
       const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
       const uint32_t p = (hi << K) | (lo0 + t);
       s_in[t * gstride + padx(hi)] = __ldg(src + ((p & 1) ? (n >> 1) + (p >> 1) : (p >> 1)));
     }
     __syncthreads();
     run_layers<false>(s_in, gstride, G, M, K, TW_big, n << B, vb);
-    #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
-      const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
-      dst[((size_t)hi << K) + lo0 + t] = s_in[t * gstride + padx(hi)];
-    }
+    mid_order<0, 0, 0>(K, M, G, lo0, [&](uint32_t so, size_t go) { dst[go] = s_in[so]; });
     return;
   }
-  #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
-    const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
-    s_in[t * gstride + padx(hi)] = __ldg(src + ((size_t)hi << K) + lo0 + t);
-  }
+  mid_order<KC, MC, GC>(K, M, G, lo0, [&](uint32_t so, size_t go) { s_in[so] = __ldg(src + go); });
   __syncthreads();
-  run_layers<true>(s_in, gstride, G, M, K, ITW_small, n, vb);
   // 1/n = 2^(31 - L) mod p: scaling is a rotation of the 31-bit word.
   const unsigned inv_n_shift = (31 - L) % 31;
   if (mode == MID_IFFT_ONLY) {
+    run_layers<true>(s_in, gstride, G, M, K, ITW_small, n, vb);
     #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
+    for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
       const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
       const uint32_t p = (hi << K) | (lo0 + t);
       const uint32_t v = mshl(s_in[t * gstride + padx(hi)], inv_n_shift);
@@ -497,23 +596,25 @@ __global__ void __launch_bounds__(512, 2) k_mid(const uint32_t* __restrict__ in,
     }
     return;
   }
-  #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
-    const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
-    const uint32_t a = t * gstride + padx(hi);
-    s_in[a] = mshl(s_in[a], inv_n_shift);
-  }
-  __syncthreads();
-  for (uint32_t q = 0; q < (1u << B); ++q) {
-    for (uint32_t idx = threadIdx.x; idx < G * gstride; idx += blockDim.x) s_w[idx] = s_in[idx];
-    if (threadIdx.x < G) vb[threadIdx.x] = q << M;
+  if constexpr (FAST) {
+    run_layers_ct<true, MC, 0, true>(s_in, s_in, gstride, G, K, ITW_small, n, vb, inv_n_shift);
+  } else {
+    run_layers<true>(s_in, gstride, G, M, K, ITW_small, n, vb);
+    mid_order<0, 0, 0>(K, M, G, lo0, [&](uint32_t so, size_t) { s_in[so] = mshl(s_in[so], inv_n_shift); });
     __syncthreads();
-    run_layers<false>(s_w, gstride, G, M, K, TW_big, n << B, vb);
-    #pragma unroll 8
-  for (uint32_t idx = threadIdx.x; idx < (G << M); idx += blockDim.x) {
-      const uint32_t t = idx & (G - 1), hi = idx >> lg_g;
-      dst[(size_t)q * n + ((size_t)hi << K) + lo0 + t] = s_w[t * gstride + padx(hi)];
+  }
+  for (uint32_t q = 0; q < (1u << B); ++q) {
+    if (threadIdx.x < G) vb[threadIdx.x] = q << M;
+    if constexpr (FAST) {
+      __syncthreads();
+      run_layers_ct<false, MC, 0>(s_in, s_w, gstride, G, K, TW_big, n << B, vb);
+    } else {
+      for (uint32_t idx = threadIdx.x; idx < G * gstride; idx += blockDim.x) s_w[idx] = s_in[idx];
+      __syncthreads();
+      run_layers<false>(s_w, gstride, G, M, K, TW_big, n << B, vb);
     }
+    uint32_t* dq = dst + (size_t)q * n;
+    mid_order<KC, MC, GC>(K, M, G, lo0, [&](uint32_t so, size_t go) { dq[go] = s_w[so]; });
     __syncthreads();
   }
 }
@@ -523,7 +624,6 @@ __global__ void __launch_bounds__(512, 2) k_mid(const uint32_t* __restrict__ in,
 // ---------------------------------------------------------------------------
 
 namespace {
-constexpr unsigned kThreads = 512;
 constexpr uint32_t kGroupWords = 16384;  // words of group data per shared buffer
 
 unsigned pick_split(unsigned L) {
@@ -547,7 +647,6 @@ void set_smem(const void* fn, size_t bytes) {
 // The low pass (k_low) over C columns of a size-2^LG transform split at K: batches of
 // G groups (at most kLowWords words each), `iters` batches per CTA.
 constexpr uint32_t kLowWords = 8192;
-constexpr unsigned kLowThreads = 256;
 template <bool INV>
 void launch_low(const uint32_t* src, size_t src_stride, uint32_t* dst, size_t dst_stride, uint32_t C, unsigned LG,
                 unsigned K, const uint32_t* tw, cudaStream_t st) {
@@ -557,8 +656,31 @@ void launch_low(const uint32_t* src, size_t src_stride, uint32_t* dst, size_t ds
   unsigned iters = 1;
   while (iters < 8 && batches % (iters * 2) == 0 && batches / (iters * 2) >= 16) iters *= 2;
   const size_t sb = ((size_t)2 * G * group_stride(K) + 2 * G) * sizeof(uint32_t);
-  set_smem((const void*)k_low<INV>, sb);
-  k_low<INV><<<dim3(batches / iters, C), kLowThreads, sb, st>>>(src, src_stride, dst, dst_stride, LG, K, G, iters, tw);
+  if (K == 10 && G == 8) {  // the 2^20 -> 2^22 LDE's groups: compile-time layout
+    set_smem((const void*)k_low<INV, 10, 8>, sb);
+    k_low<INV, 10, 8><<<dim3(batches / iters, C), kLowThreads, sb, st>>>(src, src_stride, dst, dst_stride, LG, K, G,
+                                                                         iters, tw);
+  } else {
+    set_smem((const void*)k_low<INV>, sb);
+    k_low<INV><<<dim3(batches / iters, C), kLowThreads, sb, st>>>(src, src_stride, dst, dst_stride, LG, K, G, iters,
+                                                                  tw);
+  }
+}
+// The middle pass (k_mid) over C columns of a size-2^L transform split at K.
+void launch_mid(const uint32_t* in, size_t in_stride, uint32_t* out, size_t out_stride, uint32_t C, unsigned L,
+                unsigned K, unsigned B, const uint32_t* itw, const uint32_t* tw, int mode, cudaStream_t st) {
+  const unsigned M = L - K;
+  const uint32_t ngroups = 1u << K;
+  const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
+  const size_t sb = smem_bytes(M, G, 2);
+  const dim3 grid(ngroups / G, C);
+  if (K == 10 && M == 10 && G == 8) {  // the 2^20 -> 2^22 LDE: compile-time layout
+    set_smem((const void*)k_mid<10, 10, 8>, sb);
+    k_mid<10, 10, 8><<<grid, kMidThreads, sb, st>>>(in, in_stride, out, out_stride, L, K, B, G, itw, tw, mode);
+  } else {
+    set_smem((const void*)k_mid<>, sb);
+    k_mid<><<<grid, kMidThreads, sb, st>>>(in, in_stride, out, out_stride, L, K, B, G, itw, tw, mode);
+  }
 }
 }  // namespace
 
@@ -576,48 +698,26 @@ void circle_lde(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, size_t 
   uint32_t* tmp = scratch;
   uint32_t* mid = scratch + (size_t)C * n;
   launch_low<true>(d_in, in_stride, tmp, n, C, L, K, small.itw, st);
-  {
-    const unsigned M = L - K;
-    const uint32_t ngroups = 1u << K;
-    const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
-    const size_t sb = smem_bytes(M, G, 2);
-    set_smem((const void*)k_mid, sb);
-    k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(tmp, n, mid, (size_t)n << B, L, K, B, G, small.itw, big.tw,
-                                                      MID_LDE);
-  }
+  launch_mid(tmp, n, mid, (size_t)n << B, C, L, K, B, small.itw, big.tw, MID_LDE, st);
   launch_low<false>(mid, (size_t)n << B, d_out, out_stride, C, L + B, K, big.tw, st);
   ZS_CUDA(cudaGetLastError());
 }
 
 void circle_fft(const uint32_t* d_coeffs, uint32_t* d_evals, uint32_t C, const CircleDomain& dom, uint32_t* scratch,
                 cudaStream_t st) {
-  const unsigned L = dom.lg, K = pick_split(L), M = L - K;
+  const unsigned L = dom.lg, K = pick_split(L);
   const uint32_t n = 1u << L;
-  {
-    const uint32_t ngroups = 1u << K;
-    const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
-    const size_t sb = smem_bytes(M, G, 2);
-    set_smem((const void*)k_mid, sb);
-    k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(d_coeffs, n, scratch, n, L, K, 0, G, dom.itw, dom.tw,
-                                                      MID_FFT_ONLY);
-  }
+  launch_mid(d_coeffs, n, scratch, n, C, L, K, 0, dom.itw, dom.tw, MID_FFT_ONLY, st);
   launch_low<false>(scratch, n, d_evals, n, C, L, K, dom.tw, st);
   ZS_CUDA(cudaGetLastError());
 }
 
 void circle_ifft(const uint32_t* d_evals, uint32_t* d_coeffs, uint32_t C, const CircleDomain& dom, uint32_t* scratch,
                  cudaStream_t st) {
-  const unsigned L = dom.lg, K = pick_split(L), M = L - K;
+  const unsigned L = dom.lg, K = pick_split(L);
   const uint32_t n = 1u << L;
   launch_low<true>(d_evals, n, scratch, n, C, L, K, dom.itw, st);
-  {
-    const uint32_t ngroups = 1u << K;
-    const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
-    const size_t sb = smem_bytes(M, G, 2);
-    set_smem((const void*)k_mid, sb);
-    k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(scratch, n, d_coeffs, n, L, K, 0, G, dom.itw, dom.tw,
-                                                      MID_IFFT_ONLY);
-  }
+  launch_mid(scratch, n, d_coeffs, n, C, L, K, 0, dom.itw, dom.tw, MID_IFFT_ONLY, st);
   ZS_CUDA(cudaGetLastError());
 }
 
@@ -652,15 +752,7 @@ void circle_lde_tables(const uint32_t* d_in, size_t in_stride, uint32_t* d_out, 
   uint32_t* tmp = scratch;
   uint32_t* mid = scratch + (size_t)C * n;
   launch_low<true>(d_in, in_stride, tmp, n, C, L, K, itw_small, st);
-  {
-    const unsigned M = L - K;
-    const uint32_t ngroups = 1u << K;
-    const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
-    const size_t sb = smem_bytes(M, G, 2);
-    set_smem((const void*)k_mid, sb);
-    k_mid<<<dim3(ngroups / G, C), kThreads, sb, st>>>(tmp, n, mid, (size_t)n << B, L, K, B, G, itw_small, tw_big,
-                                                      MID_LDE);
-  }
+  launch_mid(tmp, n, mid, (size_t)n << B, C, L, K, B, itw_small, tw_big, MID_LDE, st);
   launch_low<false>(mid, (size_t)n << B, d_out, out_stride, C, L + B, K, tw_big, st);
   ZS_CUDA(cudaGetLastError());
 }
