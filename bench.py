@@ -45,6 +45,9 @@ def parse():
                          "stacked Rescue 2^18); batch: mixed-size proof batch, batched vs one at a time; "
                          "serve: Poisson request stream, p50/p99 latency")
     ap.add_argument("--jobs", type=int, default=512, help="batch: number of traces")
+    ap.add_argument("--batch-arm", default="both", choices=["both", "plain"],
+                    help="batch: 'plain' runs only the one-at-a-time arm and reports each shape's time "
+                         "(for profiling the proofs one by one)")
     ap.add_argument("--log-min", type=int, default=None)
     ap.add_argument("--log-max", type=int, default=None)
     ap.add_argument("--concurrency", type=int, default=8, help="batch / serve: prover workers")
@@ -313,6 +316,21 @@ def run_batch(args, world, rank, local):
 
     def plain():
         return [native.prove(**k) for k in kw]
+
+    if args.batch_arm == "plain":
+        ref = plain()
+        per_shape = {}
+        for _ in range(args.steps):
+            for k, (air, params, *_rest) in zip(kw, jobs):
+                t0 = time.perf_counter()
+                native.prove(**k)
+                per_shape.setdefault(f"{air}:{params[0]}", []).append(time.perf_counter() - t0)
+        if rank == 0:
+            print(json.dumps({"workload": "batch", "arm": "plain", "jobs": args.jobs, "steps": args.steps,
+                              "plain_s_per_pass": sum(sum(v) for v in per_shape.values()) / args.steps,
+                              "per_shape_ms": {k: {"count": len(v) // args.steps, "ms_median": 1e3 * sorted(v)[len(v) // 2]}
+                                               for k, v in sorted(per_shape.items())}}), flush=True)
+        return
 
     ref = batched()  # grows the device pool to the batch's working set
     assert all(isinstance(p, bytes) for p in ref), "a batch job failed"
