@@ -1,8 +1,8 @@
 #!/usr/bin/env bash
 # ORACLE — test and benchmark infrastructure only. Compiles the reference's own GPU
-# circle FFT kernels from their source in the reference tree, for sm_100a, and the
-# host driver that calls them the way src/cuda/circlefft_gpu.zig does, into
-# oracle/_ref/ (git-ignored; the built files travel with the repository to the GPU
+# circle FFT and sum-check kernels from their source in the reference tree, for sm_100a,
+# and the host drivers that call them the way src/cuda/circlefft_gpu.zig and
+# src/cuda/sumcheck_gpu.zig do, into oracle/_ref/ (git-ignored; the built files travel with the repository to the GPU
 # host, which has no reference tree). Nothing is copied out of the reference tree.
 #   REF: the reference checkout (default /root/reference)
 set -euo pipefail
@@ -25,4 +25,16 @@ if [ ! "$OUT/libref_circlefft.so" -nt "$HERE/ref_circlefft_driver.cpp" ] || \
    [ ! "$OUT/libref_circlefft.so" -nt "$HERE/circle.hpp" ]; then
   "$CXX" -O2 -std=c++17 -fPIC -shared -I"$HERE" -I"$CUDA_HOME/include" \
     -o "$OUT/libref_circlefft.so" "$HERE/ref_circlefft_driver.cpp" -L"$CUDA_HOME/lib64/stubs" -lcuda
+fi
+
+SC_SRC="$REF/src/cuda/kernels/sumcheck.cu"
+if [ -f "$SC_SRC" ]; then
+  if [ ! "$OUT/sumcheck.cubin" -nt "$SC_SRC" ]; then
+    "$NVCC" -gencode arch=compute_100a,code=sm_100a -O3 -cubin -I"$REF/src/cuda/kernels" \
+      -o "$OUT/sumcheck.cubin" "$SC_SRC"
+  fi
+  if [ ! "$OUT/libref_sumcheck.so" -nt "$HERE/ref_sumcheck_driver.cpp" ]; then
+    "$CXX" -O2 -std=c++17 -fPIC -shared -I"$CUDA_HOME/include" \
+      -o "$OUT/libref_sumcheck.so" "$HERE/ref_sumcheck_driver.cpp" -L"$CUDA_HOME/lib64/stubs" -lcuda
+  fi
 fi

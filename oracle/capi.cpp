@@ -7,6 +7,7 @@
 #include <exception>
 #include <vector>
 
+#include "binius.hpp"
 #include "pipeline.hpp"
 #include "stark.hpp"
 
@@ -309,6 +310,138 @@ int orc_commit_columns(const uint8_t* cols, size_t cols_len, unsigned trace_log,
 }
 
 // Re-serializes a proof after a round trip through the wire reader.
+// Binius tower multiply at `level` (1..7) of two little-endian u128 values (2 x u64).
+void orc_tower_mul(unsigned level, const uint64_t* a, const uint64_t* b, uint64_t* out) {
+  const u128 x = ((u128)a[1] << 64) | a[0], y = ((u128)b[1] << 64) | b[0];
+  const u128 r = towerMul(level, x & towerMask(level), y & towerMask(level));
+  out[0] = (uint64_t)r;
+  out[1] = (uint64_t)(r >> 64);
+}
+
+// One sum-check round's values[t] in the flattened form of the accelerator hook
+// (src/binius/accel.zig:9-26, 43-47): level 3 (Gf256, one byte per element) or level 7
+// (Gf2_128, 16 little-endian bytes per element). Returns 0, or -2 on malformed input.
+int orc_binius_values(unsigned level, const uint8_t* cur_flat, size_t len, size_t m, const uint8_t* coeffs,
+                      size_t nterms, const uint32_t* indices, size_t n_indices, const uint32_t* offsets,
+                      size_t dmax, size_t half, uint8_t* out) {
+  if (level != 3 && level != 7) return -2;
+  const size_t es = level == 3 ? 1 : 16;
+  if (2 * half > len || offsets[0] != 0 || offsets[nterms] != n_indices) return -2;
+  auto get = [&](const uint8_t* p) {
+    u128 v = 0;
+    for (size_t k = 0; k < es; ++k) v |= (u128)p[k] << (8 * k);
+    return v;
+  };
+  std::vector<std::vector<u128>> cur(m, std::vector<u128>(len));
+  for (size_t f = 0; f < m; ++f)
+    for (size_t i = 0; i < len; ++i) cur[f][i] = get(cur_flat + (f * len + i) * es);
+  std::vector<u128> cf(nterms);
+  for (size_t k = 0; k < nterms; ++k) cf[k] = get(coeffs + k * es);
+  for (size_t j = 0; j < n_indices; ++j)
+    if (indices[j] >= m) return -2;
+  const std::vector<uint32_t> idx(indices, indices + n_indices), off(offsets, offsets + nterms + 1);
+  const std::vector<u128> v = sumcheckRoundValues(level, cur, cf, idx, off, dmax, half);
+  for (size_t t = 0; t <= dmax; ++t)
+    for (size_t k = 0; k < es; ++k) out[t * es + k] = (uint8_t)(v[t] >> (8 * k));
+  return 0;
+}
+
+// SHA-256 of msg (the transcript hash of src/binius/sumcheck.zig:47-87).
+void orc_sha256(const uint8_t* msg, size_t n, uint8_t* out) {
+  const auto h = sha256(msg, n);
+  std::memcpy(out, h.data(), 32);
+}
+
+namespace {
+bool binius_inputs(unsigned level, const uint8_t* tables, size_t len, size_t m, const uint8_t* coeffs, size_t nterms,
+                   const uint32_t* indices, size_t n_indices, const uint32_t* offsets,
+                   std::vector<std::vector<u128>>& cur, SumcheckTerms& tm) {
+  if (level != 3 && level != 7) return false;
+  if (offsets[0] != 0 || offsets[nterms] != n_indices) return false;
+  for (size_t j = 0; j < n_indices; ++j)
+    if (indices[j] >= m) return false;
+  const size_t es = towerSize(level);
+  cur.assign(m, std::vector<u128>(len));
+  for (size_t f = 0; f < m; ++f)
+    for (size_t i = 0; i < len; ++i) cur[f][i] = towerFromBytes(level, tables + (f * len + i) * es);
+  tm.coeffs.resize(nterms);
+  for (size_t k = 0; k < nterms; ++k) tm.coeffs[k] = towerFromBytes(level, coeffs + k * es);
+  tm.indices.assign(indices, indices + n_indices);
+  tm.offsets.assign(offsets, offsets + nterms + 1);
+  return true;
+}
+}  // namespace
+
+// Sumcheck(F).proveCombination (proveSeeded's transcript when has_seed): claimed_out one
+// element, rounds_out k * (dmax + 1) elements.
+int orc_binius_prove(unsigned level, const uint8_t* tables, size_t k, size_t m, const uint8_t* coeffs, size_t nterms,
+                     const uint32_t* indices, size_t n_indices, const uint32_t* offsets, const uint8_t* seed,
+                     size_t seed_len, int has_seed, uint8_t* claimed_out, uint8_t* rounds_out) {
+  std::vector<std::vector<u128>> cur;
+  SumcheckTerms tm;
+  if (!binius_inputs(level, tables, (size_t)1 << k, m, coeffs, nterms, indices, n_indices, offsets, cur, tm)) return -2;
+  const std::vector<uint8_t> sd(seed, seed + (has_seed ? seed_len : 0));
+  const SumcheckProof pf = proveCombination(level, k, cur, tm, has_seed ? &sd : nullptr);
+  const size_t es = towerSize(level), d1 = tm.dmax() + 1;
+  towerToBytes(level, pf.claimed, claimed_out);
+  for (size_t i = 0; i < k; ++i)
+    for (size_t t = 0; t < d1; ++t) towerToBytes(level, pf.rounds[i][t], rounds_out + (i * d1 + t) * es);
+  return 0;
+}
+
+// 1 when the proof replays and ends at g(challenges), 0 when not, -2 for bad inputs.
+int orc_binius_verify(unsigned level, const uint8_t* tables, size_t k, size_t m, const uint8_t* coeffs, size_t nterms,
+                      const uint32_t* indices, size_t n_indices, const uint32_t* offsets, const uint8_t* seed,
+                      size_t seed_len, int has_seed, const uint8_t* claimed, const uint8_t* rounds) {
+  std::vector<std::vector<u128>> cur;
+  SumcheckTerms tm;
+  if (!binius_inputs(level, tables, (size_t)1 << k, m, coeffs, nterms, indices, n_indices, offsets, cur, tm)) return -2;
+  const size_t es = towerSize(level), d1 = tm.dmax() + 1;
+  SumcheckProof pf{towerFromBytes(level, claimed), std::vector<std::vector<u128>>(k, std::vector<u128>(d1))};
+  for (size_t i = 0; i < k; ++i)
+    for (size_t t = 0; t < d1; ++t) pf.rounds[i][t] = towerFromBytes(level, rounds + (i * d1 + t) * es);
+  const std::vector<uint8_t> sd(seed, seed + (has_seed ? seed_len : 0));
+  return verifyCombination(level, k, cur, tm, pf, has_seed ? &sd : nullptr) ? 1 : 0;
+}
+
+// The fold of m tables of len elements at r into m tables of len / 2 (next).
+int orc_binius_fold(unsigned level, const uint8_t* tables, size_t len, size_t m, const uint8_t* r, uint8_t* next) {
+  if (level != 3 && level != 7) return -2;
+  const size_t es = towerSize(level);
+  std::vector<std::vector<u128>> cur(m, std::vector<u128>(len));
+  for (size_t f = 0; f < m; ++f)
+    for (size_t i = 0; i < len; ++i) cur[f][i] = towerFromBytes(level, tables + (f * len + i) * es);
+  foldTables(level, cur, len, towerFromBytes(level, r));
+  for (size_t f = 0; f < m; ++f)
+    for (size_t i = 0; i < len / 2; ++i) towerToBytes(level, cur[f][i], next + (f * (len / 2) + i) * es);
+  return 0;
+}
+
+// A transcript seeded with `seed` absorbing one-element coefficient lists in turn
+// (sumcheck.zig:697-713): out[i] = the challenge after absorbing element i.
+int orc_binius_challenges(unsigned level, const uint8_t* seed, size_t seed_len, const uint8_t* elems, size_t n,
+                          uint8_t* out) {
+  if (level != 3 && level != 7) return -2;
+  const size_t es = towerSize(level);
+  SumcheckTranscript tr = SumcheckTranscript::initBytes(level, std::vector<uint8_t>(seed, seed + seed_len));
+  for (size_t i = 0; i < n; ++i) towerToBytes(level, tr.absorb({towerFromBytes(level, elems + i * es)}), out + i * es);
+  return 0;
+}
+
+// interpolateCoeffs through the points 0..n-1 (n <= 64).
+int orc_binius_interpolate(unsigned level, const uint8_t* values, size_t n, uint8_t* coeffs_out) {
+  if ((level != 3 && level != 7) || n == 0 || n > 64) return -2;
+  const size_t es = towerSize(level);
+  std::vector<u128> pts(n), vals(n);
+  for (size_t i = 0; i < n; ++i) {
+    pts[i] = (u128)i;
+    vals[i] = towerFromBytes(level, values + i * es);
+  }
+  const std::vector<u128> cs = interpolateCoeffs(level, pts, vals);
+  for (size_t i = 0; i < n; ++i) towerToBytes(level, cs[i], coeffs_out + i * es);
+  return 0;
+}
+
 // serialization.zig:220-250 "golden wire layout is stable": the struct
 // {name: [3]u8 = "abc", count: u32 = 0x01020304, rows: []u16 = {0x0102, 0x0304},
 // flag: bool = true, maybe: ?[2]u8 = {0xde, 0xad}} through the oracle's Writer.

@@ -45,6 +45,16 @@ def lib():
         L.orc_circle_eval_at.argtypes = [u32p, ctypes.c_uint, ctypes.c_uint32, ctypes.c_uint32]
         L.orc_circle_eval_at.restype = ctypes.c_uint32
         L.orc_wire_golden.restype = ctypes.c_size_t
+        L.orc_binius_values.argtypes = [ctypes.c_uint, ctypes.c_char_p, ctypes.c_size_t, ctypes.c_size_t,
+                                        ctypes.c_char_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t,
+                                        ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_char_p]
+        vp, sz, cp = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_char_p
+        L.orc_sha256.argtypes = [cp, sz, cp]
+        L.orc_binius_prove.argtypes = [ctypes.c_uint, cp, sz, sz, cp, sz, vp, sz, vp, cp, sz, ctypes.c_int, cp, cp]
+        L.orc_binius_verify.argtypes = [ctypes.c_uint, cp, sz, sz, cp, sz, vp, sz, vp, cp, sz, ctypes.c_int, cp, cp]
+        L.orc_binius_fold.argtypes = [ctypes.c_uint, cp, sz, sz, cp, cp]
+        L.orc_binius_interpolate.argtypes = [ctypes.c_uint, cp, sz, cp]
+        L.orc_binius_challenges.argtypes = [ctypes.c_uint, cp, sz, cp, sz, cp]
         L.orc_circle_twiddles.argtypes = [ctypes.c_uint, u32p]
         L.orc_merkle_root.argtypes = [ctypes.c_char_p, ctypes.c_size_t, u8p]
         L.orc_interpolate_subgroup.argtypes = [u32p, ctypes.c_uint, ctypes.c_int, u32p]
@@ -307,3 +317,105 @@ def commit_columns(columns: bytes, n_columns, trace_log, log_blowup):
     if rc != 0:
         raise RuntimeError(f"orc_commit_columns failed: {rc}")
     return [bytes(out)[32 * j:32 * j + 32] for j in range(n_columns)]
+
+
+def tower_mul(level, a, b):
+    """Binius tower multiply (src/binius/tower.zig mulRec) of two ints < 2^(2^level)."""
+    au = (ctypes.c_uint64 * 2)(a & (2**64 - 1), a >> 64)
+    bu = (ctypes.c_uint64 * 2)(b & (2**64 - 1), b >> 64)
+    out = (ctypes.c_uint64 * 2)()
+    lib().orc_tower_mul(level, au, bu, out)
+    return out[0] | (out[1] << 64)
+
+
+def binius_values(level, cur_flat: bytes, length, m, coeffs: bytes, indices, offsets, dmax, half):
+    """One sum-check round's values[t] (src/binius/sumcheck.zig:357-372) in the accelerator
+    hook's byte form (level 3: Gf256 bytes, level 7: Gf2_128 16-byte values)."""
+    es = 1 if level == 3 else 16
+    idx = np.ascontiguousarray(indices, dtype=np.uint32)
+    off = np.ascontiguousarray(offsets, dtype=np.uint32)
+    out = ctypes.create_string_buffer((dmax + 1) * es)
+    rc = lib().orc_binius_values(level, cur_flat, length, m, coeffs, len(coeffs) // es, idx.ctypes.data,
+                                 idx.size, off.ctypes.data, dmax, half, out)
+    if rc != 0:
+        raise RuntimeError(f"orc_binius_values failed: {rc}")
+    return out.raw
+
+
+def sha256(msg: bytes) -> bytes:
+    """The oracle's SHA-256 (FIPS 180-4), the sum-check transcript hash."""
+    out = ctypes.create_string_buffer(32)
+    lib().orc_sha256(bytes(msg), len(msg), out)
+    return out.raw
+
+
+def _terms(terms, es):
+    """[(indices, coeff int)] -> (coeff bytes, indices array, offsets array)."""
+    coeffs = b"".join(int(c).to_bytes(es, "little") for _, c in terms)
+    idx = np.array([f for fs, _ in terms for f in fs], dtype=np.uint32)
+    off = np.zeros(len(terms) + 1, dtype=np.uint32)
+    off[1:] = np.cumsum([len(fs) for fs, _ in terms])
+    return coeffs, idx, off
+
+
+def binius_prove(level, tables: bytes, k, m, terms, seed=None):
+    """Sumcheck(F).proveCombination (proveSeeded's transcript when seed is bytes) over
+    TowerField(level), level 3 or 7: tables = m tables of 2^k elements, little-endian.
+    Returns (claimed bytes, rounds bytes: k * (dmax + 1) elements)."""
+    es = 1 if level == 3 else 16
+    coeffs, idx, off = _terms(terms, es)
+    dmax = max(len(fs) for fs, _ in terms)
+    claimed = ctypes.create_string_buffer(es)
+    rounds = ctypes.create_string_buffer(max(1, k * (dmax + 1) * es))
+    sd = b"" if seed is None else bytes(seed)
+    rc = lib().orc_binius_prove(level, bytes(tables), k, m, coeffs, len(terms), idx.ctypes.data, idx.size,
+                                off.ctypes.data, sd, len(sd), int(seed is not None), claimed, rounds)
+    if rc != 0:
+        raise RuntimeError(f"orc_binius_prove failed: {rc}")
+    return claimed.raw, rounds.raw[:k * (dmax + 1) * es]
+
+
+def binius_verify(level, tables: bytes, k, m, terms, claimed: bytes, rounds: bytes, seed=None):
+    """True when the proof's rounds replay and end at g(challenges) (sumcheck.zig:632-665)."""
+    es = 1 if level == 3 else 16
+    coeffs, idx, off = _terms(terms, es)
+    sd = b"" if seed is None else bytes(seed)
+    rc = lib().orc_binius_verify(level, bytes(tables), k, m, coeffs, len(terms), idx.ctypes.data, idx.size,
+                                 off.ctypes.data, sd, len(sd), int(seed is not None), bytes(claimed),
+                                 bytes(rounds) or b"\0")
+    if rc < 0:
+        raise RuntimeError(f"orc_binius_verify failed: {rc}")
+    return rc == 1
+
+
+def binius_fold(level, tables: bytes, length, m, r: int):
+    """m tables of `length` elements folded at r into m tables of length // 2."""
+    es = 1 if level == 3 else 16
+    out = ctypes.create_string_buffer(max(1, m * (length // 2) * es))
+    rc = lib().orc_binius_fold(level, bytes(tables), length, m, int(r).to_bytes(es, "little"), out)
+    if rc != 0:
+        raise RuntimeError(f"orc_binius_fold failed: {rc}")
+    return out.raw[:m * (length // 2) * es]
+
+
+def binius_interpolate(level, values):
+    """Low-first coefficients of the polynomial through (t, values[t]), t = 0..n-1."""
+    es = 1 if level == 3 else 16
+    out = ctypes.create_string_buffer(len(values) * es)
+    rc = lib().orc_binius_interpolate(level, b"".join(int(v).to_bytes(es, "little") for v in values),
+                                      len(values), out)
+    if rc != 0:
+        raise RuntimeError(f"orc_binius_interpolate failed: {rc}")
+    return [int.from_bytes(out.raw[i * es:(i + 1) * es], "little") for i in range(len(values))]
+
+
+def binius_challenges(level, seed: bytes, elems):
+    """Transcript.initBytes(seed), then absorb([e]) for each e: the challenges."""
+    es = 1 if level == 3 else 16
+    out = ctypes.create_string_buffer(max(1, len(elems) * es))
+    rc = lib().orc_binius_challenges(level, bytes(seed), len(seed),
+                                     b"".join(int(e).to_bytes(es, "little") for e in elems) or b"\0",
+                                     len(elems), out)
+    if rc != 0:
+        raise RuntimeError(f"orc_binius_challenges failed: {rc}")
+    return [int.from_bytes(out.raw[i * es:(i + 1) * es], "little") for i in range(len(elems))]

@@ -74,3 +74,50 @@ def fft(coeffs):
 def ifft(evals):
     """circleIFFT of one column. Returns (coeffs, wall ms, device ms)."""
     return _call(lib().ref_cfft_ifft, evals)
+
+
+# ---- the reference's GPU sum-check round kernels (src/cuda/kernels/sumcheck.cu) ----------
+
+SC_LIB = os.path.join(REF_DIR, "libref_sumcheck.so")
+SC_CUBIN = os.path.join(REF_DIR, "sumcheck.cubin")
+_sc_lib = None
+
+
+def sumcheck_available():
+    return os.path.exists(SC_LIB) and os.path.exists(SC_CUBIN)
+
+
+def sumcheck_lib():
+    global _sc_lib
+    if _sc_lib is None:
+        if not sumcheck_available():
+            raise RuntimeError("the reference GPU sum-check kernels are not built (oracle/build_ref.sh)")
+        L = ctypes.CDLL(SC_LIB)
+        L.ref_sc_init.argtypes = [ctypes.c_char_p]
+        L.ref_sc_init.restype = ctypes.c_int
+        sz = ctypes.c_size_t
+        L.ref_sc_values.argtypes = [ctypes.c_int, ctypes.c_char_p, sz, sz, ctypes.c_char_p, sz, ctypes.c_void_p, sz,
+                                    ctypes.c_void_p, sz, sz, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+        L.ref_sc_values.restype = ctypes.c_int
+        rc = L.ref_sc_init(SC_CUBIN.encode())
+        if rc != 0:
+            raise RuntimeError(f"ref_sc_init failed: {rc}")
+        _sc_lib = L
+    return _sc_lib
+
+
+def sumcheck_values(wide, cur_flat: bytes, length, m, coeffs: bytes, indices, offsets, dmax, half):
+    """One round through the reference's own kernel, driven as src/cuda/sumcheck_gpu.zig
+    drives it (buffers allocated and copied per call). Returns (values bytes, wall ms of
+    the call, device ms of the launch)."""
+    es = 16 if wide else 1
+    idx = np.ascontiguousarray(indices, dtype=np.uint32)
+    off = np.ascontiguousarray(offsets, dtype=np.uint32)
+    out = ctypes.create_string_buffer((dmax + 1) * es)
+    t = (ctypes.c_double * 2)()
+    rc = sumcheck_lib().ref_sc_values(int(bool(wide)), bytes(cur_flat), length, m, bytes(coeffs),
+                                      len(coeffs) // es, idx.ctypes.data, idx.size, off.ctypes.data, dmax, half,
+                                      out, t)
+    if rc != 0:
+        raise RuntimeError(f"reference GPU sum-check round failed: {rc}")
+    return out.raw, t[0], t[1]

@@ -71,3 +71,25 @@ def test_context_entry_points_check_arguments_first():
     assert L.zs_m31_prove_ctx(None, *args, ctypes.byref(out), ctypes.byref(n)) == -2
     L.zs_m31_ctx_destroy(None)
     assert L.zs_m31_ctx_device(None) == -2
+
+
+def test_binius_entry_points_reject_malformed_arguments_first():
+    """The sum-check entry points check their arguments before any device work and
+    return -2 (so this runs without a GPU)."""
+    from zs_b200 import native
+    cur = bytes(16)
+    bad_calls = [
+        lambda: native.binius_gf256_values(cur, 8, 2, b"\x01", [0, 2], [0, 2], 2, 4),      # index >= m
+        lambda: native.binius_gf256_values(cur, 8, 2, b"\x01", [0, 1], [0, 2], 2, 5),      # 2 half > len
+        lambda: native.binius_gf256_values(cur, 8, 2, b"\x01", [0, 1], [0, 2], 256, 4),    # 257 points
+        lambda: native.binius_gf256_values(cur, 8, 2, b"\x01\x01", [0, 1], [0, 2, 1], 2, 4),  # offsets decrease
+        lambda: native.binius_gf256_values(cur, 8, 2, b"\x01", [0] * 1025, [0, 1025], 1025, 4),  # > 1024 factors
+        lambda: native.binius_gf256_values(cur, 8, 2, b"\x01" * 257, [], [0] * 258, 0, 4),  # > 256 terms
+        lambda: native.binius_prove_combination(8, cur, 3, 2, [([0] * 64, 1)]),             # 65 points
+        lambda: native.binius_prove_combination(16, cur, 3, 2, [([0], 1)]),                 # field_bits
+        lambda: native.binius_fold_device(128, 0, 8, 2, 3, 0),                               # null buffers
+    ]
+    for call in bad_calls:
+        with pytest.raises(native.ZsError) as e:
+            call()
+        assert e.value.code == -2

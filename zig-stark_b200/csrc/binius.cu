@@ -1,0 +1,839 @@
+// The Binius sum-check on the device: the values[t] hook of src/binius/accel.zig:9-47
+// (computed in src/binius/sumcheck.zig:357-372, GPU-ported by src/cuda/kernels/sumcheck.cu
+// and src/cuda/sumcheck_gpu.zig:36-151), the table fold of sumcheck.zig:379-388, and the
+// combination prover of sumcheck.zig:208-395 with its tables resident in device memory.
+//
+//   values[t] = sum_{rest < half} sum_terms coeff * prod_{f in term} (a_f + t (a_f + b_f)),
+//   a_f = cur[f][2 rest], b_f = cur[f][2 rest + 1], t = 0..dmax, in the tower field
+//   TowerField(3) = GF(2^8) or TowerField(7) = GF(2^128) (src/binius/tower.zig), where
+//   addition is XOR.
+//
+// Tower arithmetic. The product of two GF(2^8) elements comes from a 64 KB table held in
+// each CTA's shared memory, built once per device by the Karatsuba recursion that defines
+// the tower (tower.zig:192-212). Above GF(2^8) a product at level L is three products at
+// level L - 1 and one product by the level's constant beta = X_(L-2), the adjoined root of
+// level L - 1: for c = c0 + c1 X_(L-2), c X_(L-2) = c1 + (c0 + c1 beta') X_(L-2), so it
+// costs one table lookup at any level. A GF(2^128) product is 81 + 40 lookups. The points
+// t < 256 lie in the GF(2^8) subfield, and a subfield scalar multiplies the 16 byte
+// coordinates of a GF(2^128) element independently (the tower is a GF(2^8)-vector space
+// on the monomials of X_3..X_6); t = 0 and t = 1 need no product at all (a and b).
+//
+// The round's term list (at most 256 terms and 1024 factor indices) travels as the
+// kernel's parameter (7.2 KB, within the 32 KB parameter space of sm_70 and later), so a
+// round needs no device copy of it.
+//
+// Reduction. Each thread accumulates its rows for every point in registers (up to eight
+// points; beyond that one point per pass), a warp XOR-reduces with shuffles, each warp
+// XORs its result into shared memory, and each CTA XORs its values into the output words:
+// one atomic per CTA and word, where the reference kernel takes one per thread.
+//
+// Fold. next[f][rest] = a + r (a + b). Over GF(2^8) the product by r is one lookup in row r
+// of the table. Over GF(2^128) the product by a fixed r is GF(2^8)-linear in the 16 byte
+// coordinates of (a + b): a 16 x 256 table of r * (v X^byte k), built once per fold, turns
+// it into 16 lookups of 16 bytes.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "../../include/zs_binius.h"
+#include "common.cuh"
+
+namespace zs {
+namespace {
+
+using u128 = unsigned __int128;
+
+constexpr unsigned kBThreads = 256;
+constexpr uint32_t kMaxTerms = 256, kMaxFactors = 1024, kMaxPoint = 255, kMaxTables = 65535;
+constexpr uint32_t kProveMaxPoints = 64;  // sumcheck.zig:243 (dmax + 1 <= 64)
+constexpr int kRegPoints = 8;             // dmax < kRegPoints: every point in registers
+
+// ---- host: tower arithmetic ------------------------------------------------------
+
+uint32_t tower_mul_small(unsigned level, uint32_t a, uint32_t b) {  // level <= 3
+  if (level == 0) return a & b & 1u;
+  const unsigned half = 1u << (level - 1);
+  const uint32_t mask = (1u << half) - 1;
+  const uint32_t a0 = a & mask, a1 = (a >> half) & mask, b0 = b & mask, b1 = (b >> half) & mask;
+  const uint32_t c0 = tower_mul_small(level - 1, a0, b0), c1 = tower_mul_small(level - 1, a1, b1);
+  const uint32_t c2 = tower_mul_small(level - 1, a0 ^ a1, b0 ^ b1);
+  const uint32_t beta = level == 1 ? 1u : 1u << (1u << (level - 2));
+  return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ tower_mul_small(level - 1, c1, beta)) << half);
+}
+
+// Levels 3..7 over the GF(2^8) product table; inverses by the norm to the subfield:
+// for a = a0 + a1 y with y^2 = beta y + 1, a (a0 + a1 beta + a1 y) = a0^2 + a0 a1 beta + a1^2.
+struct HostTower {
+  std::vector<uint8_t> T, I;
+  HostTower() : T(65536), I(256, 0) {
+    for (uint32_t a = 0; a < 256; ++a)
+      for (uint32_t b = 0; b < 256; ++b) {
+        T[(a << 8) | b] = (uint8_t)tower_mul_small(3, a, b);
+        if (T[(a << 8) | b] == 1) I[a] = (uint8_t)b;
+      }
+  }
+  static u128 beta(unsigned level) { return (u128)1 << (1u << (level - 2)); }
+  u128 mul(unsigned level, u128 a, u128 b) const {
+    if (level == 3) return T[((uint32_t)a << 8) | (uint32_t)b];
+    const unsigned half = 1u << (level - 1);
+    const u128 mask = ((u128)1 << half) - 1;
+    const u128 a0 = a & mask, a1 = a >> half, b0 = b & mask, b1 = b >> half;
+    const u128 c0 = mul(level - 1, a0, b0), c1 = mul(level - 1, a1, b1), c2 = mul(level - 1, a0 ^ a1, b0 ^ b1);
+    return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ mul(level - 1, c1, beta(level))) << half);
+  }
+  u128 inv(unsigned level, u128 a) const {
+    if (level == 3) return I[(uint32_t)a];
+    const unsigned half = 1u << (level - 1);
+    const u128 mask = ((u128)1 << half) - 1;
+    const u128 a0 = a & mask, a1 = a >> half, bt = beta(level);
+    const u128 lo = a0 ^ mul(level - 1, a1, bt);
+    const u128 nrm = mul(level - 1, a0, lo) ^ mul(level - 1, a1, a1);
+    const u128 ni = inv(level - 1, nrm);
+    return mul(level - 1, lo, ni) | (mul(level - 1, a1, ni) << half);
+  }
+};
+
+const HostTower& host_tower() {
+  static const HostTower t;
+  return t;
+}
+
+// ---- host: SHA-256 (FIPS 180-4), the sum-check transcript's hash --------------------
+
+class Sha256 {
+ public:
+  Sha256() { reset(); }
+  void update(const uint8_t* p, size_t n) {
+    total_ += n;
+    while (n) {
+      const size_t take = std::min(n, (size_t)64 - fill_);
+      std::memcpy(buf_ + fill_, p, take);
+      fill_ += take;
+      p += take;
+      n -= take;
+      if (fill_ == 64) {
+        block(buf_);
+        fill_ = 0;
+      }
+    }
+  }
+  void final(uint8_t out[32]) {
+    const uint64_t bits = total_ * 8;
+    const uint8_t one = 0x80, zero = 0;
+    update(&one, 1);
+    while (fill_ != 56) update(&zero, 1);
+    uint8_t len[8];
+    for (int i = 0; i < 8; ++i) len[i] = (uint8_t)(bits >> (56 - 8 * i));
+    update(len, 8);
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 4; ++j) out[4 * i + j] = (uint8_t)(h_[i] >> (24 - 8 * j));
+    reset();
+  }
+  static void hash(const uint8_t* p, size_t n, uint8_t out[32]) {
+    Sha256 s;
+    s.update(p, n);
+    s.final(out);
+  }
+
+ private:
+  static uint32_t rotr(uint32_t x, unsigned r) { return (x >> r) | (x << (32 - r)); }
+  void reset() {
+    static const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
+                                   0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+    std::memcpy(h_, iv, sizeof(iv));
+    fill_ = 0;
+    total_ = 0;
+  }
+  void block(const uint8_t* p) {
+    static const uint32_t K[64] = {
+        0x428a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4, 0xab1c5ed5,
+        0xd807aa98, 0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe, 0x9bdc06a7, 0xc19bf174,
+        0xe49b69c1, 0xefbe4786, 0x0fc19dc6, 0x240ca1cc, 0x2de92c6f, 0x4a7484aa, 0x5cb0a9dc, 0x76f988da,
+        0x983e5152, 0xa831c66d, 0xb00327c8, 0xbf597fc7, 0xc6e00bf3, 0xd5a79147, 0x06ca6351, 0x14292967,
+        0x27b70a85, 0x2e1b2138, 0x4d2c6dfc, 0x53380d13, 0x650a7354, 0x766a0abb, 0x81c2c92e, 0x92722c85,
+        0xa2bfe8a1, 0xa81a664b, 0xc24b8b70, 0xc76c51a3, 0xd192e819, 0xd6990624, 0xf40e3585, 0x106aa070,
+        0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
+        0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
+    uint32_t w[64];
+    for (int i = 0; i < 16; ++i)
+      w[i] = (uint32_t)p[4 * i] << 24 | (uint32_t)p[4 * i + 1] << 16 | (uint32_t)p[4 * i + 2] << 8 | p[4 * i + 3];
+    for (int i = 16; i < 64; ++i) {
+      const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
+      const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
+      w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+    }
+    uint32_t a = h_[0], b = h_[1], c = h_[2], d = h_[3], e = h_[4], f = h_[5], g = h_[6], h = h_[7];
+    for (int i = 0; i < 64; ++i) {
+      const uint32_t t1 = h + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + K[i] + w[i];
+      const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+      h = g;
+      g = f;
+      f = e;
+      e = d + t1;
+      d = c;
+      c = b;
+      b = a;
+      a = t1 + t2;
+    }
+    h_[0] += a, h_[1] += b, h_[2] += c, h_[3] += d, h_[4] += e, h_[5] += f, h_[6] += g, h_[7] += h;
+  }
+  uint32_t h_[8];
+  uint8_t buf_[64];
+  size_t fill_;
+  uint64_t total_;
+};
+
+// ---- device: the GF(2^8) table, tower arithmetic over it ---------------------------
+
+std::mutex g_table_mu;
+uint8_t* g_tables[64] = {};
+
+const uint8_t* product_table(cudaStream_t st) {
+  int dev = 0;
+  ZS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Error(ZS_EDEVICE, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_table_mu);
+  if (!g_tables[dev]) {
+    const HostTower& ht = host_tower();
+    uint8_t* d = nullptr;
+    ZS_CUDA(cudaMalloc(&d, 65536));
+    ZS_CUDA(cudaMemcpyAsync(d, ht.T.data(), 65536, cudaMemcpyHostToDevice, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+    g_tables[dev] = d;
+  }
+  return g_tables[dev];
+}
+
+struct g128 {
+  uint64_t lo, hi;
+};
+__device__ __forceinline__ g128 gxor(const g128& a, const g128& b) { return {a.lo ^ b.lo, a.hi ^ b.hi}; }
+
+struct Tower {
+  const uint8_t* T;  // shared memory, T[(a << 8) | b] = a * b in GF(2^8)
+  __device__ __forceinline__ uint32_t m8(uint32_t a, uint32_t b) const { return T[(a << 8) | b]; }
+  // x * X_3 at level 4 (x * 0x100), from x = e0 + e1 X_3: e1 + (e0 + e1 X_2) X_3
+  __device__ __forceinline__ uint32_t a16(uint32_t x) const {
+    const uint32_t e0 = x & 0xff, e1 = x >> 8;
+    return e1 | ((e0 ^ m8(e1, 0x10)) << 8);
+  }
+  __device__ __forceinline__ uint32_t m16(uint32_t a, uint32_t b) const {
+    const uint32_t a0 = a & 0xff, a1 = a >> 8, b0 = b & 0xff, b1 = b >> 8;
+    const uint32_t c0 = m8(a0, b0), c1 = m8(a1, b1), c2 = m8(a0 ^ a1, b0 ^ b1);
+    return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ m8(c1, 0x10)) << 8);
+  }
+  __device__ __forceinline__ uint32_t a32(uint32_t x) const {
+    const uint32_t e0 = x & 0xffff, e1 = x >> 16;
+    return e1 | ((e0 ^ a16(e1)) << 16);
+  }
+  __device__ __forceinline__ uint32_t m32(uint32_t a, uint32_t b) const {
+    const uint32_t a0 = a & 0xffff, a1 = a >> 16, b0 = b & 0xffff, b1 = b >> 16;
+    const uint32_t c0 = m16(a0, b0), c1 = m16(a1, b1), c2 = m16(a0 ^ a1, b0 ^ b1);
+    return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ a16(c1)) << 16);
+  }
+  __device__ __forceinline__ uint64_t a64(uint64_t x) const {
+    const uint32_t e0 = (uint32_t)x, e1 = (uint32_t)(x >> 32);
+    return (uint64_t)e1 | ((uint64_t)(e0 ^ a32(e1)) << 32);
+  }
+  __device__ __forceinline__ uint64_t m64(uint64_t a, uint64_t b) const {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    const uint32_t c0 = m32(a0, b0), c1 = m32(a1, b1), c2 = m32(a0 ^ a1, b0 ^ b1);
+    return (uint64_t)(c0 ^ c1) | ((uint64_t)(c2 ^ c0 ^ c1 ^ a32(c1)) << 32);
+  }
+  // level 7: beta = X_5, the root of level 6
+  __device__ __forceinline__ g128 m128(const g128& a, const g128& b) const {
+    const uint64_t c0 = m64(a.lo, b.lo), c1 = m64(a.hi, b.hi), c2 = m64(a.lo ^ a.hi, b.lo ^ b.hi);
+    return {c0 ^ c1, c2 ^ c0 ^ c1 ^ a64(c1)};
+  }
+  // s * x for a GF(2^8) scalar s: every byte coordinate of x times s
+  __device__ __forceinline__ uint64_t s64(uint32_t s, uint64_t x) const {
+    uint64_t r = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r |= (uint64_t)m8(s, (uint32_t)(x >> (8 * k)) & 0xff) << (8 * k);
+    return r;
+  }
+  __device__ __forceinline__ g128 s128(uint32_t s, const g128& x) const { return {s64(s, x.lo), s64(s, x.hi)}; }
+};
+
+// One round's term list, passed by value: coefficient k at coef[es k ..], its factor tables
+// idx[off[k] .. off[k + 1]).
+struct Terms {
+  uint32_t nterms;
+  uint32_t off[kMaxTerms + 1];
+  uint16_t idx[kMaxFactors];
+  alignas(16) uint8_t coef[16 * kMaxTerms];
+};
+
+__device__ __forceinline__ void load_table(uint8_t* s_T, const uint8_t* __restrict__ gT) {
+  const uint4* src = reinterpret_cast<const uint4*>(gT);
+  uint4* dst = reinterpret_cast<uint4*>(s_T);
+  for (uint32_t k = threadIdx.x; k < 65536 / 16; k += blockDim.x) dst[k] = src[k];
+}
+
+// XOR of `v` over the warp into `acc` (shared memory).
+__device__ __forceinline__ void warp_xor_into(uint32_t v, uint32_t* acc) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v ^= __shfl_xor_sync(0xffffffffu, v, d);
+  if ((threadIdx.x & 31) == 0 && v) atomicXor(acc, v);
+}
+
+// The point t's linear factor a + t (a + b): a at t = 0, b at t = 1.
+template <int t>
+__device__ __forceinline__ uint32_t at_point8(const Tower& F, uint32_t a, uint32_t b) {
+  if constexpr (t == 0) return a;
+  else if constexpr (t == 1) return b;
+  else return a ^ F.m8(t, a ^ b);
+}
+template <int t>
+__device__ __forceinline__ g128 at_point128(const Tower& F, const g128& a, const g128& b) {
+  if constexpr (t == 0) return a;
+  else if constexpr (t == 1) return b;
+  else return gxor(a, F.s128(t, gxor(a, b)));
+}
+
+template <int D, int t = 0>
+__device__ __forceinline__ void factor8(const Tower& F, uint32_t (&prod)[D], uint32_t a, uint32_t b) {
+  if constexpr (t < D) {
+    prod[t] = F.m8(prod[t], at_point8<t>(F, a, b));
+    factor8<D, t + 1>(F, prod, a, b);
+  }
+}
+template <int D, int t = 0>
+__device__ __forceinline__ void factor128(const Tower& F, g128 (&prod)[D], const g128& a, const g128& b) {
+  if constexpr (t < D) {
+    prod[t] = F.m128(prod[t], at_point128<t>(F, a, b));
+    factor128<D, t + 1>(F, prod, a, b);
+  }
+}
+
+// GF(2^8) round. D > 0: the D = dmax + 1 points in registers; D = 0: one point per pass.
+// out: (dmax + 1) bytes packed four to a word (little-endian: byte t is values[t]).
+template <int D>
+__global__ void __launch_bounds__(kBThreads) k_values8(const uint8_t* __restrict__ cur, uint32_t len, uint32_t half,
+                                                       uint32_t dmax, const __grid_constant__ Terms tm,
+                                                       const uint8_t* __restrict__ gT, uint32_t* __restrict__ out) {
+  extern __shared__ uint4 smem_b[];
+  uint8_t* s_T = reinterpret_cast<uint8_t*>(smem_b);
+  uint32_t* s_acc = reinterpret_cast<uint32_t*>(s_T + 65536);
+  const uint32_t words = (dmax + 4) / 4;
+  load_table(s_T, gT);
+  for (uint32_t k = threadIdx.x; k < words; k += blockDim.x) s_acc[k] = 0;
+  __syncthreads();
+  const Tower F{s_T};
+  const uint32_t stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (D > 0) {
+    uint32_t acc[D];
+#pragma unroll
+    for (int t = 0; t < D; ++t) acc[t] = 0;
+    for (uint32_t rest = first; rest < half; rest += stride) {
+      for (uint32_t k = 0; k < tm.nterms; ++k) {
+        uint32_t prod[D];
+#pragma unroll
+        for (int t = 0; t < D; ++t) prod[t] = tm.coef[k];
+        for (uint32_t j = tm.off[k]; j < tm.off[k + 1]; ++j) {
+          const uint8_t* c = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
+          factor8<D>(F, prod, c[0], c[1]);
+        }
+#pragma unroll
+        for (int t = 0; t < D; ++t) acc[t] ^= prod[t];
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < D; ++t) warp_xor_into(acc[t] << (8 * (t & 3)), s_acc + (t >> 2));
+  } else {
+    for (uint32_t t = 0; t <= dmax; ++t) {
+      uint32_t acc = 0;
+      for (uint32_t rest = first; rest < half; rest += stride) {
+        for (uint32_t k = 0; k < tm.nterms; ++k) {
+          uint32_t prod = tm.coef[k];
+          for (uint32_t j = tm.off[k]; j < tm.off[k + 1]; ++j) {
+            const uint8_t* c = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
+            const uint32_t a = c[0];
+            prod = F.m8(prod, a ^ F.m8(t, a ^ c[1]));
+          }
+          acc ^= prod;
+        }
+      }
+      warp_xor_into(acc << (8 * (t & 3)), s_acc + (t >> 2));
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < words; k += blockDim.x)
+    if (s_acc[k]) atomicXor(out + k, s_acc[k]);
+}
+
+__device__ __forceinline__ void warp_xor_into128(const g128& v, uint32_t* acc) {
+  warp_xor_into((uint32_t)v.lo, acc);
+  warp_xor_into((uint32_t)(v.lo >> 32), acc + 1);
+  warp_xor_into((uint32_t)v.hi, acc + 2);
+  warp_xor_into((uint32_t)(v.hi >> 32), acc + 3);
+}
+
+// GF(2^128) round; out: (dmax + 1) values of four little-endian words.
+template <int D>
+__global__ void __launch_bounds__(kBThreads) k_values128(const uint4* __restrict__ cur, uint32_t len, uint32_t half,
+                                                         uint32_t dmax, const __grid_constant__ Terms tm,
+                                                         const uint8_t* __restrict__ gT, uint32_t* __restrict__ out) {
+  extern __shared__ uint4 smem_b[];
+  uint8_t* s_T = reinterpret_cast<uint8_t*>(smem_b);
+  uint32_t* s_acc = reinterpret_cast<uint32_t*>(s_T + 65536);
+  const uint32_t words = 4 * (dmax + 1);
+  load_table(s_T, gT);
+  for (uint32_t k = threadIdx.x; k < words; k += blockDim.x) s_acc[k] = 0;
+  __syncthreads();
+  const Tower F{s_T};
+  const uint32_t stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
+  auto coef = [&](uint32_t k) {
+    const uint64_t* cf = reinterpret_cast<const uint64_t*>(tm.coef + 16 * k);
+    return g128{cf[0], cf[1]};
+  };
+  auto elem = [&](const uint4* p) { return g128{(uint64_t)p->y << 32 | p->x, (uint64_t)p->w << 32 | p->z}; };
+  if constexpr (D > 0) {
+    g128 acc[D];
+#pragma unroll
+    for (int t = 0; t < D; ++t) acc[t] = {0, 0};
+    for (uint32_t rest = first; rest < half; rest += stride) {
+      for (uint32_t k = 0; k < tm.nterms; ++k) {
+        g128 prod[D];
+        const g128 c0 = coef(k);
+#pragma unroll
+        for (int t = 0; t < D; ++t) prod[t] = c0;
+        for (uint32_t j = tm.off[k]; j < tm.off[k + 1]; ++j) {
+          const uint4* c = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
+          factor128<D>(F, prod, elem(c), elem(c + 1));
+        }
+#pragma unroll
+        for (int t = 0; t < D; ++t) acc[t] = gxor(acc[t], prod[t]);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < D; ++t) warp_xor_into128(acc[t], s_acc + 4 * t);
+  } else {
+    for (uint32_t t = 0; t <= dmax; ++t) {
+      g128 acc{0, 0};
+      for (uint32_t rest = first; rest < half; rest += stride) {
+        for (uint32_t k = 0; k < tm.nterms; ++k) {
+          g128 prod = coef(k);
+          for (uint32_t j = tm.off[k]; j < tm.off[k + 1]; ++j) {
+            const uint4* c = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
+            const g128 a = elem(c), b = elem(c + 1);
+            prod = F.m128(prod, gxor(a, F.s128(t, gxor(a, b))));
+          }
+          acc = gxor(acc, prod);
+        }
+      }
+      warp_xor_into128(acc, s_acc + 4 * t);
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.x; k < words; k += blockDim.x)
+    if (s_acc[k]) atomicXor(out + k, s_acc[k]);
+}
+
+// next[f][rest] = a + r (a + b) over GF(2^8); grid.y runs over the tables.
+__global__ void __launch_bounds__(kBThreads) k_fold8(const uint8_t* __restrict__ cur, uint32_t len, uint32_t half,
+                                                     uint32_t r, const uint8_t* __restrict__ gT,
+                                                     uint8_t* __restrict__ next) {
+  __shared__ uint8_t row[256];
+  for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) row[k] = gT[(r << 8) | k];
+  __syncthreads();
+  const uint8_t* src = cur + (size_t)blockIdx.y * len;
+  uint8_t* dst = next + (size_t)blockIdx.y * half;
+  for (uint32_t rest = blockIdx.x * blockDim.x + threadIdx.x; rest < half; rest += gridDim.x * blockDim.x) {
+    const uint32_t a = src[2 * (size_t)rest], b = src[2 * (size_t)rest + 1];
+    dst[rest] = (uint8_t)(a ^ row[a ^ b]);
+  }
+}
+
+// R[k][v] = r * (v at byte k), the GF(2^8)-linear map x -> r x on byte coordinates.
+__global__ void __launch_bounds__(kBThreads) k_mul_table128(uint64_t r_lo, uint64_t r_hi,
+                                                            const uint8_t* __restrict__ gT, uint4* __restrict__ R) {
+  extern __shared__ uint4 smem_b[];
+  uint8_t* s_T = reinterpret_cast<uint8_t*>(smem_b);
+  load_table(s_T, gT);
+  __syncthreads();
+  const Tower F{s_T};
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;  // < 4096 by the launch
+  const uint32_t k = i >> 8, v = i & 255;
+  const g128 x{k < 8 ? (uint64_t)v << (8 * k) : 0, k >= 8 ? (uint64_t)v << (8 * (k - 8)) : 0};
+  const g128 p = F.m128(g128{r_lo, r_hi}, x);
+  R[i] = make_uint4((uint32_t)p.lo, (uint32_t)(p.lo >> 32), (uint32_t)p.hi, (uint32_t)(p.hi >> 32));
+}
+
+__global__ void __launch_bounds__(kBThreads) k_fold128(const uint4* __restrict__ cur, uint32_t len, uint32_t half,
+                                                       const uint4* __restrict__ R, uint4* __restrict__ next) {
+  extern __shared__ uint4 smem_b[];
+  uint4* s_R = smem_b;
+  for (uint32_t k = threadIdx.x; k < 4096; k += blockDim.x) s_R[k] = R[k];
+  __syncthreads();
+  const uint4* src = cur + (size_t)blockIdx.y * len;
+  uint4* dst = next + (size_t)blockIdx.y * half;
+  for (uint32_t rest = blockIdx.x * blockDim.x + threadIdx.x; rest < half; rest += gridDim.x * blockDim.x) {
+    const uint4 a = src[2 * (size_t)rest], b = src[2 * (size_t)rest + 1];
+    const uint32_t d[4] = {a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w};
+    uint4 o = a;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint4 e = s_R[(k << 8) | ((d[k >> 2] >> (8 * (k & 3))) & 0xff)];
+      o.x ^= e.x, o.y ^= e.y, o.z ^= e.z, o.w ^= e.w;
+    }
+    dst[rest] = o;
+  }
+}
+
+// ---- host: argument checks and launches -------------------------------------------
+
+Terms pack_terms(bool wide, size_t m, const uint8_t* coeffs, size_t nterms, const uint32_t* indices,
+                 size_t n_indices, const uint32_t* offsets) {
+  if (!coeffs || !offsets || (n_indices && !indices)) throw Error(ZS_EMALFORMED, "null terms");
+  if (nterms == 0 || nterms > kMaxTerms || n_indices > kMaxFactors) throw Error(ZS_EMALFORMED, "too many terms");
+  if (m == 0 || m > kMaxTables) throw Error(ZS_EMALFORMED, "table count");
+  if (offsets[0] != 0 || offsets[nterms] != n_indices) throw Error(ZS_EMALFORMED, "term offsets");
+  Terms tm;
+  std::memset(&tm, 0, sizeof(tm));
+  tm.nterms = (uint32_t)nterms;
+  for (size_t k = 0; k <= nterms; ++k) {
+    if (k && offsets[k] < offsets[k - 1]) throw Error(ZS_EMALFORMED, "term offsets");
+    tm.off[k] = offsets[k];
+  }
+  for (size_t j = 0; j < n_indices; ++j) {
+    if (indices[j] >= m) throw Error(ZS_EMALFORMED, "factor table out of range");
+    tm.idx[j] = (uint16_t)indices[j];
+  }
+  std::memcpy(tm.coef, coeffs, nterms * (wide ? 16 : 1));
+  return tm;
+}
+
+void check_rows(size_t len, size_t half, size_t dmax) {
+  if (2 * half > len || len > 0xffffffffu) throw Error(ZS_EMALFORMED, "table length");
+  if (dmax > kMaxPoint) throw Error(ZS_EMALFORMED, "more than 256 points");
+}
+
+int sm_count() {
+  int dev = 0, sms = 0;
+  ZS_CUDA(cudaGetDevice(&dev));
+  ZS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return sms;
+}
+
+// Zeroes d_out and accumulates one round's values into it, asynchronously on `st`.
+void values_async(bool wide, const void* d_cur, size_t len, size_t half, size_t dmax, const Terms& tm, void* d_out,
+                  cudaStream_t st) {
+  const size_t words = wide ? 4 * (dmax + 1) : (dmax + 4) / 4;
+  ZS_CUDA(cudaMemsetAsync(d_out, 0, words * 4, st));
+  if (half == 0) return;
+  const uint8_t* T = product_table(st);
+  const size_t smem = 65536 + 4 * words;
+  const size_t want = (half + kBThreads - 1) / kBThreads;
+  const int sms = sm_count();
+  uint32_t* out = static_cast<uint32_t*>(d_out);
+  const uint32_t L = (uint32_t)len, H = (uint32_t)half, M = (uint32_t)dmax;
+  // one wave: as many CTAs as fit on every SM (shared memory and registers), fewer for
+  // small tables
+#define ZS_VALUES_CASE(KERN, PTR, DD)                                                                  \
+  do {                                                                                                 \
+    ZS_CUDA(cudaFuncSetAttribute(KERN<DD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));   \
+    int per_sm = 1;                                                                                    \
+    ZS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KERN<DD>, kBThreads, smem));        \
+    const uint32_t blocks = (uint32_t)std::min<size_t>(want, (size_t)sms * std::max(per_sm, 1));       \
+    KERN<DD><<<blocks, kBThreads, smem, st>>>(static_cast<PTR>(d_cur), L, H, M, tm, T, out);          \
+  } while (0)
+  const int D = dmax + 1 <= (size_t)kRegPoints ? (int)dmax + 1 : 0;
+  if (wide) {
+    switch (D) {
+      case 1: ZS_VALUES_CASE(k_values128, const uint4*, 1); break;
+      case 2: ZS_VALUES_CASE(k_values128, const uint4*, 2); break;
+      case 3: ZS_VALUES_CASE(k_values128, const uint4*, 3); break;
+      case 4: ZS_VALUES_CASE(k_values128, const uint4*, 4); break;
+      case 5: ZS_VALUES_CASE(k_values128, const uint4*, 5); break;
+      case 6: ZS_VALUES_CASE(k_values128, const uint4*, 6); break;
+      case 7: ZS_VALUES_CASE(k_values128, const uint4*, 7); break;
+      case 8: ZS_VALUES_CASE(k_values128, const uint4*, 8); break;
+      default: ZS_VALUES_CASE(k_values128, const uint4*, 0); break;
+    }
+  } else {
+    switch (D) {
+      case 1: ZS_VALUES_CASE(k_values8, const uint8_t*, 1); break;
+      case 2: ZS_VALUES_CASE(k_values8, const uint8_t*, 2); break;
+      case 3: ZS_VALUES_CASE(k_values8, const uint8_t*, 3); break;
+      case 4: ZS_VALUES_CASE(k_values8, const uint8_t*, 4); break;
+      case 5: ZS_VALUES_CASE(k_values8, const uint8_t*, 5); break;
+      case 6: ZS_VALUES_CASE(k_values8, const uint8_t*, 6); break;
+      case 7: ZS_VALUES_CASE(k_values8, const uint8_t*, 7); break;
+      case 8: ZS_VALUES_CASE(k_values8, const uint8_t*, 8); break;
+      default: ZS_VALUES_CASE(k_values8, const uint8_t*, 0); break;
+    }
+  }
+#undef ZS_VALUES_CASE
+  ZS_CUDA(cudaGetLastError());
+}
+
+// next (m tables of len / 2) = fold of cur (m tables of len) at r, asynchronously on `st`.
+// r_mul: a 64 KB device buffer for the GF(2^128) multiply table.
+void fold_async(bool wide, const void* d_cur, size_t len, size_t m, u128 r, void* d_next, uint4* r_mul,
+                cudaStream_t st) {
+  const size_t half = len / 2;
+  if (half == 0) return;
+  const uint8_t* T = product_table(st);
+  const uint32_t bx = (uint32_t)std::min<size_t>((half + kBThreads - 1) / kBThreads,
+                                                 std::max<size_t>(1, (size_t)sm_count() * 8 / m));
+  const dim3 grid(bx, (unsigned)m);
+  if (!wide) {
+    k_fold8<<<grid, kBThreads, 0, st>>>(static_cast<const uint8_t*>(d_cur), (uint32_t)len, (uint32_t)half,
+                                        (uint32_t)r, T, static_cast<uint8_t*>(d_next));
+  } else {
+    ZS_CUDA(cudaFuncSetAttribute(k_mul_table128, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
+    k_mul_table128<<<4096 / kBThreads, kBThreads, 65536, st>>>((uint64_t)r, (uint64_t)(r >> 64), T, r_mul);
+    ZS_CUDA(cudaFuncSetAttribute(k_fold128, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
+    k_fold128<<<grid, kBThreads, 65536, st>>>(static_cast<const uint4*>(d_cur), (uint32_t)len, (uint32_t)half,
+                                              r_mul, static_cast<uint4*>(d_next));
+  }
+  ZS_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+struct DevMem {
+  T* p = nullptr;
+  cudaStream_t st;
+  DevMem(size_t n, cudaStream_t s) : st(s) { ZS_CUDA(cudaMallocAsync((void**)&p, n ? n * sizeof(T) : 1, s)); }
+  ~DevMem() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+};
+
+template <typename F>
+int32_t guarded(F&& f) {
+  try {
+    f();
+    return ZS_OK;
+  } catch (const Error& e) {
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    return ZS_ENOMEM;
+  } catch (...) {
+    return ZS_EGENERIC;
+  }
+}
+
+bool field_wide(uint32_t field_bits) {
+  if (field_bits != 8 && field_bits != 128) throw Error(ZS_EMALFORMED, "field_bits is 8 or 128");
+  return field_bits == 128;
+}
+
+int32_t hook_values(bool wide, const uint8_t* cur_flat, size_t len, size_t m, const uint8_t* coeffs, size_t nterms,
+                    const uint32_t* indices, size_t n_indices, const uint32_t* offsets, size_t dmax, size_t half,
+                    uint8_t* out, void* stream) {
+  return guarded([&] {
+    if (!cur_flat || !out) throw Error(ZS_EMALFORMED, "null buffer");
+    check_rows(len, half, dmax);
+    const Terms tm = pack_terms(wide, m, coeffs, nterms, indices, n_indices, offsets);
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t es = wide ? 16 : 1, words = wide ? 4 * (dmax + 1) : (dmax + 4) / 4;
+    DevMem<uint4> d_cur((m * len * es + 15) / 16, st);
+    DevMem<uint32_t> d_out(words, st);
+    if (m * len) ZS_CUDA(cudaMemcpyAsync(d_cur.p, cur_flat, m * len * es, cudaMemcpyHostToDevice, st));
+    values_async(wide, d_cur.p, len, half, dmax, tm, d_out.p, st);
+    std::vector<uint32_t> h(words);
+    ZS_CUDA(cudaMemcpyAsync(h.data(), d_out.p, words * 4, cudaMemcpyDeviceToHost, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(out, h.data(), (dmax + 1) * es);
+  });
+}
+
+// ---- host: the combination prover (sumcheck.zig:208-395) ---------------------------
+
+u128 load_elem(const uint8_t* p, size_t es) {
+  u128 v = 0;
+  for (size_t i = es; i-- > 0;) v = (v << 8) | p[i];
+  return v;
+}
+void store_elem(uint8_t* p, size_t es, u128 v) {
+  for (size_t i = 0; i < es; ++i) p[i] = (uint8_t)(v >> (8 * i));
+}
+
+// Lagrange interpolation through the points 0..n-1 (sumcheck.zig:124-162): low-first
+// coefficients. The denominators depend on the points only and come precomputed.
+std::vector<u128> interpolate(const HostTower& ht, unsigned level, const std::vector<u128>& values,
+                              const std::vector<u128>& inv_denom) {
+  const size_t n = values.size();
+  std::vector<u128> coeffs(n, 0), basis(n + 1), next(n + 1);
+  for (size_t i = 0; i < n; ++i) {
+    basis[0] = 1;
+    size_t deg = 1;
+    for (size_t j = 0; j < n; ++j) {
+      if (j == i) continue;
+      for (size_t d = 0; d <= deg; ++d) {  // basis *= (x + j)
+        const u128 lo = d == 0 ? 0 : basis[d - 1], hi = d == deg ? 0 : basis[d];
+        next[d] = lo ^ ht.mul(level, (u128)j, hi);
+      }
+      std::copy(next.begin(), next.begin() + deg + 1, basis.begin());
+      ++deg;
+    }
+    const u128 scale = ht.mul(level, inv_denom[i], values[i]);
+    for (size_t d = 0; d < deg; ++d) coeffs[d] ^= ht.mul(level, basis[d], scale);
+  }
+  return coeffs;
+}
+
+int32_t prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k, size_t m, const uint8_t* coeffs,
+                          size_t nterms, const uint32_t* indices, size_t n_indices, const uint32_t* offsets,
+                          const uint8_t* seed, size_t seed_len, int32_t has_seed, uint8_t* claimed_out,
+                          uint8_t* rounds_out, void* stream) {
+  return guarded([&] {
+    const bool wide = field_wide(field_bits);
+    const unsigned level = wide ? 7 : 3;
+    const size_t es = wide ? 16 : 1;
+    if (!tables || !claimed_out || (k && !rounds_out) || (has_seed && seed_len && !seed))
+      throw Error(ZS_EMALFORMED, "null buffer");
+    if (k > 31) throw Error(ZS_EMALFORMED, "more than 2^31 rows");
+    const Terms tm = pack_terms(wide, m, coeffs, nterms, indices, n_indices, offsets);
+    size_t dmax = 0;
+    for (size_t t = 0; t < nterms; ++t) dmax = std::max<size_t>(dmax, offsets[t + 1] - offsets[t]);
+    if (dmax + 1 > kProveMaxPoints) throw Error(ZS_EMALFORMED, "more than 64 points");
+    const size_t n = (size_t)1 << k;
+    if (m > (((size_t)1 << 36) / es) / n) throw Error(ZS_EMALFORMED, "tables larger than 64 GB");
+    const HostTower& ht = host_tower();
+
+    // the transcript (sumcheck.zig:47-87)
+    uint8_t state[32];
+    auto absorb = [&](const std::vector<u128>& cs) {
+      Sha256 h;
+      h.update(state, 32);
+      uint8_t b[16];
+      for (u128 c : cs) {
+        store_elem(b, es, c);
+        h.update(b, es);
+      }
+      h.final(state);
+      return wide ? load_elem(state + 16, 16) : (u128)state[31];
+    };
+    auto start = [&](u128 claimed) {
+      if (has_seed) {
+        Sha256::hash(seed, seed_len, state);
+      } else {
+        uint8_t b[16];
+        store_elem(b, es, claimed);
+        Sha256::hash(b, es, state);
+      }
+    };
+
+    if (k == 0) {  // one row: the claimed sum is g at it, no rounds
+      u128 h = 0;
+      for (size_t t = 0; t < nterms; ++t) {
+        u128 p = load_elem(coeffs + es * t, es);
+        for (uint32_t j = offsets[t]; j < offsets[t + 1]; ++j) p = ht.mul(level, p, load_elem(tables + es * indices[j], es));
+        h ^= p;
+      }
+      store_elem(claimed_out, es, h);
+      return;
+    }
+
+    // 1 / prod_{j != i} (i + j) for the points 0..dmax
+    std::vector<u128> inv_denom(dmax + 1);
+    for (size_t i = 0; i <= dmax; ++i) {
+      u128 d = 1;
+      for (size_t j = 0; j <= dmax; ++j)
+        if (j != i) d = ht.mul(level, d, (u128)(i ^ j));
+      inv_denom[i] = ht.inv(level, d);
+    }
+
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t words = wide ? 4 * (dmax + 1) : (dmax + 4) / 4;
+    DevMem<uint4> d_a((m * n * es + 15) / 16, st), d_b((m * (n / 2) * es + 15) / 16, st);
+    DevMem<uint32_t> d_vals(words, st);
+    DevMem<uint4> d_rmul(wide ? 4096 : 0, st);
+    uint32_t* h_vals = nullptr;
+    ZS_CUDA(cudaMallocHost((void**)&h_vals, words * 4));
+    std::unique_ptr<uint32_t, decltype(&cudaFreeHost)> h_guard(h_vals, &cudaFreeHost);
+    ZS_CUDA(cudaMemcpyAsync(d_a.p, tables, m * n * es, cudaMemcpyHostToDevice, st));
+
+    void* cur = d_a.p;
+    void* nxt = d_b.p;
+    size_t len = n;
+    std::vector<u128> values(dmax + 1);
+    for (size_t i = 0; i < k; ++i) {
+      const size_t half = len / 2;
+      values_async(wide, cur, len, half, dmax, tm, d_vals.p, st);
+      ZS_CUDA(cudaMemcpyAsync(h_vals, d_vals.p, words * 4, cudaMemcpyDeviceToHost, st));
+      ZS_CUDA(cudaStreamSynchronize(st));
+      const uint8_t* vb = reinterpret_cast<const uint8_t*>(h_vals);
+      for (size_t t = 0; t <= dmax; ++t) values[t] = load_elem(vb + es * t, es);
+      if (i == 0) {  // the hypercube sum: g over the even rows plus g over the odd rows
+        const u128 h = values[0] ^ (dmax >= 1 ? values[1] : values[0]);
+        store_elem(claimed_out, es, h);
+        start(h);
+      }
+      const std::vector<u128> cs = interpolate(ht, level, values, inv_denom);
+      for (size_t t = 0; t <= dmax; ++t) store_elem(rounds_out + es * ((dmax + 1) * i + t), es, cs[t]);
+      const u128 r = absorb(cs);
+      if (i + 1 < k) {
+        fold_async(wide, cur, len, m, r, nxt, d_rmul.p, st);
+        std::swap(cur, nxt);
+      }
+      len = half;
+    }
+    ZS_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+}  // namespace
+}  // namespace zs
+
+extern "C" int32_t zs_binius_sumcheck_values_gf256(const uint8_t* cur_flat, size_t len, size_t m,
+                                                   const uint8_t* coeffs, size_t nterms, const uint32_t* indices,
+                                                   size_t n_indices, const uint32_t* offsets, size_t dmax, size_t half,
+                                                   uint8_t* out, void* stream) {
+  return zs::hook_values(false, cur_flat, len, m, coeffs, nterms, indices, n_indices, offsets, dmax, half, out,
+                         stream);
+}
+
+extern "C" int32_t zs_binius_sumcheck_values_gf128(const uint8_t* cur_flat, size_t len, size_t m,
+                                                   const uint8_t* coeffs, size_t nterms, const uint32_t* indices,
+                                                   size_t n_indices, const uint32_t* offsets, size_t dmax,
+                                                   size_t half, uint8_t* out, void* stream) {
+  return zs::hook_values(true, cur_flat, len, m, coeffs, nterms, indices, n_indices, offsets, dmax, half, out,
+                         stream);
+}
+
+extern "C" int32_t zs_binius_sumcheck_values_device(uint32_t field_bits, const void* d_cur, size_t len, size_t m,
+                                                    const uint8_t* coeffs, size_t nterms, const uint32_t* indices,
+                                                    size_t n_indices, const uint32_t* offsets, size_t dmax,
+                                                    size_t half, void* d_out, void* stream) {
+  return zs::guarded([&] {
+    const bool wide = zs::field_wide(field_bits);
+    if (!d_cur || !d_out) throw zs::Error(zs::ZS_EMALFORMED, "null buffer");
+    if ((reinterpret_cast<uintptr_t>(d_out) & 3) || (wide && (reinterpret_cast<uintptr_t>(d_cur) & 15)))
+      throw zs::Error(zs::ZS_EMALFORMED, "misaligned buffer");
+    zs::check_rows(len, half, dmax);
+    const zs::Terms tm = zs::pack_terms(wide, m, coeffs, nterms, indices, n_indices, offsets);
+    zs::values_async(wide, d_cur, len, half, dmax, tm, d_out, (cudaStream_t)stream);
+  });
+}
+
+extern "C" int32_t zs_binius_sumcheck_fold_device(uint32_t field_bits, const void* d_cur, size_t len, size_t m,
+                                                  const uint8_t* r, void* d_next, void* d_scratch, void* stream) {
+  return zs::guarded([&] {
+    const bool wide = zs::field_wide(field_bits);
+    if (!d_cur || !d_next || !r || (wide && !d_scratch)) throw zs::Error(zs::ZS_EMALFORMED, "null buffer");
+    if (wide && ((reinterpret_cast<uintptr_t>(d_cur) | reinterpret_cast<uintptr_t>(d_next) |
+                  reinterpret_cast<uintptr_t>(d_scratch)) & 15))
+      throw zs::Error(zs::ZS_EMALFORMED, "misaligned buffer");
+    if (len > 0xffffffffu || m == 0 || m > zs::kMaxTables) throw zs::Error(zs::ZS_EMALFORMED, "table shape");
+    zs::fold_async(wide, d_cur, len, m, zs::load_elem(r, wide ? 16 : 1), d_next, static_cast<uint4*>(d_scratch),
+                   (cudaStream_t)stream);
+  });
+}
+
+extern "C" int32_t zs_binius_sumcheck_prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k,
+                                                        size_t m, const uint8_t* coeffs, size_t nterms,
+                                                        const uint32_t* indices, size_t n_indices,
+                                                        const uint32_t* offsets, const uint8_t* seed,
+                                                        size_t seed_len, int32_t has_seed, uint8_t* claimed_out,
+                                                        uint8_t* rounds_out, void* stream) {
+  return zs::prove_combination(field_bits, tables, k, m, coeffs, nterms, indices, n_indices, offsets, seed,
+                               seed_len, has_seed, claimed_out, rounds_out, stream);
+}

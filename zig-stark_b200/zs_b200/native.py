@@ -548,3 +548,96 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def _binius_values(fn, es, cur_flat, length, m, coeffs, indices, offsets, dmax, half):
+    cur_flat, coeffs = bytes(cur_flat), bytes(coeffs)
+    if len(cur_flat) != m * length * es or len(coeffs) % es:
+        raise ZsError(-2, "binius values: buffer sizes")
+    idx = np.ascontiguousarray(indices, dtype=np.uint32)
+    off = np.ascontiguousarray(offsets, dtype=np.uint32)
+    if off.size != len(coeffs) // es + 1:
+        raise ZsError(-2, "binius values: offsets")
+    out = ctypes.create_string_buffer((dmax + 1) * es)
+    check(fn(cur_flat, length, m, coeffs, len(coeffs) // es, idx.ctypes.data_as(u32p), idx.size,
+             off.ctypes.data_as(u32p), dmax, half, out, None), fn.__name__)
+    return out.raw
+
+
+def _bind_binius():
+    L = lib()
+    if not getattr(L, "_binius_bound", False):
+        sz, cp, vp = ctypes.c_size_t, ctypes.c_char_p, ctypes.c_void_p
+        for fn in (L.zs_binius_sumcheck_values_gf256, L.zs_binius_sumcheck_values_gf128):
+            fn.argtypes = [cp, sz, sz, cp, sz, u32p, sz, u32p, sz, sz, cp, vp]
+        L.zs_binius_sumcheck_values_device.argtypes = [ctypes.c_uint32, vp, sz, sz, cp, sz, u32p, sz, u32p, sz, sz,
+                                                       vp, vp]
+        L.zs_binius_sumcheck_fold_device.argtypes = [ctypes.c_uint32, vp, sz, sz, cp, vp, vp, vp]
+        L.zs_binius_sumcheck_prove_combination.argtypes = [ctypes.c_uint32, cp, sz, sz, cp, sz, u32p, sz, u32p, cp,
+                                                           sz, ctypes.c_int32, cp, cp, vp]
+        L._binius_bound = True
+    return L
+
+
+def binius_terms(terms, es):
+    """[(factor table indices, coefficient int)] -> (coefficient bytes, indices, offsets)."""
+    coeffs = b"".join(int(c).to_bytes(es, "little") for _, c in terms)
+    idx = np.array([f for fs, _ in terms for f in fs], dtype=np.uint32)
+    off = np.zeros(len(terms) + 1, dtype=np.uint32)
+    off[1:] = np.cumsum([len(fs) for fs, _ in terms])
+    return coeffs, idx, off
+
+
+def binius_values_device(field_bits, d_cur, length, m, terms, dmax, half, d_out, stream=None):
+    """zs_binius_sumcheck_values_device on device tables (pointers as ints); asynchronous."""
+    es = 1 if field_bits == 8 else 16
+    coeffs, idx, off = binius_terms(terms, es)
+    L = _bind_binius()
+    check(L.zs_binius_sumcheck_values_device(field_bits, d_cur, length, m, coeffs, len(terms),
+                                             idx.ctypes.data_as(u32p), idx.size, off.ctypes.data_as(u32p), dmax,
+                                             half, d_out, stream), "zs_binius_sumcheck_values_device")
+
+
+def binius_fold_device(field_bits, d_cur, length, m, r, d_next, d_scratch=None, stream=None):
+    """zs_binius_sumcheck_fold_device: d_next = the fold of d_cur at r (an int)."""
+    es = 1 if field_bits == 8 else 16
+    L = _bind_binius()
+    check(L.zs_binius_sumcheck_fold_device(field_bits, d_cur, length, m, int(r).to_bytes(es, "little"), d_next,
+                                           d_scratch, stream), "zs_binius_sumcheck_fold_device")
+
+
+def binius_prove_combination(field_bits, tables, k, m, terms, seed=None, stream=None):
+    """Sumcheck(F).proveCombination (src/binius/sumcheck.zig:208-395) on the device:
+    tables = m tables of 2^k elements (bytes, little-endian; 1 byte per element for
+    field_bits 8, 16 for 128); terms = [(factor indices, coefficient int)]; seed = bytes
+    for proveSeeded's transcript. Returns (claimed sum bytes, rounds bytes)."""
+    es = 1 if field_bits == 8 else 16
+    coeffs, idx, off = binius_terms(terms, es)
+    dmax = max((len(fs) for fs, _ in terms), default=0)
+    claimed = ctypes.create_string_buffer(es)
+    rounds = ctypes.create_string_buffer(max(1, k * (dmax + 1) * es))
+    sd = b"" if seed is None else bytes(seed)
+    L = _bind_binius()
+    check(L.zs_binius_sumcheck_prove_combination(field_bits, bytes(tables), k, m, coeffs, len(terms),
+                                                 idx.ctypes.data_as(u32p), idx.size, off.ctypes.data_as(u32p), sd,
+                                                 len(sd), int(seed is not None), claimed, rounds, stream),
+          "zs_binius_sumcheck_prove_combination")
+    return claimed.raw, rounds.raw[:k * (dmax + 1) * es]
+
+
+def binius_gf256_values(cur_flat, length, m, coeffs, indices, offsets, dmax, half):
+    """accel.Gf256ValuesFn (src/binius/accel.zig:9-26): one sum-check round's values[t],
+    t = 0..dmax, over GF(2^8) (zs_binius_sumcheck_values_gf256). cur_flat holds m tables
+    of `length` bytes; term k has coefficient coeffs[k] and the factor tables
+    indices[offsets[k]:offsets[k + 1]]. Returns dmax + 1 bytes."""
+    L = _bind_binius()
+    return _binius_values(L.zs_binius_sumcheck_values_gf256, 1, cur_flat, length, m, coeffs, indices, offsets,
+                          dmax, half)
+
+
+def binius_gf128_values(cur_flat, length, m, coeffs, indices, offsets, dmax, half):
+    """accel.Gf128ValuesFn (src/binius/accel.zig:43-47): as binius_gf256_values over
+    GF(2^128), every element 16 little-endian bytes. Returns (dmax + 1) * 16 bytes."""
+    L = _bind_binius()
+    return _binius_values(L.zs_binius_sumcheck_values_gf128, 16, cur_flat, length, m, coeffs, indices, offsets,
+                          dmax, half)
