@@ -38,6 +38,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--log-rows", type=int, default=LOG_ROWS, help="smaller cases for profiling")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-binius", action="store_true", help="skip the Binius sum-check figures")
     ap.add_argument("--no-proofs", action="store_true",
                     help="skip the proof workloads and the reference-kernel bar after the commit step")
     ap.add_argument("--workload", default="commit", choices=["commit", "prove", "batch", "serve"],
@@ -557,6 +558,122 @@ def reference_gpu_bar(n_cols=64):
                     "twiddles, allocations and copies"}
 
 
+SC_TERMS = [([0, 1, 2], 1), ([0], 2)]  # src/cuda/sumcheck_test.zig:40-43: t0 t1 t2 + 2 t0
+
+
+def _sc_lookups_per_row(bits, terms, dmax):
+    """GF(2^8) table lookups the round kernel makes per row for `terms` (its own
+    arithmetic: a GF(2^128) product is 121 lookups, a subfield scalar times a GF(2^128)
+    element 16, a GF(2^8) product 1; the points 0 and 1 need none for the linear factor,
+    a unit coefficient none, a GF(2^8) coefficient of a GF(2^128) term 16)."""
+    mul, scal = (1, 1) if bits == 8 else (121, 16)
+    total = 0
+    for fs, c in terms:
+        if not fs:
+            continue
+        for t in range(dmax + 1):
+            total += (scal if t >= 2 else 0) * len(fs) + mul * (len(fs) - 1)
+            if c != 1:
+                total += mul if (bits == 8 or c >= 256) else scal
+    return total
+
+
+def binius_metrics(clock_mhz):
+    """The Binius sum-check (src/binius/sumcheck.zig; its GPU hook src/binius/accel.zig),
+    three tables and the terms of src/cuda/sumcheck_test.zig, seeded random elements:
+    one round's values on tables resident in device memory (a CUDA graph of 20 rounds,
+    CUDA events), the hook with host tables (copies included), and the whole combination
+    prover; beside the reference's own kernels (src/cuda/kernels/sumcheck.cu built for
+    sm_100a, driven as src/cuda/sumcheck_gpu.zig does: copies per call, one thread per
+    row) and the oracle's single-threaded CPU prover at a smaller size. The round kernel
+    is bound by shared-memory table lookups: its roofline is lookups per second against
+    one lookup per lane per cycle on every SM."""
+    import numpy as np
+    import torch
+    from zs_b200 import native
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    import ref_gpu
+    idx, off = [0, 1, 2, 0], [0, 3, 4]
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    out = {"terms": "t0 t1 t2 + 2 t0 over 3 tables (src/cuda/sumcheck_test.zig:40-43)", "dmax": 3}
+    for bits, k, k_cpu in ((8, 24, 16), (128, 20, 10)):
+        es = 1 if bits == 8 else 16
+        n = 1 << k
+        rng = np.random.default_rng(0x5EED0100 + bits)
+        tables = rng.bytes(3 * n * es)
+        coeffs = b"".join(c.to_bytes(es, "little") for _, c in SC_TERMS)
+        hook = native.binius_gf256_values if bits == 8 else native.binius_gf128_values
+        d_cur = torch.frombuffer(bytearray(tables), dtype=torch.uint8).cuda()
+        d_out = torch.zeros(64, dtype=torch.uint8, device="cuda")
+        s = torch.cuda.Stream()
+        call = lambda: native.binius_values_device(bits, d_cur.data_ptr(), n, 3, SC_TERMS, 3, n // 2,  # noqa: E731
+                                                   d_out.data_ptr(), s.cuda_stream)
+        with torch.cuda.stream(s):
+            call()
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        reps = 20
+        with torch.cuda.graph(g, stream=s):
+            for _ in range(reps):
+                call()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        for _ in range(3):
+            g.replay()
+        torch.cuda.synchronize()
+        dev = []
+        for _ in range(3):
+            ev[0].record(s)
+            with torch.cuda.stream(s):
+                g.replay()
+            ev[1].record(s)
+            torch.cuda.synchronize()
+            dev.append(ev[0].elapsed_time(ev[1]) / reps)
+        dev_ms = min(dev)
+        got = hook(tables, n, 3, coeffs, idx, off, 3, n // 2)
+        hook_ms = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            hook(tables, n, 3, coeffs, idx, off, 3, n // 2)
+            hook_ms.append((time.perf_counter() - t0) * 1e3)
+        per_row = _sc_lookups_per_row(bits, SC_TERMS, 3)
+        achieved = (n // 2) * per_row / (dev_ms * 1e-3)
+        peak = sms * 32 * clock_mhz * 1e6
+        r = {"rows": n, "round_device_ms": dev_ms, "round_rows_per_s": n / (dev_ms * 1e-3),
+             "hook_ms": min(hook_ms), "hook_h2d_bytes": 3 * n * es,
+             "roofline": {"bound": "shared-memory lookups", "lookups_per_row_pair": per_row,
+                          "achieved": achieved, "peak": peak, "unit": "lookups/s", "frac": achieved / peak,
+                          "peak_basis": f"{sms} SMs x 32 lanes x {clock_mhz:.0f} MHz"}}
+        if ref_gpu.sumcheck_available():
+            ref_gpu.sumcheck_values(bits == 128, tables, n, 3, coeffs, idx, off, 3, n // 2)
+            runs = [ref_gpu.sumcheck_values(bits == 128, tables, n, 3, coeffs, idx, off, 3, n // 2) for _ in range(2)]
+            r["reference_kernel_device_ms"] = min(x[2] for x in runs)
+            r["reference_hook_ms"] = min(x[1] for x in runs)
+            r["reference_values_equal"] = all(x[0] == got for x in runs)
+            r["round_speedup_vs_reference_kernel"] = r["reference_kernel_device_ms"] / dev_ms
+        else:
+            r["reference_kernel"] = "unavailable: oracle/_ref not built (the reference tree was absent)"
+        native.binius_prove_combination(bits, tables, k, 3, SC_TERMS)
+        pm = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            native.binius_prove_combination(bits, tables, k, 3, SC_TERMS)
+            pm.append((time.perf_counter() - t0) * 1e3)
+        r["prove_ms"] = min(pm)
+        small = rng.bytes(3 * (1 << k_cpu) * es)
+        t0 = time.perf_counter()
+        want = oracle.binius_prove(7 if bits == 128 else 3, small, k_cpu, 3, SC_TERMS)
+        cpu_ms = (time.perf_counter() - t0) * 1e3
+        t0 = time.perf_counter()
+        mine = native.binius_prove_combination(bits, small, k_cpu, 3, SC_TERMS)
+        r[f"prove_2^{k_cpu}_ms"] = (time.perf_counter() - t0) * 1e3
+        r[f"cpu_oracle_prove_2^{k_cpu}_ms"] = cpu_ms
+        r[f"prove_2^{k_cpu}_equal_oracle"] = mine == want
+        out[f"gf2^{bits}"] = r
+        del d_cur, g
+    return out
+
+
 def main():
     args = parse()
     # the reference arm runs on the host cores only: its ranks meet over gloo
@@ -723,6 +840,8 @@ def main():
         except Exception as e:  # the bar is reported, never required
             line["reference_gpu_circle_fft"] = {"unavailable": f"{type(e).__name__}: {e}"}
         line["proofs"] = proof_metrics(args, local)
+    if world == 1 and log_rows == LOG_ROWS and not args.no_binius:
+        line["binius_sumcheck"] = binius_metrics(cs.get("sm_mhz") or 1965.0)
     if rank == 0:
         print(json.dumps(line), flush=True)
     barrier(world)

@@ -50,7 +50,7 @@ constexpr uint32_t kMaxTerms = 256, kMaxFactors = 1024, kMaxPoint = 255, kMaxTab
 constexpr uint32_t kProveMaxPoints = 64;  // sumcheck.zig:243 (dmax + 1 <= 64)
 constexpr int kRegPoints = 8;             // dmax < kRegPoints: every point in registers
 
-// ---- host: tower arithmetic ------------------------------------------------------
+// ---- host: the GF(2^8) product table ---------------------------------------------
 
 uint32_t tower_mul_small(unsigned level, uint32_t a, uint32_t b) {  // level <= 3
   if (level == 0) return a & b & 1u;
@@ -63,7 +63,63 @@ uint32_t tower_mul_small(unsigned level, uint32_t a, uint32_t b) {  // level <= 
   return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ tower_mul_small(level - 1, c1, beta)) << half);
 }
 
-// Levels 3..7 over the GF(2^8) product table; inverses by the norm to the subfield:
+// ---- tower arithmetic over a GF(2^8) product table (host and device) ----------
+
+struct g128 {
+  uint64_t lo, hi;
+};
+ZS_HD g128 gxor(const g128& a, const g128& b) { return {a.lo ^ b.lo, a.hi ^ b.hi}; }
+
+struct Tower {
+  // T[(a << 8) | b] = a * b in GF(2^8): shared memory on the device. A constant operand
+  // goes first: its row is fixed and the variable operand spreads the lanes of a warp
+  // over the banks (a constant second operand puts every lane in one bank).
+  const uint8_t* T;
+  ZS_HD uint32_t m8(uint32_t a, uint32_t b) const { return T[(a << 8) | b]; }
+  // x * X_3 at level 4 (x * 0x100), from x = e0 + e1 X_3: e1 + (e0 + e1 X_2) X_3
+  ZS_HD uint32_t a16(uint32_t x) const {
+    const uint32_t e0 = x & 0xff, e1 = x >> 8;
+    return e1 | ((e0 ^ m8(0x10, e1)) << 8);
+  }
+  ZS_HD uint32_t m16(uint32_t a, uint32_t b) const {
+    const uint32_t a0 = a & 0xff, a1 = a >> 8, b0 = b & 0xff, b1 = b >> 8;
+    const uint32_t c0 = m8(a0, b0), c1 = m8(a1, b1), c2 = m8(a0 ^ a1, b0 ^ b1);
+    return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ m8(0x10, c1)) << 8);
+  }
+  ZS_HD uint32_t a32(uint32_t x) const {
+    const uint32_t e0 = x & 0xffff, e1 = x >> 16;
+    return e1 | ((e0 ^ a16(e1)) << 16);
+  }
+  ZS_HD uint32_t m32(uint32_t a, uint32_t b) const {
+    const uint32_t a0 = a & 0xffff, a1 = a >> 16, b0 = b & 0xffff, b1 = b >> 16;
+    const uint32_t c0 = m16(a0, b0), c1 = m16(a1, b1), c2 = m16(a0 ^ a1, b0 ^ b1);
+    return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ a16(c1)) << 16);
+  }
+  ZS_HD uint64_t a64(uint64_t x) const {
+    const uint32_t e0 = (uint32_t)x, e1 = (uint32_t)(x >> 32);
+    return (uint64_t)e1 | ((uint64_t)(e0 ^ a32(e1)) << 32);
+  }
+  ZS_HD uint64_t m64(uint64_t a, uint64_t b) const {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    const uint32_t c0 = m32(a0, b0), c1 = m32(a1, b1), c2 = m32(a0 ^ a1, b0 ^ b1);
+    return (uint64_t)(c0 ^ c1) | ((uint64_t)(c2 ^ c0 ^ c1 ^ a32(c1)) << 32);
+  }
+  // level 7: beta = X_5, the root of level 6
+  ZS_HD g128 m128(const g128& a, const g128& b) const {
+    const uint64_t c0 = m64(a.lo, b.lo), c1 = m64(a.hi, b.hi), c2 = m64(a.lo ^ a.hi, b.lo ^ b.hi);
+    return {c0 ^ c1, c2 ^ c0 ^ c1 ^ a64(c1)};
+  }
+  // s * x for a GF(2^8) scalar s: every byte coordinate of x times s
+  ZS_HD uint64_t s64(uint32_t s, uint64_t x) const {
+    uint64_t r = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) r |= (uint64_t)m8(s, (uint32_t)(x >> (8 * k)) & 0xff) << (8 * k);
+    return r;
+  }
+  ZS_HD g128 s128(uint32_t s, const g128& x) const { return {s64(s, x.lo), s64(s, x.hi)}; }
+};
+
+// Levels 3..7 on the host over the GF(2^8) product table; inverses by the norm to the subfield:
 // for a = a0 + a1 y with y^2 = beta y + 1, a (a0 + a1 beta + a1 y) = a0^2 + a0 a1 beta + a1^2.
 struct HostTower {
   std::vector<uint8_t> T, I;
@@ -76,12 +132,17 @@ struct HostTower {
   }
   static u128 beta(unsigned level) { return (u128)1 << (1u << (level - 2)); }
   u128 mul(unsigned level, u128 a, u128 b) const {
-    if (level == 3) return T[((uint32_t)a << 8) | (uint32_t)b];
-    const unsigned half = 1u << (level - 1);
-    const u128 mask = ((u128)1 << half) - 1;
-    const u128 a0 = a & mask, a1 = a >> half, b0 = b & mask, b1 = b >> half;
-    const u128 c0 = mul(level - 1, a0, b0), c1 = mul(level - 1, a1, b1), c2 = mul(level - 1, a0 ^ a1, b0 ^ b1);
-    return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ mul(level - 1, c1, beta(level))) << half);
+    const Tower F{T.data()};
+    switch (level) {
+      case 3: return F.m8((uint32_t)a, (uint32_t)b);
+      case 4: return F.m16((uint32_t)a, (uint32_t)b);
+      case 5: return F.m32((uint32_t)a, (uint32_t)b);
+      case 6: return F.m64((uint64_t)a, (uint64_t)b);
+      default: {
+        const g128 p = F.m128({(uint64_t)a, (uint64_t)(a >> 64)}, {(uint64_t)b, (uint64_t)(b >> 64)});
+        return (u128)p.hi << 64 | p.lo;
+      }
+    }
   }
   u128 inv(unsigned level, u128 a) const {
     if (level == 3) return I[(uint32_t)a];
@@ -185,84 +246,16 @@ class Sha256 {
   uint64_t total_;
 };
 
-// ---- device: the GF(2^8) table, tower arithmetic over it ---------------------------
+// ---- device: the product table and the kernels -----------------------------------
 
-std::mutex g_table_mu;
-uint8_t* g_tables[64] = {};
-
-const uint8_t* product_table(cudaStream_t st) {
-  int dev = 0;
-  ZS_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) throw Error(ZS_EDEVICE, "device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_table_mu);
-  if (!g_tables[dev]) {
-    const HostTower& ht = host_tower();
-    uint8_t* d = nullptr;
-    ZS_CUDA(cudaMalloc(&d, 65536));
-    ZS_CUDA(cudaMemcpyAsync(d, ht.T.data(), 65536, cudaMemcpyHostToDevice, st));
-    ZS_CUDA(cudaStreamSynchronize(st));
-    g_tables[dev] = d;
-  }
-  return g_tables[dev];
-}
-
-struct g128 {
-  uint64_t lo, hi;
-};
-__device__ __forceinline__ g128 gxor(const g128& a, const g128& b) { return {a.lo ^ b.lo, a.hi ^ b.hi}; }
-
-struct Tower {
-  const uint8_t* T;  // shared memory, T[(a << 8) | b] = a * b in GF(2^8)
-  __device__ __forceinline__ uint32_t m8(uint32_t a, uint32_t b) const { return T[(a << 8) | b]; }
-  // x * X_3 at level 4 (x * 0x100), from x = e0 + e1 X_3: e1 + (e0 + e1 X_2) X_3
-  __device__ __forceinline__ uint32_t a16(uint32_t x) const {
-    const uint32_t e0 = x & 0xff, e1 = x >> 8;
-    return e1 | ((e0 ^ m8(e1, 0x10)) << 8);
-  }
-  __device__ __forceinline__ uint32_t m16(uint32_t a, uint32_t b) const {
-    const uint32_t a0 = a & 0xff, a1 = a >> 8, b0 = b & 0xff, b1 = b >> 8;
-    const uint32_t c0 = m8(a0, b0), c1 = m8(a1, b1), c2 = m8(a0 ^ a1, b0 ^ b1);
-    return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ m8(c1, 0x10)) << 8);
-  }
-  __device__ __forceinline__ uint32_t a32(uint32_t x) const {
-    const uint32_t e0 = x & 0xffff, e1 = x >> 16;
-    return e1 | ((e0 ^ a16(e1)) << 16);
-  }
-  __device__ __forceinline__ uint32_t m32(uint32_t a, uint32_t b) const {
-    const uint32_t a0 = a & 0xffff, a1 = a >> 16, b0 = b & 0xffff, b1 = b >> 16;
-    const uint32_t c0 = m16(a0, b0), c1 = m16(a1, b1), c2 = m16(a0 ^ a1, b0 ^ b1);
-    return (c0 ^ c1) | ((c2 ^ c0 ^ c1 ^ a16(c1)) << 16);
-  }
-  __device__ __forceinline__ uint64_t a64(uint64_t x) const {
-    const uint32_t e0 = (uint32_t)x, e1 = (uint32_t)(x >> 32);
-    return (uint64_t)e1 | ((uint64_t)(e0 ^ a32(e1)) << 32);
-  }
-  __device__ __forceinline__ uint64_t m64(uint64_t a, uint64_t b) const {
-    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
-    const uint32_t c0 = m32(a0, b0), c1 = m32(a1, b1), c2 = m32(a0 ^ a1, b0 ^ b1);
-    return (uint64_t)(c0 ^ c1) | ((uint64_t)(c2 ^ c0 ^ c1 ^ a32(c1)) << 32);
-  }
-  // level 7: beta = X_5, the root of level 6
-  __device__ __forceinline__ g128 m128(const g128& a, const g128& b) const {
-    const uint64_t c0 = m64(a.lo, b.lo), c1 = m64(a.hi, b.hi), c2 = m64(a.lo ^ a.hi, b.lo ^ b.hi);
-    return {c0 ^ c1, c2 ^ c0 ^ c1 ^ a64(c1)};
-  }
-  // s * x for a GF(2^8) scalar s: every byte coordinate of x times s
-  __device__ __forceinline__ uint64_t s64(uint32_t s, uint64_t x) const {
-    uint64_t r = 0;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) r |= (uint64_t)m8(s, (uint32_t)(x >> (8 * k)) & 0xff) << (8 * k);
-    return r;
-  }
-  __device__ __forceinline__ g128 s128(uint32_t s, const g128& x) const { return {s64(s, x.lo), s64(s, x.hi)}; }
-};
-
-// One round's term list, passed by value: coefficient k at coef[es k ..], its factor tables
-// idx[off[k] .. off[k + 1]).
+// One round's term list, passed by value: term k multiplies coefficient k (coef[es k ..];
+// kind[k]: 0 = the unit, 1 = an element of the GF(2^8) subfield, 2 = any other) by its
+// factor tables idx[off[k] .. off[k + 1]).
 struct Terms {
   uint32_t nterms;
   uint32_t off[kMaxTerms + 1];
   uint16_t idx[kMaxFactors];
+  uint8_t kind[kMaxTerms];
   alignas(16) uint8_t coef[16 * kMaxTerms];
 };
 
@@ -279,6 +272,13 @@ __device__ __forceinline__ void warp_xor_into(uint32_t v, uint32_t* acc) {
   if ((threadIdx.x & 31) == 0 && v) atomicXor(acc, v);
 }
 
+__device__ __forceinline__ void warp_xor_into128(const g128& v, uint32_t* acc) {
+  warp_xor_into((uint32_t)v.lo, acc);
+  warp_xor_into((uint32_t)(v.lo >> 32), acc + 1);
+  warp_xor_into((uint32_t)v.hi, acc + 2);
+  warp_xor_into((uint32_t)(v.hi >> 32), acc + 3);
+}
+
 // The point t's linear factor a + t (a + b): a at t = 0, b at t = 1.
 template <int t>
 __device__ __forceinline__ uint32_t at_point8(const Tower& F, uint32_t a, uint32_t b) {
@@ -293,11 +293,26 @@ __device__ __forceinline__ g128 at_point128(const Tower& F, const g128& a, const
   else return gxor(a, F.s128(t, gxor(a, b)));
 }
 
+// prod[t] = (first factor at t), then prod[t] *= (next factor at t), for t < D.
+template <int D, int t = 0>
+__device__ __forceinline__ void first8(const Tower& F, uint32_t (&prod)[D], uint32_t a, uint32_t b) {
+  if constexpr (t < D) {
+    prod[t] = at_point8<t>(F, a, b);
+    first8<D, t + 1>(F, prod, a, b);
+  }
+}
 template <int D, int t = 0>
 __device__ __forceinline__ void factor8(const Tower& F, uint32_t (&prod)[D], uint32_t a, uint32_t b) {
   if constexpr (t < D) {
     prod[t] = F.m8(prod[t], at_point8<t>(F, a, b));
     factor8<D, t + 1>(F, prod, a, b);
+  }
+}
+template <int D, int t = 0>
+__device__ __forceinline__ void first128(const Tower& F, g128 (&prod)[D], const g128& a, const g128& b) {
+  if constexpr (t < D) {
+    prod[t] = at_point128<t>(F, a, b);
+    first128<D, t + 1>(F, prod, a, b);
   }
 }
 template <int D, int t = 0>
@@ -308,8 +323,15 @@ __device__ __forceinline__ void factor128(const Tower& F, g128 (&prod)[D], const
   }
 }
 
-// GF(2^8) round. D > 0: the D = dmax + 1 points in registers; D = 0: one point per pass.
-// out: (dmax + 1) bytes packed four to a word (little-endian: byte t is values[t]).
+// coefficient * v by the coefficient's kind: v itself, 16 subfield lookups, or a full product
+__device__ __forceinline__ g128 times_coef(const Tower& F, uint32_t kind, const g128& c, const g128& v) {
+  return kind == 0 ? v : kind == 1 ? F.s128((uint32_t)c.lo, v) : F.m128(c, v);
+}
+
+// GF(2^8) round; out: (dmax + 1) bytes packed four to a word (little-endian: byte t is
+// values[t]). D > 0: the D = dmax + 1 points in registers, every row once. D = 0: one
+// point per pass, points t = blockIdx.y, blockIdx.y + gridDim.y, ... (a grid of dmax + 1
+// rows of CTAs gives each point its own CTAs when the rows alone cannot fill the GPU).
 template <int D>
 __global__ void __launch_bounds__(kBThreads) k_values8(const uint8_t* __restrict__ cur, uint32_t len, uint32_t half,
                                                        uint32_t dmax, const __grid_constant__ Terms tm,
@@ -324,34 +346,66 @@ __global__ void __launch_bounds__(kBThreads) k_values8(const uint8_t* __restrict
   const Tower F{s_T};
   const uint32_t stride = gridDim.x * blockDim.x, first = blockIdx.x * blockDim.x + threadIdx.x;
   if constexpr (D > 0) {
+    // kRows rows per thread and pass, their loads issued together (the byte loads are
+    // latency-bound otherwise); a row past the end loads zeros, whose products are zero
+    constexpr int kRows = 4;
     uint32_t acc[D];
 #pragma unroll
     for (int t = 0; t < D; ++t) acc[t] = 0;
-    for (uint32_t rest = first; rest < half; rest += stride) {
-      for (uint32_t k = 0; k < tm.nterms; ++k) {
-        uint32_t prod[D];
+    for (uint32_t base = first; base < half; base += kRows * stride) {
+      uint32_t valid = 0;
 #pragma unroll
-        for (int t = 0; t < D; ++t) prod[t] = tm.coef[k];
-        for (uint32_t j = tm.off[k]; j < tm.off[k + 1]; ++j) {
-          const uint8_t* c = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
-          factor8<D>(F, prod, c[0], c[1]);
+      for (int r = 0; r < kRows; ++r) valid += base + r * stride < half;
+      for (uint32_t k = 0; k < tm.nterms; ++k) {
+        const uint32_t j0 = tm.off[k], j1 = tm.off[k + 1], c = tm.coef[k];
+        if (j0 == j1) {
+#pragma unroll
+          for (int t = 0; t < D; ++t) acc[t] ^= (valid & 1) ? c : 0;
+          continue;
+        }
+        uint32_t a[kRows], b[kRows], prod[kRows][D];
+        auto load = [&](uint32_t j) {
+          const uint8_t* col = cur + (size_t)tm.idx[j] * len;
+#pragma unroll
+          for (int r = 0; r < kRows; ++r) {
+            const uint32_t row = base + r * stride;
+            a[r] = row < half ? col[2 * (size_t)row] : 0;
+            b[r] = row < half ? col[2 * (size_t)row + 1] : 0;
+          }
+        };
+        load(j0);
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+          first8<D>(F, prod[r], a[r], b[r]);
+          if (tm.kind[k] != 0) {
+#pragma unroll
+            for (int t = 0; t < D; ++t) prod[r][t] = F.m8(c, prod[r][t]);
+          }
+        }
+        for (uint32_t j = j0 + 1; j < j1; ++j) {
+          load(j);
+#pragma unroll
+          for (int r = 0; r < kRows; ++r) factor8<D>(F, prod[r], a[r], b[r]);
         }
 #pragma unroll
-        for (int t = 0; t < D; ++t) acc[t] ^= prod[t];
+        for (int r = 0; r < kRows; ++r)
+#pragma unroll
+          for (int t = 0; t < D; ++t) acc[t] ^= prod[r][t];
       }
     }
 #pragma unroll
     for (int t = 0; t < D; ++t) warp_xor_into(acc[t] << (8 * (t & 3)), s_acc + (t >> 2));
   } else {
-    for (uint32_t t = 0; t <= dmax; ++t) {
+    for (uint32_t t = blockIdx.y; t <= dmax; t += gridDim.y) {
       uint32_t acc = 0;
       for (uint32_t rest = first; rest < half; rest += stride) {
         for (uint32_t k = 0; k < tm.nterms; ++k) {
+          const uint32_t j0 = tm.off[k], j1 = tm.off[k + 1];
           uint32_t prod = tm.coef[k];
-          for (uint32_t j = tm.off[k]; j < tm.off[k + 1]; ++j) {
-            const uint8_t* c = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
-            const uint32_t a = c[0];
-            prod = F.m8(prod, a ^ F.m8(t, a ^ c[1]));
+          for (uint32_t j = j0; j < j1; ++j) {
+            const uint8_t* p = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
+            const uint32_t a = p[0], v = a ^ F.m8(t, a ^ p[1]);
+            prod = (j == j0 && tm.kind[k] == 0) ? v : F.m8(prod, v);
           }
           acc ^= prod;
         }
@@ -364,14 +418,12 @@ __global__ void __launch_bounds__(kBThreads) k_values8(const uint8_t* __restrict
     if (s_acc[k]) atomicXor(out + k, s_acc[k]);
 }
 
-__device__ __forceinline__ void warp_xor_into128(const g128& v, uint32_t* acc) {
-  warp_xor_into((uint32_t)v.lo, acc);
-  warp_xor_into((uint32_t)(v.lo >> 32), acc + 1);
-  warp_xor_into((uint32_t)v.hi, acc + 2);
-  warp_xor_into((uint32_t)(v.hi >> 32), acc + 3);
+__device__ __forceinline__ g128 load_g128(const uint4* p) {
+  const uint4 v = *p;
+  return {(uint64_t)v.y << 32 | v.x, (uint64_t)v.w << 32 | v.z};
 }
 
-// GF(2^128) round; out: (dmax + 1) values of four little-endian words.
+// GF(2^128) round; out: (dmax + 1) values of four little-endian words. D as k_values8.
 template <int D>
 __global__ void __launch_bounds__(kBThreads) k_values128(const uint4* __restrict__ cur, uint32_t len, uint32_t half,
                                                          uint32_t dmax, const __grid_constant__ Terms tm,
@@ -389,20 +441,29 @@ __global__ void __launch_bounds__(kBThreads) k_values128(const uint4* __restrict
     const uint64_t* cf = reinterpret_cast<const uint64_t*>(tm.coef + 16 * k);
     return g128{cf[0], cf[1]};
   };
-  auto elem = [&](const uint4* p) { return g128{(uint64_t)p->y << 32 | p->x, (uint64_t)p->w << 32 | p->z}; };
   if constexpr (D > 0) {
     g128 acc[D];
 #pragma unroll
     for (int t = 0; t < D; ++t) acc[t] = {0, 0};
     for (uint32_t rest = first; rest < half; rest += stride) {
       for (uint32_t k = 0; k < tm.nterms; ++k) {
-        g128 prod[D];
-        const g128 c0 = coef(k);
+        const uint32_t j0 = tm.off[k], j1 = tm.off[k + 1], kind = tm.kind[k];
+        const g128 c = coef(k);
+        if (j0 == j1) {
 #pragma unroll
-        for (int t = 0; t < D; ++t) prod[t] = c0;
-        for (uint32_t j = tm.off[k]; j < tm.off[k + 1]; ++j) {
-          const uint4* c = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
-          factor128<D>(F, prod, elem(c), elem(c + 1));
+          for (int t = 0; t < D; ++t) acc[t] = gxor(acc[t], c);
+          continue;
+        }
+        g128 prod[D];
+        const uint4* p = cur + (size_t)tm.idx[j0] * len + 2 * (size_t)rest;
+        first128<D>(F, prod, load_g128(p), load_g128(p + 1));
+        if (kind != 0) {
+#pragma unroll
+          for (int t = 0; t < D; ++t) prod[t] = times_coef(F, kind, c, prod[t]);
+        }
+        for (uint32_t j = j0 + 1; j < j1; ++j) {
+          p = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
+          factor128<D>(F, prod, load_g128(p), load_g128(p + 1));
         }
 #pragma unroll
         for (int t = 0; t < D; ++t) acc[t] = gxor(acc[t], prod[t]);
@@ -411,15 +472,17 @@ __global__ void __launch_bounds__(kBThreads) k_values128(const uint4* __restrict
 #pragma unroll
     for (int t = 0; t < D; ++t) warp_xor_into128(acc[t], s_acc + 4 * t);
   } else {
-    for (uint32_t t = 0; t <= dmax; ++t) {
+    for (uint32_t t = blockIdx.y; t <= dmax; t += gridDim.y) {
       g128 acc{0, 0};
       for (uint32_t rest = first; rest < half; rest += stride) {
         for (uint32_t k = 0; k < tm.nterms; ++k) {
-          g128 prod = coef(k);
-          for (uint32_t j = tm.off[k]; j < tm.off[k + 1]; ++j) {
-            const uint4* c = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
-            const g128 a = elem(c), b = elem(c + 1);
-            prod = F.m128(prod, gxor(a, F.s128(t, gxor(a, b))));
+          const uint32_t j0 = tm.off[k], j1 = tm.off[k + 1], kind = tm.kind[k];
+          const g128 c = coef(k);
+          g128 prod = c;
+          for (uint32_t j = j0; j < j1; ++j) {
+            const uint4* p = cur + (size_t)tm.idx[j] * len + 2 * (size_t)rest;
+            const g128 a = load_g128(p), v = gxor(a, F.s128(t, gxor(a, load_g128(p + 1))));
+            prod = j == j0 ? times_coef(F, kind, c, v) : F.m128(prod, v);
           }
           acc = gxor(acc, prod);
         }
@@ -502,7 +565,13 @@ Terms pack_terms(bool wide, size_t m, const uint8_t* coeffs, size_t nterms, cons
     if (indices[j] >= m) throw Error(ZS_EMALFORMED, "factor table out of range");
     tm.idx[j] = (uint16_t)indices[j];
   }
-  std::memcpy(tm.coef, coeffs, nterms * (wide ? 16 : 1));
+  const size_t es = wide ? 16 : 1;
+  std::memcpy(tm.coef, coeffs, nterms * es);
+  for (size_t k = 0; k < nterms; ++k) {
+    bool high_zero = true;  // the coefficient lies in GF(2^8)
+    for (size_t b = 1; b < es; ++b) high_zero = high_zero && coeffs[es * k + b] == 0;
+    tm.kind[k] = high_zero && coeffs[es * k] == 1 ? 0 : (wide && high_zero ? 1 : 2);
+  }
   return tm;
 }
 
@@ -511,63 +580,85 @@ void check_rows(size_t len, size_t half, size_t dmax) {
   if (dmax > kMaxPoint) throw Error(ZS_EMALFORMED, "more than 256 points");
 }
 
-int sm_count() {
-  int dev = 0, sms = 0;
+// The values kernels by point count (index D, 0 = one point per pass) and the shared
+// memory they are launched with at most: the table and the largest accumulator.
+const void* const kValues8[kRegPoints + 1] = {
+    (const void*)k_values8<0>, (const void*)k_values8<1>, (const void*)k_values8<2>,
+    (const void*)k_values8<3>, (const void*)k_values8<4>, (const void*)k_values8<5>,
+    (const void*)k_values8<6>, (const void*)k_values8<7>, (const void*)k_values8<8>};
+const void* const kValues128[kRegPoints + 1] = {
+    (const void*)k_values128<0>, (const void*)k_values128<1>, (const void*)k_values128<2>,
+    (const void*)k_values128<3>, (const void*)k_values128<4>, (const void*)k_values128<5>,
+    (const void*)k_values128<6>, (const void*)k_values128<7>, (const void*)k_values128<8>};
+constexpr size_t kValuesSmem = 65536 + 16 * (kMaxPoint + 1);
+
+// Per device, set up on first use: the product table, the SM count, the kernels' shared
+// memory limits and how many CTAs of each fit on an SM.
+struct DeviceState {
+  uint8_t* table = nullptr;
+  int sms = 0;
+  int per_sm8[kRegPoints + 1] = {}, per_sm128[kRegPoints + 1] = {};
+};
+std::mutex g_dev_mu;
+DeviceState g_dev[64];
+
+const DeviceState& device_state(cudaStream_t st) {
+  int dev = 0;
   ZS_CUDA(cudaGetDevice(&dev));
-  ZS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  return sms;
+  if (dev < 0 || dev >= 64) throw Error(ZS_EDEVICE, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  DeviceState& d = g_dev[dev];
+  if (!d.table) {
+    ZS_CUDA(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    for (int D = 0; D <= kRegPoints; ++D) {
+      for (int w = 0; w < 2; ++w) {
+        const void* fn = w ? kValues128[D] : kValues8[D];
+        int* per_sm = w ? &d.per_sm128[D] : &d.per_sm8[D];
+        ZS_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kValuesSmem));
+        ZS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, fn, kBThreads, kValuesSmem));
+        *per_sm = std::max(*per_sm, 1);
+      }
+    }
+    ZS_CUDA(cudaFuncSetAttribute(k_mul_table128, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
+    ZS_CUDA(cudaFuncSetAttribute(k_fold128, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
+    uint8_t* t = nullptr;
+    ZS_CUDA(cudaMalloc(&t, 65536));
+    ZS_CUDA(cudaMemcpyAsync(t, host_tower().T.data(), 65536, cudaMemcpyHostToDevice, st));
+    ZS_CUDA(cudaStreamSynchronize(st));
+    d.table = t;
+  }
+  return d;
 }
 
-// Zeroes d_out and accumulates one round's values into it, asynchronously on `st`.
+// Zeroes d_out and accumulates one round's values into it, asynchronously on `st`. With
+// enough rows to give every SM a CTA, each thread takes all points of its rows (up to
+// eight; one point per pass beyond that); with fewer rows, the points get CTAs of their
+// own (a grid of dmax + 1 rows), so that small rounds still spread over the GPU.
 void values_async(bool wide, const void* d_cur, size_t len, size_t half, size_t dmax, const Terms& tm, void* d_out,
                   cudaStream_t st) {
   const size_t words = wide ? 4 * (dmax + 1) : (dmax + 4) / 4;
   ZS_CUDA(cudaMemsetAsync(d_out, 0, words * 4, st));
   if (half == 0) return;
-  const uint8_t* T = product_table(st);
-  const size_t smem = 65536 + 4 * words;
-  const size_t want = (half + kBThreads - 1) / kBThreads;
-  const int sms = sm_count();
-  uint32_t* out = static_cast<uint32_t*>(d_out);
-  const uint32_t L = (uint32_t)len, H = (uint32_t)half, M = (uint32_t)dmax;
-  // one wave: as many CTAs as fit on every SM (shared memory and registers), fewer for
-  // small tables
-#define ZS_VALUES_CASE(KERN, PTR, DD)                                                                  \
-  do {                                                                                                 \
-    ZS_CUDA(cudaFuncSetAttribute(KERN<DD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));   \
-    int per_sm = 1;                                                                                    \
-    ZS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KERN<DD>, kBThreads, smem));        \
-    const uint32_t blocks = (uint32_t)std::min<size_t>(want, (size_t)sms * std::max(per_sm, 1));       \
-    KERN<DD><<<blocks, kBThreads, smem, st>>>(static_cast<PTR>(d_cur), L, H, M, tm, T, out);          \
-  } while (0)
+  const DeviceState& ds = device_state(st);
   const int D = dmax + 1 <= (size_t)kRegPoints ? (int)dmax + 1 : 0;
-  if (wide) {
-    switch (D) {
-      case 1: ZS_VALUES_CASE(k_values128, const uint4*, 1); break;
-      case 2: ZS_VALUES_CASE(k_values128, const uint4*, 2); break;
-      case 3: ZS_VALUES_CASE(k_values128, const uint4*, 3); break;
-      case 4: ZS_VALUES_CASE(k_values128, const uint4*, 4); break;
-      case 5: ZS_VALUES_CASE(k_values128, const uint4*, 5); break;
-      case 6: ZS_VALUES_CASE(k_values128, const uint4*, 6); break;
-      case 7: ZS_VALUES_CASE(k_values128, const uint4*, 7); break;
-      case 8: ZS_VALUES_CASE(k_values128, const uint4*, 8); break;
-      default: ZS_VALUES_CASE(k_values128, const uint4*, 0); break;
-    }
+  const size_t row_blocks = (half + kBThreads - 1) / kBThreads;
+  const bool per_row = D > 0 && row_blocks >= (size_t)ds.sms;
+  const int kd = per_row ? D : 0;
+  const size_t slots = (size_t)ds.sms * (wide ? ds.per_sm128[kd] : ds.per_sm8[kd]);
+  dim3 grid(1, 1);
+  if (per_row) {
+    grid.x = (unsigned)std::min(row_blocks, slots);
   } else {
-    switch (D) {
-      case 1: ZS_VALUES_CASE(k_values8, const uint8_t*, 1); break;
-      case 2: ZS_VALUES_CASE(k_values8, const uint8_t*, 2); break;
-      case 3: ZS_VALUES_CASE(k_values8, const uint8_t*, 3); break;
-      case 4: ZS_VALUES_CASE(k_values8, const uint8_t*, 4); break;
-      case 5: ZS_VALUES_CASE(k_values8, const uint8_t*, 5); break;
-      case 6: ZS_VALUES_CASE(k_values8, const uint8_t*, 6); break;
-      case 7: ZS_VALUES_CASE(k_values8, const uint8_t*, 7); break;
-      case 8: ZS_VALUES_CASE(k_values8, const uint8_t*, 8); break;
-      default: ZS_VALUES_CASE(k_values8, const uint8_t*, 0); break;
-    }
+    grid.y = (unsigned)(dmax + 1);
+    grid.x = (unsigned)std::min(row_blocks, std::max<size_t>(1, (slots + dmax) / (dmax + 1)));
   }
-#undef ZS_VALUES_CASE
-  ZS_CUDA(cudaGetLastError());
+  const void* cur = d_cur;
+  uint32_t L = (uint32_t)len, H = (uint32_t)half, M = (uint32_t)dmax;
+  const uint8_t* T = ds.table;
+  uint32_t* out = static_cast<uint32_t*>(d_out);
+  void* args[] = {&cur, &L, &H, &M, const_cast<Terms*>(&tm), &T, &out};
+  ZS_CUDA(cudaLaunchKernel(wide ? kValues128[kd] : kValues8[kd], grid, dim3(kBThreads), args, 65536 + 4 * words,
+                           st));
 }
 
 // next (m tables of len / 2) = fold of cur (m tables of len) at r, asynchronously on `st`.
@@ -576,17 +667,15 @@ void fold_async(bool wide, const void* d_cur, size_t len, size_t m, u128 r, void
                 cudaStream_t st) {
   const size_t half = len / 2;
   if (half == 0) return;
-  const uint8_t* T = product_table(st);
+  const DeviceState& ds = device_state(st);
   const uint32_t bx = (uint32_t)std::min<size_t>((half + kBThreads - 1) / kBThreads,
-                                                 std::max<size_t>(1, (size_t)sm_count() * 8 / m));
+                                                 std::max<size_t>(1, (size_t)ds.sms * 8 / m));
   const dim3 grid(bx, (unsigned)m);
   if (!wide) {
     k_fold8<<<grid, kBThreads, 0, st>>>(static_cast<const uint8_t*>(d_cur), (uint32_t)len, (uint32_t)half,
-                                        (uint32_t)r, T, static_cast<uint8_t*>(d_next));
+                                        (uint32_t)r, ds.table, static_cast<uint8_t*>(d_next));
   } else {
-    ZS_CUDA(cudaFuncSetAttribute(k_mul_table128, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
-    k_mul_table128<<<4096 / kBThreads, kBThreads, 65536, st>>>((uint64_t)r, (uint64_t)(r >> 64), T, r_mul);
-    ZS_CUDA(cudaFuncSetAttribute(k_fold128, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
+    k_mul_table128<<<4096 / kBThreads, kBThreads, 65536, st>>>((uint64_t)r, (uint64_t)(r >> 64), ds.table, r_mul);
     k_fold128<<<grid, kBThreads, 65536, st>>>(static_cast<const uint4*>(d_cur), (uint32_t)len, (uint32_t)half,
                                               r_mul, static_cast<uint4*>(d_next));
   }
@@ -655,27 +744,38 @@ void store_elem(uint8_t* p, size_t es, u128 v) {
   for (size_t i = 0; i < es; ++i) p[i] = (uint8_t)(v >> (8 * i));
 }
 
-// Lagrange interpolation through the points 0..n-1 (sumcheck.zig:124-162): low-first
-// coefficients. The denominators depend on the points only and come precomputed.
-std::vector<u128> interpolate(const HostTower& ht, unsigned level, const std::vector<u128>& values,
-                              const std::vector<u128>& inv_denom) {
-  const size_t n = values.size();
-  std::vector<u128> coeffs(n, 0), basis(n + 1), next(n + 1);
+// Lagrange interpolation through the points 0..n-1 (sumcheck.zig:124-162) as a matrix:
+// row i holds the low-first coefficients of prod_{j != i} (x + j) / (i + j), so a round's
+// coefficients are coeffs[d] = sum_i values[i] * lag[i][d]. The matrix depends on the
+// points only and is built once per proof.
+std::vector<std::vector<u128>> lagrange_matrix(const HostTower& ht, unsigned level, size_t n) {
+  std::vector<std::vector<u128>> lag(n, std::vector<u128>(n, 0));
   for (size_t i = 0; i < n; ++i) {
-    basis[0] = 1;
-    size_t deg = 1;
+    std::vector<u128> basis{1};
+    u128 denom = 1;
     for (size_t j = 0; j < n; ++j) {
       if (j == i) continue;
-      for (size_t d = 0; d <= deg; ++d) {  // basis *= (x + j)
-        const u128 lo = d == 0 ? 0 : basis[d - 1], hi = d == deg ? 0 : basis[d];
-        next[d] = lo ^ ht.mul(level, (u128)j, hi);
+      std::vector<u128> next(basis.size() + 1, 0);  // basis * (x + j)
+      for (size_t d = 0; d < basis.size(); ++d) {
+        next[d + 1] ^= basis[d];
+        next[d] ^= ht.mul(level, (u128)j, basis[d]);
       }
-      std::copy(next.begin(), next.begin() + deg + 1, basis.begin());
-      ++deg;
+      basis.swap(next);
+      denom = ht.mul(level, denom, (u128)(i ^ j));
     }
-    const u128 scale = ht.mul(level, inv_denom[i], values[i]);
-    for (size_t d = 0; d < deg; ++d) coeffs[d] ^= ht.mul(level, basis[d], scale);
+    const u128 inv = ht.inv(level, denom);
+    for (size_t d = 0; d < n; ++d) lag[i][d] = ht.mul(level, basis[d], inv);
   }
+  return lag;
+}
+
+std::vector<u128> interpolate(const HostTower& ht, unsigned level, const std::vector<u128>& values,
+                              const std::vector<std::vector<u128>>& lag) {
+  const size_t n = values.size();
+  std::vector<u128> coeffs(n, 0);
+  for (size_t i = 0; i < n; ++i)
+    if (values[i])
+      for (size_t d = 0; d < n; ++d) coeffs[d] ^= ht.mul(level, values[i], lag[i][d]);
   return coeffs;
 }
 
@@ -732,23 +832,15 @@ int32_t prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k, 
       return;
     }
 
-    // 1 / prod_{j != i} (i + j) for the points 0..dmax
-    std::vector<u128> inv_denom(dmax + 1);
-    for (size_t i = 0; i <= dmax; ++i) {
-      u128 d = 1;
-      for (size_t j = 0; j <= dmax; ++j)
-        if (j != i) d = ht.mul(level, d, (u128)(i ^ j));
-      inv_denom[i] = ht.inv(level, d);
-    }
+    const std::vector<std::vector<u128>> lag = lagrange_matrix(ht, level, dmax + 1);
 
     cudaStream_t st = (cudaStream_t)stream;
+    retain_pool_memory();
     const size_t words = wide ? 4 * (dmax + 1) : (dmax + 4) / 4;
     DevMem<uint4> d_a((m * n * es + 15) / 16, st), d_b((m * (n / 2) * es + 15) / 16, st);
     DevMem<uint32_t> d_vals(words, st);
     DevMem<uint4> d_rmul(wide ? 4096 : 0, st);
-    uint32_t* h_vals = nullptr;
-    ZS_CUDA(cudaMallocHost((void**)&h_vals, words * 4));
-    std::unique_ptr<uint32_t, decltype(&cudaFreeHost)> h_guard(h_vals, &cudaFreeHost);
+    std::vector<uint32_t> h_vals(words);
     ZS_CUDA(cudaMemcpyAsync(d_a.p, tables, m * n * es, cudaMemcpyHostToDevice, st));
 
     void* cur = d_a.p;
@@ -758,16 +850,16 @@ int32_t prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k, 
     for (size_t i = 0; i < k; ++i) {
       const size_t half = len / 2;
       values_async(wide, cur, len, half, dmax, tm, d_vals.p, st);
-      ZS_CUDA(cudaMemcpyAsync(h_vals, d_vals.p, words * 4, cudaMemcpyDeviceToHost, st));
+      ZS_CUDA(cudaMemcpyAsync(h_vals.data(), d_vals.p, words * 4, cudaMemcpyDeviceToHost, st));
       ZS_CUDA(cudaStreamSynchronize(st));
-      const uint8_t* vb = reinterpret_cast<const uint8_t*>(h_vals);
+      const uint8_t* vb = reinterpret_cast<const uint8_t*>(h_vals.data());
       for (size_t t = 0; t <= dmax; ++t) values[t] = load_elem(vb + es * t, es);
       if (i == 0) {  // the hypercube sum: g over the even rows plus g over the odd rows
         const u128 h = values[0] ^ (dmax >= 1 ? values[1] : values[0]);
         store_elem(claimed_out, es, h);
         start(h);
       }
-      const std::vector<u128> cs = interpolate(ht, level, values, inv_denom);
+      const std::vector<u128> cs = interpolate(ht, level, values, lag);
       for (size_t t = 0; t <= dmax; ++t) store_elem(rounds_out + es * ((dmax + 1) * i + t), es, cs[t]);
       const u128 r = absorb(cs);
       if (i + 1 < k) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -43,6 +44,26 @@ ZS_HD uint32_t bitrev(uint32_t x, unsigned bits) {
   for (unsigned b = 0; b < bits; ++b) r |= ((x >> b) & 1u) << (bits - 1 - b);
   return r;
 #endif
+}
+
+// Freed blocks stay in the device's stream-ordered pool instead of going back to the
+// driver at every synchronization, so repeated proofs do not map their memory again.
+inline void retain_pool_memory() {
+  static std::mutex mu;
+  static uint64_t done = 0;
+  int dev = 0;
+  ZS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 64 && (done >> dev & 1)) return;
+  cudaMemPool_t pool;
+  ZS_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t keep = UINT64_MAX;
+  ZS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  // A block freed on one prover's stream is reused by another only once the free has
+  // completed: the pool never makes one proof's stream wait on another's.
+  int no = 0;
+  ZS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+  if (dev < 64) done |= 1ull << dev;
 }
 
 }  // namespace zs

@@ -530,26 +530,6 @@ constexpr size_t kPriorityUpload = (size_t)64 << 20;  // wire bytes from which u
 constexpr size_t kGroupMin = (size_t)8 << 20;    // wire bytes below which one group suffices
 constexpr size_t kGroupBytes = (size_t)16 << 20;  // wire bytes per upload group
 
-// Freed blocks stay in the device's stream-ordered pool instead of going back to the
-// driver at every synchronization, so repeated proofs do not map their memory again.
-void retain_pool_memory() {
-  static std::mutex mu;
-  static uint64_t done = 0;
-  int dev = 0;
-  ZS_CUDA(cudaGetDevice(&dev));
-  std::lock_guard<std::mutex> lk(mu);
-  if (dev < 64 && (done >> dev & 1)) return;
-  cudaMemPool_t pool;
-  ZS_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
-  uint64_t keep = UINT64_MAX;
-  ZS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
-  // A block freed on one prover's stream is reused by another only once the free has
-  // completed: the pool never makes one proof's stream wait on another's.
-  int no = 0;
-  ZS_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no));
-  if (dev < 64) done |= 1ull << dev;
-}
-
 }  // namespace
 
 std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_t params_len, const uint8_t* pi,
