@@ -597,6 +597,7 @@ def binius_metrics(clock_mhz):
     idx, off = [0, 1, 2, 0], [0, 3, 4]
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     out = {"terms": "t0 t1 t2 + 2 t0 over 3 tables (src/cuda/sumcheck_test.zig:40-43)", "dmax": 3}
+    wavefronts = {8: 2.70, 128: 2.86}
     for bits, k, k_cpu in ((8, 24, 16), (128, 20, 10)):
         es = 1 if bits == 8 else 16
         n = 1 << k
@@ -632,7 +633,7 @@ def binius_metrics(clock_mhz):
         dev_ms = min(dev)
         got = hook(tables, n, 3, coeffs, idx, off, 3, n // 2)
         hook_ms = []
-        for _ in range(3):
+        for _ in range(3):  # pageable host tables, as the reference's hook receives them
             t0 = time.perf_counter()
             hook(tables, n, 3, coeffs, idx, off, 3, n // 2)
             hook_ms.append((time.perf_counter() - t0) * 1e3)
@@ -643,7 +644,11 @@ def binius_metrics(clock_mhz):
              "hook_ms": min(hook_ms), "hook_h2d_bytes": 3 * n * es,
              "roofline": {"bound": "shared-memory lookups", "lookups_per_row_pair": per_row,
                           "achieved": achieved, "peak": peak, "unit": "lookups/s", "frac": achieved / peak,
-                          "peak_basis": f"{sms} SMs x 32 lanes x {clock_mhz:.0f} MHz"}}
+                          "peak_basis": f"{sms} SMs x 32 lanes x {clock_mhz:.0f} MHz",
+                          # shared-memory wavefronts per warp lookup at random addresses,
+                          # from the committed capture (profiles/binius_sumcheck_round.md)
+                          "wavefronts_per_lookup": wavefronts[bits],
+                          "frac_of_bank_conflict_ceiling": achieved / peak * wavefronts[bits]}}
         if ref_gpu.sumcheck_available():
             ref_gpu.sumcheck_values(bits == 128, tables, n, 3, coeffs, idx, off, 3, n // 2)
             runs = [ref_gpu.sumcheck_values(bits == 128, tables, n, 3, coeffs, idx, off, 3, n // 2) for _ in range(2)]
@@ -653,13 +658,22 @@ def binius_metrics(clock_mhz):
             r["round_speedup_vs_reference_kernel"] = r["reference_kernel_device_ms"] / dev_ms
         else:
             r["reference_kernel"] = "unavailable: oracle/_ref not built (the reference tree was absent)"
-        native.binius_prove_combination(bits, tables, k, 3, SC_TERMS)
-        pm = []
-        for _ in range(2):
-            t0 = time.perf_counter()
-            native.binius_prove_combination(bits, tables, k, 3, SC_TERMS)
-            pm.append((time.perf_counter() - t0) * 1e3)
-        r["prove_ms"] = min(pm)
+        pinned = torch.frombuffer(bytearray(tables), dtype=torch.uint8).pin_memory()
+
+        def best_ms(fn, reps=3):
+            fn()
+            ts = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                fn()
+                ts.append((time.perf_counter() - t0) * 1e3)
+            return min(ts)
+
+        r["hook_pinned_ms"] = best_ms(lambda: hook(pinned, n, 3, coeffs, idx, off, 3, n // 2))
+        # the whole proof from host tables: k rounds, every round's values and fold on the device
+        r["prove_ms"] = best_ms(lambda: native.binius_prove_combination(bits, pinned, k, 3, SC_TERMS))
+        r["prove_pageable_ms"] = best_ms(lambda: native.binius_prove_combination(bits, tables, k, 3, SC_TERMS))
+        r["prove_input"] = "prove_ms: tables in pinned host memory; prove_pageable_ms: a Python bytes object"
         small = rng.bytes(3 * (1 << k_cpu) * es)
         t0 = time.perf_counter()
         want = oracle.binius_prove(7 if bits == 128 else 3, small, k_cpu, 3, SC_TERMS)

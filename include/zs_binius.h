@@ -65,10 +65,11 @@ int32_t zs_binius_sumcheck_values_device(uint32_t field_bits, const void *d_cur,
 int32_t zs_binius_sumcheck_fold_device(uint32_t field_bits, const void *d_cur, size_t len, size_t m,
                                        const uint8_t *r, void *d_next, void *d_scratch, void *stream);
 
-/* Sumcheck(F).proveCombination (src/binius/sumcheck.zig:208-395), or proveSeeded's
- * transcript when has_seed is set: m tables of 2^k elements (host memory, m * 2^k
- * element sizes), copied to the device once; every round's values and fold run on the
- * device, the interpolation and the SHA-256 transcript on the host.
+/* Sumcheck(F).proveCombination (src/binius/sumcheck.zig:208-395) with its optional
+ * transcript seed (Transcript.initBytes(seed) when has_seed is set, else
+ * Transcript.init(claimed sum)): m tables of 2^k elements (host memory, m * 2^k element
+ * sizes), copied to the device once; every round's values and fold run on the device,
+ * the interpolation and the SHA-256 transcript on the host.
  * claimed_out: one element (the hypercube sum). rounds_out: k * (dmax + 1) elements, round
  * i's low-first coefficients at i * (dmax + 1), dmax = the longest term (dmax + 1 <= 64).
  * Synchronous. */

@@ -372,7 +372,7 @@ bool binius_inputs(unsigned level, const uint8_t* tables, size_t len, size_t m, 
 }
 }  // namespace
 
-// Sumcheck(F).proveCombination (proveSeeded's transcript when has_seed): claimed_out one
+// Sumcheck(F).proveCombination (with its optional transcript seed when has_seed): claimed_out one
 // element, rounds_out k * (dmax + 1) elements.
 int orc_binius_prove(unsigned level, const uint8_t* tables, size_t k, size_t m, const uint8_t* coeffs, size_t nterms,
                      const uint32_t* indices, size_t n_indices, const uint32_t* offsets, const uint8_t* seed,

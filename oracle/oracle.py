@@ -359,7 +359,7 @@ def _terms(terms, es):
 
 
 def binius_prove(level, tables: bytes, k, m, terms, seed=None):
-    """Sumcheck(F).proveCombination (proveSeeded's transcript when seed is bytes) over
+    """Sumcheck(F).proveCombination (its optional transcript seed when seed is bytes) over
     TowerField(level), level 3 or 7: tables = m tables of 2^k elements, little-endian.
     Returns (claimed bytes, rounds bytes: k * (dmax + 1) elements)."""
     es = 1 if level == 3 else 16

@@ -5,7 +5,7 @@ src/cuda/sumcheck_gpu.zig drives them).
 
 Covered: the values hook over GF(2^8) and GF(2^128) at the shapes of
 src/cuda/sumcheck_test.zig (three tables, terms t0 t1 t2 + 2 t0, k = 4..9 and 4..7) and
-beyond (2^20 rows, every point count 1..13 on both the register and the looped paths,
+beyond (2^20 rows, every point count 1..14 on both the register and the looped paths,
 empty terms, repeated factors, 256 terms and 1024 factors, half < len / 2, odd len,
 half = 0); the device-resident round and fold; the combination prover bit-exact with the
 oracle's proveCombination (plain and seeded transcripts, k = 0..10) and, at 2^20 rows,

@@ -5,9 +5,17 @@
 proves the same job `repeat` times through zs_m31_prove and prints the proof size and
 the wall time of each call. The job is `workload.proof_job(air, log_rows, seed, sep)`:
 blowup 4, 16 queries, remainder_log 3.
+
+    PYTHONPATH=zig-stark_b200 python -m zs_b200.cli --sumcheck gf8 --log-rows 22 --repeat 1
+
+runs one Binius sum-check round (the values hook, zs_binius_sumcheck_values_gf256 or
+_gf128) over three seeded tables of 2^log_rows elements with the terms t0 t1 t2 + 2 t0,
+`repeat` times, and prints the values and the wall time of each call.
 """
 import argparse
 import time
+
+import numpy as np
 
 from . import native
 from . import workload as wl
@@ -21,7 +29,19 @@ def main(argv=None):
     ap.add_argument("--log-rows", type=int, default=18)
     ap.add_argument("--repeat", type=int, default=2)
     ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--sumcheck", choices=["gf8", "gf128"], default=None)
     args = ap.parse_args(argv)
+    if args.sumcheck:
+        es = 1 if args.sumcheck == "gf8" else 16
+        hook = native.binius_gf256_values if es == 1 else native.binius_gf128_values
+        n = 1 << args.log_rows
+        tables = np.random.default_rng(args.seed).bytes(3 * n * es)
+        for i in range(args.repeat):
+            t0 = time.perf_counter()
+            vals = hook(tables, n, 3, bytes([1] + [0] * (es - 1) + [2] + [0] * (es - 1)), [0, 1, 2, 0], [0, 3, 4], 3,
+                        n // 2)
+            print(f"round {i}: {vals.hex()} in {1e3 * (time.perf_counter() - t0):.2f} ms", flush=True)
+        return
     air, params, pi, trace, sep, pre = wl.proof_job(AIRS[args.air], args.log_rows, args.seed, b"zig-stark:cli")
     for i in range(args.repeat):
         t0 = time.perf_counter()

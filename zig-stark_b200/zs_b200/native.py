@@ -550,16 +550,28 @@ class Server:
             pass
 
 
+def _host_buffer(buf):
+    """(pointer or bytes, size in bytes) of bytes-like host data or of a CPU tensor (pinned
+    memory makes the host-to-device copies direct)."""
+    if hasattr(buf, "data_ptr"):
+        if buf.is_cuda:
+            raise ZsError(-2, "binius: host tables expected")
+        return buf.data_ptr(), buf.numel() * buf.element_size()
+    buf = bytes(buf)
+    return buf, len(buf)
+
+
 def _binius_values(fn, es, cur_flat, length, m, coeffs, indices, offsets, dmax, half):
-    cur_flat, coeffs = bytes(cur_flat), bytes(coeffs)
-    if len(cur_flat) != m * length * es or len(coeffs) % es:
+    cur, size = _host_buffer(cur_flat)
+    coeffs = bytes(coeffs)
+    if size != m * length * es or len(coeffs) % es:
         raise ZsError(-2, "binius values: buffer sizes")
     idx = np.ascontiguousarray(indices, dtype=np.uint32)
     off = np.ascontiguousarray(offsets, dtype=np.uint32)
     if off.size != len(coeffs) // es + 1:
         raise ZsError(-2, "binius values: offsets")
     out = ctypes.create_string_buffer((dmax + 1) * es)
-    check(fn(cur_flat, length, m, coeffs, len(coeffs) // es, idx.ctypes.data_as(u32p), idx.size,
+    check(fn(cur, length, m, coeffs, len(coeffs) // es, idx.ctypes.data_as(u32p), idx.size,
              off.ctypes.data_as(u32p), dmax, half, out, None), fn.__name__)
     return out.raw
 
@@ -569,11 +581,11 @@ def _bind_binius():
     if not getattr(L, "_binius_bound", False):
         sz, cp, vp = ctypes.c_size_t, ctypes.c_char_p, ctypes.c_void_p
         for fn in (L.zs_binius_sumcheck_values_gf256, L.zs_binius_sumcheck_values_gf128):
-            fn.argtypes = [cp, sz, sz, cp, sz, u32p, sz, u32p, sz, sz, cp, vp]
+            fn.argtypes = [vp, sz, sz, cp, sz, u32p, sz, u32p, sz, sz, cp, vp]
         L.zs_binius_sumcheck_values_device.argtypes = [ctypes.c_uint32, vp, sz, sz, cp, sz, u32p, sz, u32p, sz, sz,
                                                        vp, vp]
         L.zs_binius_sumcheck_fold_device.argtypes = [ctypes.c_uint32, vp, sz, sz, cp, vp, vp, vp]
-        L.zs_binius_sumcheck_prove_combination.argtypes = [ctypes.c_uint32, cp, sz, sz, cp, sz, u32p, sz, u32p, cp,
+        L.zs_binius_sumcheck_prove_combination.argtypes = [ctypes.c_uint32, vp, sz, sz, cp, sz, u32p, sz, u32p, cp,
                                                            sz, ctypes.c_int32, cp, cp, vp]
         L._binius_bound = True
     return L
@@ -608,17 +620,20 @@ def binius_fold_device(field_bits, d_cur, length, m, r, d_next, d_scratch=None, 
 
 def binius_prove_combination(field_bits, tables, k, m, terms, seed=None, stream=None):
     """Sumcheck(F).proveCombination (src/binius/sumcheck.zig:208-395) on the device:
-    tables = m tables of 2^k elements (bytes, little-endian; 1 byte per element for
-    field_bits 8, 16 for 128); terms = [(factor indices, coefficient int)]; seed = bytes
-    for proveSeeded's transcript. Returns (claimed sum bytes, rounds bytes)."""
+    tables = m tables of 2^k elements (bytes or a CPU tensor, little-endian; 1 byte per
+    element for field_bits 8, 16 for 128); terms = [(factor indices, coefficient int)]; seed = bytes
+    for proveCombination's optional transcript seed. Returns (claimed sum bytes, rounds bytes)."""
     es = 1 if field_bits == 8 else 16
     coeffs, idx, off = binius_terms(terms, es)
     dmax = max((len(fs) for fs, _ in terms), default=0)
     claimed = ctypes.create_string_buffer(es)
     rounds = ctypes.create_string_buffer(max(1, k * (dmax + 1) * es))
     sd = b"" if seed is None else bytes(seed)
+    tab, size = _host_buffer(tables)
+    if size != m * (1 << k) * es:
+        raise ZsError(-2, "binius prove: table size")
     L = _bind_binius()
-    check(L.zs_binius_sumcheck_prove_combination(field_bits, bytes(tables), k, m, coeffs, len(terms),
+    check(L.zs_binius_sumcheck_prove_combination(field_bits, tab, k, m, coeffs, len(terms),
                                                  idx.ctypes.data_as(u32p), idx.size, off.ctypes.data_as(u32p), sd,
                                                  len(sd), int(seed is not None), claimed, rounds, stream),
           "zs_binius_sumcheck_prove_combination")
