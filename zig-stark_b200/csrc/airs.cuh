@@ -116,10 +116,14 @@ ZS_HD void air_eval(const AirConsts& k, const qm31& x, const qm31* cur, const qm
 // a table instead of raising every domain point to n/8. Same values as air_eval.
 ZS_HD void rescue_stacked_eval(const qm31* per, const qm31* cur, const qm31* next, qm31* out) {
   const qm31 z = per[0];
+  qm31 s5[4];  // t_l q_l = s_l^5, once per column
+#pragma unroll
+  for (int l = 0; l < 4; ++l) s5[l] = qmul(cur[8 + l], cur[4 + l]);
+#pragma unroll
   for (int j = 0; j < 4; ++j) {
-    qm31 expect = qzero();
-    for (int l = 0; l < 4; ++l) expect = qadd(expect, qmul_m(qmul(cur[8 + l], cur[4 + l]), rescue_mds(j, l)));
-    expect = qadd(expect, per[1 + j]);
+    qm31 expect = per[1 + j];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) expect = qadd(expect, qmul_m(s5[l], rescue_mds(j, l)));
     out[j] = qmul(z, qsub(next[j], expect));
     out[4 + j] = qsub(cur[4 + j], qmul(cur[j], cur[j]));
     out[8 + j] = qsub(cur[8 + j], qmul(cur[4 + j], cur[j]));

@@ -256,15 +256,9 @@ int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t* par
                      trace_len, channel_sep, channel_sep_len, out_proof, out_len);
     ensure_device();
     cudaStream_t st = nullptr;
-    ZS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    try {
-      prove_on(st, host, air_id, params, params_len, public_inputs, public_inputs_len, preprocessed,
-               preprocessed_len, trace, trace_len, channel_sep, channel_sep_len, out_proof, out_len);
-    } catch (...) {
-      cudaStreamDestroy(st);
-      throw;
-    }
-    cudaStreamDestroy(st);
+    thread_stream(0, &st);  // the calling thread's stream on the current device
+    prove_on(st, host, air_id, params, params_len, public_inputs, public_inputs_len, preprocessed, preprocessed_len,
+             trace, trace_len, channel_sep, channel_sep_len, out_proof, out_len);
   });
 }
 

@@ -66,4 +66,34 @@ inline void retain_pool_memory() {
   if (dev < 64) done |= 1ull << dev;
 }
 
+
+// Non-blocking streams owned by the calling thread, created on first use per device and
+// slot and kept for the thread's life (creating and destroying streams and events costs
+// tens of microseconds per proof otherwise). Slots: 0 the stream of a zs_m31_prove call,
+// 1 and 2 a proof's upload and tree side streams. `ev` is an event for the slot's use.
+struct ThreadStreams {
+  static constexpr int kDevices = 64, kSlots = 3;
+  cudaStream_t s[kDevices][kSlots] = {};
+  cudaEvent_t ev[kDevices][kSlots] = {};
+  ~ThreadStreams() {
+    for (int d = 0; d < kDevices; ++d)
+      for (int k = 0; k < kSlots; ++k) {
+        if (ev[d][k]) cudaEventDestroy(ev[d][k]);
+        if (s[d][k]) cudaStreamDestroy(s[d][k]);
+      }
+  }
+};
+inline void thread_stream(int slot, cudaStream_t* st, cudaEvent_t* ev = nullptr) {
+  static thread_local ThreadStreams ts;
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= ThreadStreams::kDevices || slot < 0 || slot >= ThreadStreams::kSlots)
+    throw Error(ZS_EDEVICE, "thread stream slot");
+  if (!ts.s[dev][slot]) {
+    cuda_check(cudaStreamCreateWithFlags(&ts.s[dev][slot], cudaStreamNonBlocking), "cudaStreamCreateWithFlags");
+    cuda_check(cudaEventCreateWithFlags(&ts.ev[dev][slot], cudaEventDisableTiming), "cudaEventCreateWithFlags");
+  }
+  *st = ts.s[dev][slot];
+  if (ev) *ev = ts.ev[dev][slot];
+}
 }  // namespace zs

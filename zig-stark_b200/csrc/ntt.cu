@@ -18,6 +18,7 @@
 // contiguous 2^11-element blocks plus passes of up to 11 stages over strided groups,
 // two stages per shared-memory round trip; results leave the CRT domain in the
 // finishing kernels.
+#include <algorithm>
 #include <vector>
 
 #include "ntt.cuh"
@@ -122,19 +123,27 @@ NttTables::~NttTables() {
 //        S0 + S1, t1 (S0 - S1), t2 (A + C), t3 (A - C)
 // the same values as the two radix-2 stages, by distributivity.
 template <bool DIF>
-__device__ __forceinline__ void ntt_radix4(qm31* s, unsigned M, uint32_t G, unsigned lo, unsigned logN, uint32_t l0,
-                                           unsigned b, const qm31* __restrict__ tw) {
+__device__ __forceinline__ void ntt_radix4(qm31* s, qm31* s_tw, unsigned M, uint32_t G, unsigned lo, unsigned logN,
+                                           uint32_t l0, unsigned b, const qm31* __restrict__ tw) {
   const uint32_t hb = 1u << b, total = G << M;
   const unsigned st = lo + 1 + b;
   const size_t half = (size_t)1 << (logN - 1);
+  // The stage pair's twiddle triples, (t1, t2, t3) for the G x 2^b distinct k, staged in
+  // shared memory first: the global loads are scattered (k << (logN - st - 1)), so all
+  // threads issue theirs at once instead of one dependent load per butterfly.
+  for (uint32_t e = threadIdx.x; e < (G << b); e += blockDim.x) {
+    const uint32_t k = ((e & (hb - 1)) << lo) | (l0 + (e >> b));
+    const size_t i2 = (size_t)k << (logN - st - 1), i3 = 3 * i2;
+    s_tw[3 * e] = ldq(tw + 2 * i2);
+    s_tw[3 * e + 1] = ldq(tw + i2);
+    s_tw[3 * e + 2] = i3 < half ? ldq(tw + i3) : crt_neg(ldq(tw + (i3 - half)));
+  }
+  __syncthreads();
   for (uint32_t q = threadIdx.x; q < (total >> 2); q += blockDim.x) {
     const uint32_t t = q >> (M - 2), r = q & ((1u << (M - 2)) - 1);
     const uint32_t m0 = ((r >> b) << (b + 2)) | (r & (hb - 1));
-    const uint32_t k = ((m0 & (hb - 1)) << lo) | (l0 + t);
-    const size_t i2 = (size_t)k << (logN - st - 1), i3 = 3 * i2;
-    const qm31 t1 = ldq(tw + 2 * i2);
-    const qm31 t2 = ldq(tw + i2);
-    const qm31 t3 = i3 < half ? ldq(tw + i3) : crt_neg(ldq(tw + (i3 - half)));
+    const uint32_t e = (t << b) | (r & (hb - 1));
+    const qm31 t1 = s_tw[3 * e], t2 = s_tw[3 * e + 1], t3 = s_tw[3 * e + 2];
     qm31* p = s + (t << M) + m0;
     const qm31 e0 = p[0], e1 = p[hb], e2 = p[2 * hb], e3 = p[3 * hb];
     if (!DIF) {
@@ -204,26 +213,37 @@ __global__ void k_to_crt_cols(const qm31* in, size_t in_stride, qm31* out, size_
 //   DIT (bit-reversed in, natural out), stages ascending:  x, y -> x + t y, x - t y;
 //   DIF (natural in, bit-reversed out), stages descending: x, y -> x + y, (x - y) t.
 // Local stages [b_lo, b_hi) run two at a time (four elements per thread in registers)
-// with a barrier per pair. `src`, when given, is read instead of `a` (QM31 values,
-// mapped into the CRT domain) and the pass writes `a`.
+// with a barrier per pair. Where the pass reads its input (`in_mode`): kInPlace `a`;
+// kToCrt QM31 values of `src` mapped into the CRT domain; kExpand `src[j >> expand]`, the
+// compact values whose 2^expand copies the first `expand` stages of a zero-padded DIT
+// would make. `to_qm31`: the pass leaves the CRT domain on its store (the last pass).
+enum InMode : unsigned { kInPlace = 0, kToCrt = 1, kExpand = 2 };
 template <bool DIF>
 __global__ void __launch_bounds__(kThreads) k_ntt_pass(qm31* a, size_t stride, const qm31* __restrict__ src,
-                                                       size_t src_stride, unsigned logN, unsigned lo, unsigned M,
+                                                       size_t src_stride, unsigned in_mode, unsigned expand,
+                                                       unsigned to_qm31, unsigned logN, unsigned lo, unsigned M,
                                                        unsigned G, unsigned b_lo, unsigned b_hi,
                                                        const qm31* __restrict__ tw) {
   extern __shared__ uint4 smem_raw[];
   qm31* s = reinterpret_cast<qm31*>(smem_raw);
+  qm31* s_tw = s + ((size_t)G << M);
   const uint32_t gpl = (1u << lo) / G;  // CTAs per hi value
   const uint32_t hi = blockIdx.x / gpl, l0 = (blockIdx.x % gpl) * G;
   const size_t off = ((size_t)hi << (lo + M)) + l0;
   qm31* col = a + (size_t)blockIdx.y * stride + off;
   const uint32_t total = G << M;
   const unsigned lg_g = 31 - __clz(G);
-  if (src) {
+  if (in_mode == kToCrt) {
     const qm31* in = src + (size_t)blockIdx.y * src_stride + off;
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
       const uint32_t t = idx & (G - 1), mid = idx >> lg_g;
       s[(t << M) + mid] = to_crt(ldq(in + ((size_t)mid << lo) + t));
+    }
+  } else if (in_mode == kExpand) {
+    const qm31* in = src + (size_t)blockIdx.y * src_stride;
+    for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), mid = idx >> lg_g;
+      s[(t << M) + mid] = ldq(in + ((off + ((size_t)mid << lo) + t) >> expand));
     }
   } else {
     for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
@@ -234,27 +254,18 @@ __global__ void __launch_bounds__(kThreads) k_ntt_pass(qm31* a, size_t stride, c
   __syncthreads();
   if (!DIF) {
     unsigned b = b_lo;
-    for (; b + 1 < b_hi; b += 2) ntt_radix4<false>(s, M, G, lo, logN, l0, b, tw);
+    for (; b + 1 < b_hi; b += 2) ntt_radix4<false>(s, s_tw, M, G, lo, logN, l0, b, tw);
     if (b < b_hi) ntt_radix2<false>(s, M, G, lo, logN, l0, b, tw);
   } else {
     int b = (int)b_hi - 1;
-    for (; b - 1 >= (int)b_lo; b -= 2) ntt_radix4<true>(s, M, G, lo, logN, l0, (unsigned)(b - 1), tw);
+    for (; b - 1 >= (int)b_lo; b -= 2) ntt_radix4<true>(s, s_tw, M, G, lo, logN, l0, (unsigned)(b - 1), tw);
     if (b >= (int)b_lo) ntt_radix2<true>(s, M, G, lo, logN, l0, (unsigned)b, tw);
   }
   for (uint32_t idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const uint32_t t = idx & (G - 1), mid = idx >> lg_g;
-    stq(col + ((size_t)mid << lo) + t, s[(t << M) + mid]);
+    const qm31 v = s[(t << M) + mid];
+    stq(col + ((size_t)mid << lo) + t, to_qm31 ? from_crt(v) : v);
   }
-}
-
-// x[i] = phi^-1(x[i]) * 2^shift (2^shift an M31 scalar: 1/n = 2^(31 - log n), or 1).
-__global__ void k_from_crt(qm31* a, size_t stride, uint32_t n, unsigned shift) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  qm31* p = a + (size_t)blockIdx.y * stride + i;
-  qm31 v = from_crt(ldq(p));
-  if (shift) v = qmake(mshl(v.a.a, shift), mshl(v.a.b, shift), mshl(v.b.a, shift), mshl(v.b.b, shift));
-  stq(p, v);
 }
 
 // The passes of a size-2^logN transform: one over contiguous 2^S-element blocks
@@ -282,25 +293,44 @@ static std::vector<PassPlan> plan_passes(unsigned logN) {
   return v;
 }
 
-template <bool DIF>
-static void launch_pass(qm31* a, size_t stride, const qm31* src, size_t src_stride, uint32_t C, unsigned logN,
-                        const PassPlan& p, unsigned b_lo, unsigned b_hi, const qm31* tw, cudaStream_t st) {
-  const size_t sb = ((size_t)p.G << p.M) * sizeof(qm31);
-  ZS_CUDA(cudaFuncSetAttribute(k_ntt_pass<DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 65536));
-  const uint32_t ctas = (1u << (logN - p.M)) / p.G;
-  k_ntt_pass<DIF><<<dim3(ctas, C), kThreads, sb, st>>>(a, stride, src, src_stride, logN, p.lo, p.M, p.G, b_lo, b_hi,
-                                                       tw);
+// Shared memory of a pass: its 2^M x G elements and the twiddle triples of its widest
+// stage pair (G x 2^(M-2) of them).
+static size_t pass_smem(const PassPlan& p) {
+  return (((size_t)p.G << p.M) + (p.M >= 2 ? (size_t)3 * (p.G << (p.M - 2)) : 0)) * sizeof(qm31);
 }
 
-// Forward DIT stages first..logN (bit-reversed input in `a`, natural output).
-static void dit_stages(qm31* a, size_t stride, uint32_t C, unsigned logN, const qm31* tw, cudaStream_t st,
-                       unsigned first) {
-  if (logN == 0 || first > logN) return;
-  for (const PassPlan& p : plan_passes(logN)) {
+template <bool DIF>
+static void launch_pass(qm31* a, size_t stride, const qm31* src, size_t src_stride, unsigned in_mode,
+                        unsigned expand, bool to_qm31, uint32_t C, unsigned logN, const PassPlan& p, unsigned b_lo,
+                        unsigned b_hi, const qm31* tw, cudaStream_t st) {
+  static const bool attr = [] {  // 64 KB of elements + 48 KB of twiddles at most (M = 11, G = 2)
+    ZS_CUDA(cudaFuncSetAttribute(k_ntt_pass<DIF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 114688));
+    return true;
+  }();
+  (void)attr;
+  const uint32_t ctas = (1u << (logN - p.M)) / p.G;
+  k_ntt_pass<DIF><<<dim3(ctas, C), kThreads, pass_smem(p), st>>>(a, stride, src, src_stride, in_mode, expand,
+                                                                 to_qm31 ? 1u : 0u, logN, p.lo, p.M, p.G, b_lo, b_hi,
+                                                                 tw);
+}
+
+// Forward DIT stages first..logN (natural output, QM31 values: the last pass leaves the
+// CRT domain). The first `first - 1` stages of the zero-padded input only copy: the
+// first pass reads the compact CRT-domain values `src` (value j at 2^(first-1) positions).
+static void dit_stages(qm31* a, size_t stride, const qm31* src, size_t src_stride, uint32_t C, unsigned logN,
+                       const qm31* tw, cudaStream_t st, unsigned first) {
+  if (logN == 0) throw Error(ZS_EGENERIC, "dit_stages: empty transform");
+  const std::vector<PassPlan> plan = plan_passes(logN);
+  bool first_pass = true;
+  for (size_t i = 0; i < plan.size(); ++i) {
+    const PassPlan& p = plan[i];
     const unsigned s_lo = p.lo + 1, s_hi = p.lo + p.M;  // global stages of this pass
-    if (s_hi < first) continue;
-    const unsigned b_lo = first > s_lo ? first - s_lo : 0;
-    launch_pass<false>(a, stride, nullptr, 0, C, logN, p, b_lo, p.M, tw, st);
+    if (s_hi < first && i + 1 < plan.size()) continue;
+    // (first > logN: every stage copies; the last pass only expands and leaves the CRT domain)
+    const unsigned b_lo = first > s_lo ? std::min(first - s_lo, p.M) : 0;
+    launch_pass<false>(a, stride, first_pass ? src : nullptr, src_stride, first_pass ? kExpand : kInPlace,
+                       first - 1, i + 1 == plan.size(), C, logN, p, b_lo, p.M, tw, st);
+    first_pass = false;
   }
   ZS_CUDA(cudaGetLastError());
 }
@@ -315,21 +345,23 @@ static void dif_all(const qm31* src, size_t src_stride, qm31* a, size_t stride, 
     return;
   }
   const std::vector<PassPlan> plan = plan_passes(logN);
-  for (size_t i = plan.size(); i-- > 0;)
-    launch_pass<true>(a, stride, i + 1 == plan.size() ? src : nullptr, src_stride, C, logN, plan[i], 0, plan[i].M,
-                      tw, st);
+  for (size_t i = plan.size(); i-- > 0;) {
+    const bool first = i + 1 == plan.size();
+    launch_pass<true>(a, stride, first ? src : nullptr, src_stride, first ? kToCrt : kInPlace, 0, false, C, logN,
+                      plan[i], 0, plan[i].M, tw, st);
+  }
   ZS_CUDA(cudaGetLastError());
 }
 
 // The inverse DIF leaves phi(n c_k) at position j = bitrev_n(k). For each j:
 // coeffs[c][j] = c_k (QM31, kept in bit-reversed order), and the forward input
-// phi(c_k offset^k) goes to position bitrev_N(k) = j << B of the size-N transform. That
-// input is zero elsewhere, so its first B stages only copy the value across the 2^B
-// block at j << B (each stage pairs a filled element with a zero one): the block is
-// written as 2^B copies and the forward transform starts at stage B + 1.
+// phi(c_k offset^k) belongs at position bitrev_N(k) = j << B of the size-N transform. That
+// input is zero elsewhere, so its first B stages only copy the value across the 2^B block
+// at j << B: the value goes to wbuf[c][j] once, and the forward transform's first pass
+// reads it for all 2^B positions and starts at stage B + 1.
 // offset_crt[j] = phi(offset^bitrev_n(j)) (bit-reversed, so every read is coalesced).
-__global__ void k_coeff_finish(qm31* coeffs, size_t c_stride, qm31* big, size_t b_stride, unsigned log_n,
-                               unsigned log_N, const qm31* __restrict__ offset_crt) {
+__global__ void k_coeff_finish(qm31* coeffs, size_t c_stride, qm31* wbuf, size_t w_stride, unsigned log_n,
+                               const qm31* __restrict__ offset_crt) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= (1u << log_n)) return;
   qm31* cp = coeffs + (size_t)blockIdx.y * c_stride + j;
@@ -337,29 +369,28 @@ __global__ void k_coeff_finish(qm31* coeffs, size_t c_stride, qm31* big, size_t 
   const unsigned sh = (31 - log_n) % 31;
   v = qmake(mshl(v.a.a, sh), mshl(v.a.b, sh), mshl(v.b.a, sh), mshl(v.b.b, sh));
   stq(cp, from_crt(v));
-  const qm31 w = crt_mul(v, ldq(offset_crt + j));
-  const unsigned B = log_N - log_n;
-  qm31* dst = big + (size_t)blockIdx.y * b_stride + ((size_t)j << B);
-  for (uint32_t r = 0; r < (1u << B); ++r) stq(dst + r, w);
+  stq(wbuf + (size_t)blockIdx.y * w_stride + j, crt_mul(v, ldq(offset_crt + j)));
 }
 
 void lde_qm31(const qm31* values, size_t v_stride, qm31* coeffs, size_t c_stride, qm31* codeword, size_t w_stride,
               uint32_t C, const NttTables& small, const NttTables& big, const qm31* offset_pows, cudaStream_t st) {
   const unsigned log_n = small.log_n, log_N = big.log_n;
-  const uint32_t n = 1u << log_n, N = 1u << log_N;
+  const uint32_t n = 1u << log_n;
+  if (log_N == 0) throw Error(ZS_EMALFORMED, "LDE onto a domain of one point");
   // inverse transform on H: natural-order values in, bit-reversed CRT-domain n c_k out
   dif_all(values, v_stride, coeffs, c_stride, C, log_n, small.inv_crt, st);
-  // scale by 1/n, leave the CRT domain for the coefficients, and fill the forward
-  // input after its first log_N - log_n stages
-  qm31* off_crt = nullptr;
+  // scale by 1/n, leave the CRT domain for the coefficients, and keep the forward
+  // input compact for the forward transform's first pass
+  qm31 *off_crt = nullptr, *wbuf = nullptr;
   ZS_CUDA(cudaMallocAsync((void**)&off_crt, (size_t)n * sizeof(qm31), st));
+  ZS_CUDA(cudaMallocAsync((void**)&wbuf, (size_t)C * n * sizeof(qm31), st));
   k_to_crt_brev<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(offset_pows, off_crt, log_n);
-  k_coeff_finish<<<dim3((n + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(coeffs, c_stride, codeword, w_stride,
-                                                                              log_n, log_N, off_crt);
-  ZS_CUDA(cudaFreeAsync(off_crt, st));
-  dit_stages(codeword, w_stride, C, log_N, big.fwd_crt, st, log_N - log_n + 1);
-  k_from_crt<<<dim3((N + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(codeword, w_stride, N, 0);
+  k_coeff_finish<<<dim3((n + kThreads - 1) / kThreads, C), kThreads, 0, st>>>(coeffs, c_stride, wbuf, n, log_n,
+                                                                              off_crt);
   ZS_CUDA(cudaGetLastError());
+  dit_stages(codeword, w_stride, wbuf, n, C, log_N, big.fwd_crt, st, log_N - log_n + 1);
+  ZS_CUDA(cudaFreeAsync(wbuf, st));
+  ZS_CUDA(cudaFreeAsync(off_crt, st));
 }
 
 }  // namespace zs

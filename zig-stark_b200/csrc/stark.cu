@@ -95,6 +95,79 @@ __global__ void __launch_bounds__(kT) k_quotient(const qm31* __restrict__ cw, qm
   stq(q + i, qmul(h, ldq(zh_tab + 2 * (size_t)zi + 1)));
 }
 
+// The stacked Rescue AIR's quotient (12 columns, 12 transitions, boundaries on columns
+// 0..3 at rows 0 and n - 1, no lookups) with every column index fixed at compile time, so
+// the row stays in registers (the generic kernel's run-time indices put its column
+// arrays in local memory). The boundary sum is taken per point p_g as
+// sum_j c_gj f_j(x) - e_g, with c_gj = sum_{b: p_b = p_g, col_b = j} beta_b and
+// e_g = sum_{b: p_b = p_g} beta_b v_b formed on the host: equal in the field to the
+// generic sum_b beta_b (f_col_b(x) - v_b), term by term.
+struct RescueQuot {
+  qm31 alphas[12];
+  qm31 bc[2][4];  // c_gj
+  qm31 be[2];     // e_g
+  qm31 bp[2];     // p_g
+};
+
+__global__ void __launch_bounds__(kT) k_quotient_rescue(const qm31* __restrict__ cw, qm31* __restrict__ q,
+                                                        const qm31* __restrict__ wpow,
+                                                        const QuotConsts* __restrict__ kp,
+                                                        const __grid_constant__ RescueQuot rq,
+                                                        const qm31* __restrict__ zh_tab,
+                                                        const qm31* __restrict__ per_tab) {
+  const QuotConsts& k = *kp;
+  const uint32_t N = 1u << k.log_N;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const uint32_t in = (i + k.shift) & (N - 1);
+  qm31 cur[12], next[4], per[5], res[12];
+#pragma unroll
+  for (int j = 0; j < 12; ++j) cur[j] = ldq(cw + (size_t)j * N + i);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) next[j] = ldq(cw + (size_t)j * N + in);
+#pragma unroll
+  for (int j = 0; j < 5; ++j) per[j] = ldq(per_tab + (size_t)5 * (i & k.per_mask) + j);
+  const qm31 x = domain_point(k, wpow, i);
+  rescue_stacked_eval(per, cur, next, res);
+  qm31 tsum = qzero();
+#pragma unroll
+  for (int t = 0; t < 12; ++t) tsum = qadd(tsum, qmul(rq.alphas[t], res[t]));
+  qm31 h = qmul(tsum, qsub(x, k.last_point));
+  const qm31 d0 = qsub(x, rq.bp[0]), d1 = qsub(x, rq.bp[1]);
+  const qm31 inv = qinv(qmul(d0, d1));  // every x - p is a unit on the evaluation domain
+  qm31 acc0 = qneg(rq.be[0]), acc1 = qneg(rq.be[1]);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    acc0 = qadd(acc0, qmul(rq.bc[0][j], cur[j]));
+    acc1 = qadd(acc1, qmul(rq.bc[1][j], cur[j]));
+  }
+  const qm31 bsum = qadd(qmul(acc0, qmul(inv, d1)), qmul(acc1, qmul(inv, d0)));
+  const uint32_t zi = i & ((1u << k.log_blowup) - 1);
+  h = qadd(h, qmul(bsum, ldq(zh_tab + 2 * (size_t)zi)));
+  stq(q + i, qmul(h, ldq(zh_tab + 2 * (size_t)zi + 1)));
+}
+
+// The RescueQuot of `k`, when its constraints have the stacked Rescue shape the
+// specialised kernel assumes (checked, not assumed).
+bool rescue_quot(const QuotConsts& k, RescueQuot& rq) {
+  if (k.air.id != AIR_RESCUE_STACKED || k.m != 12 || k.m_total != 12 || k.num_trans != 12 || k.n_rel != 0 ||
+      k.n_pre != 0 || k.n_bpts != 2)
+    return false;
+  for (int t = 0; t < 12; ++t) rq.alphas[t] = k.alphas[t];
+  for (int g = 0; g < 2; ++g) {
+    rq.bp[g] = k.bpts[g];
+    rq.be[g] = qzero();
+    for (int j = 0; j < 4; ++j) rq.bc[g][j] = qzero();
+  }
+  for (uint32_t b = 0; b < k.total_bound; ++b) {
+    const uint32_t g = k.b_grp[b], j = k.b_col[b];
+    if (g >= 2 || j >= 4) return false;
+    rq.bc[g][j] = qadd(rq.bc[g][j], k.betas[b]);
+    rq.be[g] = qadd(rq.be[g], qmul(k.betas[b], k.b_val[b]));
+  }
+  return true;
+}
+
 // LogUp row contributions (stark.zig:283-297) on H: out[i] = contribution of row i.
 __global__ void k_logup_rows(const qm31* __restrict__ vals, uint32_t n, const QuotConsts* __restrict__ kp,
                              uint32_t r, qm31* __restrict__ out) {
@@ -500,28 +573,29 @@ void upload_columns(const WireColumns& c, qm31* dst, uint32_t n, cudaStream_t st
   ZS_CUDA(cudaGetLastError());
 }
 
-// A copy stream for one proof's uploads, forked from `st` (so it sees the buffers
-// allocated there before). join() makes `st` wait for everything issued on it so far; the destructor joins too (so stream-ordered frees on `st` follow every
-// copy) and releases the stream once it has drained.
+// A side stream for one proof's uploads or trees (the calling thread's stream in `slot`),
+// forked from `st` (so it sees the buffers allocated there before). join() makes `st`
+// wait for everything issued on it so far; the destructor joins too (so stream-ordered
+// frees on `st` follow every copy) and waits for the side stream to drain.
 struct CopyStream {
   cudaStream_t s = nullptr, st;
   cudaEvent_t ev = nullptr;
-  explicit CopyStream(cudaStream_t main) : st(main) {
-    ZS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    ZS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    ZS_CUDA(cudaEventRecord(ev, st));  // buffers allocated on `st` so far are ready
-    ZS_CUDA(cudaStreamWaitEvent(s, ev, 0));
+  CopyStream(cudaStream_t main, int slot) : st(main) {
+    thread_stream(slot, &s, &ev);
+    fork();  // buffers allocated on `st` so far are ready
   }
   void join() {
     ZS_CUDA(cudaEventRecord(ev, s));
     ZS_CUDA(cudaStreamWaitEvent(st, ev, 0));
   }
+  void fork() {  // the side stream waits for everything issued on `st` so far
+    ZS_CUDA(cudaEventRecord(ev, st));
+    ZS_CUDA(cudaStreamWaitEvent(s, ev, 0));
+  }
   ~CopyStream() {
     cudaEventRecord(ev, s);
     cudaStreamWaitEvent(st, ev, 0);
     cudaStreamSynchronize(s);
-    cudaEventDestroy(ev);
-    cudaStreamDestroy(s);
   }
   CopyStream(const CopyStream&) = delete;
   CopyStream& operator=(const CopyStream&) = delete;
@@ -599,16 +673,19 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   for (uint32_t j = 0; j < ncol; ++j) trees.push_back(std::make_unique<OwnedTree>(lN, st));
   {
     // Columns [pre | main] in groups: group g+1 is packed on the host and copied on a
-    // copy stream while the LDE and trees of group g run on `st`. A proof whose columns
-    // are small goes as one group.
+    // copy stream while the LDE of group g runs on `st` and its trees on a side stream
+    // (so the narrow, latency-bound top levels of one group's trees overlap the next
+    // group's transforms). The first group is one column, so the device starts after one
+    // column's packing; the rest are kGroupBytes each. A proof whose columns are small
+    // goes as one group.
     const uint32_t C = n_pre + m;
     const size_t col_bytes = (size_t)16 * n;
     const uint32_t per = col_bytes * C < kGroupMin ? C : std::max<uint32_t>(1, (uint32_t)(kGroupBytes / col_bytes));
-    std::unique_ptr<CopyStream> cs;
-    if (per < C) cs = std::make_unique<CopyStream>(st);
+    std::unique_ptr<CopyStream> cs, ts;
+    if (per < C) cs = std::make_unique<CopyStream>(st, 1), ts = std::make_unique<CopyStream>(st, 2);
     cudaStream_t up = cs ? cs->s : st;
-    for (uint32_t c0 = 0; c0 < C; c0 += per) {
-      const uint32_t c1 = std::min(C, c0 + per);
+    for (uint32_t c0 = 0; c0 < C;) {
+      const uint32_t c1 = std::min(C, c0 + (per < C && c0 == 0 ? 1 : per));
       WireColumns gp, gt;  // this group's preprocessed and main columns
       for (uint32_t j = c0; j < std::min(c1, n_pre); ++j) gp.data.push_back(pre.data[j]), gp.len.push_back(n);
       for (uint32_t j = std::max(c0, n_pre); j < c1; ++j)
@@ -618,8 +695,15 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
       if (cs) cs->join();  // `st` waits for this group's columns only
       lde_qm31(vals.p + (size_t)c0 * n, n, coeffs.p + (size_t)c0 * n, n, cw.p + (size_t)c0 * N, N, c1 - c0, small,
                big, offset_pows, st);
-      build_qm31_trees(cw.p + (size_t)c0 * N, N, tree_ptrs(trees, c0, c1).data(), c1 - c0, st);
+      if (ts) {
+        ts->fork();
+        build_qm31_trees(cw.p + (size_t)c0 * N, N, tree_ptrs(trees, c0, c1).data(), c1 - c0, ts->s);
+      } else {
+        build_qm31_trees(cw.p + (size_t)c0 * N, N, tree_ptrs(trees, c0, c1).data(), c1 - c0, st);
+      }
+      c0 = c1;
     }
+    if (ts) ts->join();  // the roots below are read on `st`
   }
 
   Channel ch(sep, sep_len);
@@ -750,6 +834,8 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   if (wide) {
     h2d_small(d_ml->p, ml.get(), sizeof(MlConsts), st);
     k_ml_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_ml->p, zh_tab.p);
+  } else if (RescueQuot rq; rescue_quot(kc, rq)) {
+    k_quotient_rescue<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_kc.p, rq, zh_tab.p, per_tab.p);
   } else {
     k_quotient<<<(N + kT - 1) / kT, kT, 0, st>>>(cw.p, q.p, big.fwd, d_kc.p, zh_tab.p, per_tab.p);
   }
