@@ -675,17 +675,20 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
     // Columns [pre | main] in groups: group g+1 is packed on the host and copied on a
     // copy stream while the LDE of group g runs on `st` and its trees on a side stream
     // (so the narrow, latency-bound top levels of one group's trees overlap the next
-    // group's transforms). The first group is one column, so the device starts after one
-    // column's packing; the rest are kGroupBytes each. A proof whose columns are small
-    // goes as one group.
+    // group's transforms). Group sizes double from one column up to kGroupBytes: the
+    // device starts after one column's packing, and since it spends about twice as long
+    // on a column as the host spends packing one, each group is packed before the device
+    // finishes the one before it. A proof whose columns are small goes as one group.
     const uint32_t C = n_pre + m;
     const size_t col_bytes = (size_t)16 * n;
     const uint32_t per = col_bytes * C < kGroupMin ? C : std::max<uint32_t>(1, (uint32_t)(kGroupBytes / col_bytes));
     std::unique_ptr<CopyStream> cs, ts;
     if (per < C) cs = std::make_unique<CopyStream>(st, 1), ts = std::make_unique<CopyStream>(st, 2);
     cudaStream_t up = cs ? cs->s : st;
+    uint32_t gsize = per < C ? 1 : per;
     for (uint32_t c0 = 0; c0 < C;) {
-      const uint32_t c1 = std::min(C, c0 + (per < C && c0 == 0 ? 1 : per));
+      const uint32_t c1 = std::min(C, c0 + gsize);
+      gsize = std::min(per, 2 * gsize);
       WireColumns gp, gt;  // this group's preprocessed and main columns
       for (uint32_t j = c0; j < std::min(c1, n_pre); ++j) gp.data.push_back(pre.data[j]), gp.len.push_back(n);
       for (uint32_t j = std::max(c0, n_pre); j < c1; ++j)
