@@ -27,6 +27,7 @@
 #include "airs.cuh"
 #include "host.cuh"
 #include "stark.cuh"
+#include "staging.cuh"
 
 namespace zs {
 
@@ -106,7 +107,7 @@ Job copy_job(const zs_m31_job& j) {
   uint8_t* p = o.owned.get();
   auto cp = [&](const uint8_t* src, size_t n) -> const uint8_t* {
     if (n == 0) return nullptr;
-    std::memcpy(p, src, n);
+    host_copy(p, src, n);
     const uint8_t* r = p;
     p += n;
     return r;

@@ -241,6 +241,20 @@ void d2h_many(const D2H* c, size_t count, cudaStream_t st) {
     if (c[k].bytes) std::memcpy(c[k].dst, r[k], c[k].bytes);
 }
 
+void host_copy(void* dst, const void* src, size_t bytes) {
+  constexpr size_t kPart = (size_t)8 << 20;  // bytes per pool task
+  if (bytes < 2 * kPart) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  const size_t parts = (bytes + kPart - 1) / kPart;
+  HostPool::get().run(parts, [&](size_t i) {
+    const size_t off = i * kPart;
+    std::memcpy(static_cast<uint8_t*>(dst) + off, static_cast<const uint8_t*>(src) + off,
+                std::min(kPart, bytes - off));
+  });
+}
+
 void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   if (bytes == 0) return;
   Stager* sg = (bytes < kSmall || !t_slot) ? nullptr : &t_slot->stager;

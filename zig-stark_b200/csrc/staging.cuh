@@ -16,6 +16,11 @@ namespace zs {
 // `st`. Returns once `src` may be reused; the device copy completes in stream order.
 void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t st);
 
+// memcpy of host memory, split over the host copy pool when it is large (a served
+// request's copy of a 2^22-row trace is most of a gigabyte) and the pool is free; on the
+// calling thread otherwise.
+void host_copy(void* dst, const void* src, size_t bytes);
+
 // Uploads the low 32-bit word of every 16-byte element of C columns (column j: n
 // elements at cols[j]) to dst (column j at dst + j * n), packing on the host so a
 // QM31-embedded M31 column crosses PCIe at a quarter of its wire size. high[j] is set
