@@ -564,7 +564,7 @@ SC_TERMS = [([0, 1, 2], 1), ([0], 2)]  # src/cuda/sumcheck_test.zig:40-43: t0 t1
 def _sc_lookups_per_row(bits, terms, dmax):
     """GF(2^8) table lookups the round kernel makes per row for `terms` (its own
     arithmetic: a GF(2^128) product is 121 lookups, a subfield scalar times a GF(2^128)
-    element 16, a GF(2^8) product 1; the points 0 and 1 need none for the linear factor,
+    element 16, a GF(2^8) product 1; the points 0..3 need none for the linear factor,
     a unit coefficient none, a GF(2^8) coefficient of a GF(2^128) term 16)."""
     mul, scal = (1, 1) if bits == 8 else (121, 16)
     total = 0
@@ -572,7 +572,7 @@ def _sc_lookups_per_row(bits, terms, dmax):
         if not fs:
             continue
         for t in range(dmax + 1):
-            total += (scal if t >= 2 else 0) * len(fs) + mul * (len(fs) - 1)
+            total += (scal if t >= 4 else 0) * len(fs) + mul * (len(fs) - 1)
             if c != 1:
                 total += mul if (bits == 8 or c >= 256) else scal
     return total

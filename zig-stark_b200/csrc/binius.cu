@@ -16,7 +16,8 @@
 // costs one table lookup at any level. A GF(2^128) product is 81 + 40 lookups. The points
 // t < 256 lie in the GF(2^8) subfield, and a subfield scalar multiplies the 16 byte
 // coordinates of a GF(2^128) element independently (the tower is a GF(2^8)-vector space
-// on the monomials of X_3..X_6); t = 0 and t = 1 need no product at all (a and b).
+// on the monomials of X_3..X_6); t = 0 and t = 1 need no product at all (a and b), and
+// t = 2, 3 only bit operations (2 = X_0 scales each 2-bit GF(4) coordinate on its own).
 //
 // The round's term list (at most 256 terms and 1024 factor indices) travels as the
 // kernel's parameter (7.2 KB, within the 32 KB parameter space of sm_70 and later), so a
@@ -279,17 +280,29 @@ __device__ __forceinline__ void warp_xor_into128(const g128& v, uint32_t* acc) {
   warp_xor_into((uint32_t)(v.hi >> 32), acc + 3);
 }
 
-// The point t's linear factor a + t (a + b): a at t = 0, b at t = 1.
+// 2 x, by bits: 2 = X_0 lies in GF(4), and a GF(4) scalar scales each GF(4) coordinate (bit
+// pair) of a tower element on its own: (a0, a1) -> a1 + (a0 + a1) X_0.
+ZS_HD uint32_t mul2_8(uint32_t x) { return ((x >> 1) & 0x55u) | (((x << 1) ^ x) & 0xAAu); }
+ZS_HD uint64_t mul2_64(uint64_t x) {
+  return ((x >> 1) & 0x5555555555555555ull) | (((x << 1) ^ x) & 0xAAAAAAAAAAAAAAAAull);
+}
+
+// The point t's linear factor a + t (a + b): a at t = 0, b at t = 1, a + 2 (a + b) and
+// b + 2 (a + b) at t = 2 and 3 (no table lookup), a lookup beyond.
 template <int t>
 __device__ __forceinline__ uint32_t at_point8(const Tower& F, uint32_t a, uint32_t b) {
   if constexpr (t == 0) return a;
   else if constexpr (t == 1) return b;
+  else if constexpr (t == 2) return a ^ mul2_8(a ^ b);
+  else if constexpr (t == 3) return b ^ mul2_8(a ^ b);
   else return a ^ F.m8(t, a ^ b);
 }
 template <int t>
 __device__ __forceinline__ g128 at_point128(const Tower& F, const g128& a, const g128& b) {
   if constexpr (t == 0) return a;
   else if constexpr (t == 1) return b;
+  else if constexpr (t == 2) return {a.lo ^ mul2_64(a.lo ^ b.lo), a.hi ^ mul2_64(a.hi ^ b.hi)};
+  else if constexpr (t == 3) return {b.lo ^ mul2_64(a.lo ^ b.lo), b.hi ^ mul2_64(a.hi ^ b.hi)};
   else return gxor(a, F.s128(t, gxor(a, b)));
 }
 
@@ -425,7 +438,7 @@ __device__ __forceinline__ g128 load_g128(const uint4* p) {
 
 // GF(2^128) round; out: (dmax + 1) values of four little-endian words. D as k_values8.
 template <int D>
-__global__ void __launch_bounds__(kBThreads) k_values128(const uint4* __restrict__ cur, uint32_t len, uint32_t half,
+__global__ void __launch_bounds__(kBThreads, (D >= 1 && D <= 4) ? 2 : 1) k_values128(const uint4* __restrict__ cur, uint32_t len, uint32_t half,
                                                          uint32_t dmax, const __grid_constant__ Terms tm,
                                                          const uint8_t* __restrict__ gT, uint32_t* __restrict__ out) {
   extern __shared__ uint4 smem_b[];
