@@ -597,7 +597,7 @@ def binius_metrics(clock_mhz):
     idx, off = [0, 1, 2, 0], [0, 3, 4]
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     out = {"terms": "t0 t1 t2 + 2 t0 over 3 tables (src/cuda/sumcheck_test.zig:40-43)", "dmax": 3}
-    wavefronts = {8: 2.70, 128: 2.86}
+    wavefronts = {8: 3.11, 128: 2.96}
     for bits, k, k_cpu in ((8, 24, 16), (128, 20, 10)):
         es = 1 if bits == 8 else 16
         n = 1 << k
