@@ -75,7 +75,8 @@ enum {
  * On success *out_proof / *out_len hold the serialized GenericStark(Air).Proof
  * (stark.zig:107-122), allocated with `host` and released with zs_free. The proof is
  * byte-identical to the reference prover's for the same inputs. Parameters the
- * reference asserts on (stark.zig:230-232, fri.zig:228) return -4. */
+ * reference asserts on (stark.zig:230-232, fri.zig:228) return -4; a domain above 2^26
+ * points (trace_log + log_blowup > 26) or more than 2^24 queries returns -2. */
 int32_t zs_m31_prove(zs_host_allocator host, uint32_t air_id, const uint8_t *params, size_t params_len,
                      const uint8_t *public_inputs, size_t public_inputs_len, const uint8_t *preprocessed,
                      size_t preprocessed_len, const uint8_t *trace, size_t trace_len, const uint8_t *channel_sep,

@@ -340,11 +340,18 @@ __global__ void __launch_bounds__(kT) k_deep(const qm31* __restrict__ cw, const 
 }
 
 // Gather: out[r] = words [idx * w, (idx + 1) * w) of src[r] (requests prepared on the host).
-struct GatherReq {
-  const uint32_t* src;
-  uint64_t index;
-  uint32_t words;
-  uint32_t out_off;
+// One entry of a query's gather list: `words` words (4: a QM31 value, 8: a Merkle node)
+// from `base` at element index idx, where the query's position p is p0 mod 2^modlog
+// (kQLow), that plus 2^modlog (kQHigh), p0 itself (kQP0) or (p0 + shift) mod 2^lN
+// (kQShift), and idx = p for a value or (p >> lvl) ^ 1, the sibling at level lvl, for a
+// path node. `off` is its word offset within the query's slice of section `sec`.
+enum : uint8_t { kQLow = 0, kQHigh = 1, kQP0 = 2, kQShift = 3 };
+constexpr uint8_t kQValue = 0xff;
+struct QueryReq {
+  const uint32_t* base;
+  uint32_t off;
+  uint16_t words;
+  uint8_t sec, mode, modlog, lvl;
 };
 // One FRI transcript step on the device (fri.zig:199-206): absorb the layer root,
 // sample the folding challenge. One warp copies the state to shared memory and back;
@@ -369,11 +376,23 @@ __global__ void k_fri_transcript(Channel* ch, const uint32_t* __restrict__ root,
   copy_state(ch, ch_raw, sizeof(Channel));
 }
 
-__global__ void k_gather(const GatherReq* __restrict__ reqs, uint32_t count, uint32_t* __restrict__ out) {
-  const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= count) return;
-  const GatherReq q = reqs[r];
-  for (uint32_t w = 0; w < q.words; ++w) out[q.out_off + w] = q.src[q.index * q.words + w];
+// The gathered words of every query: query qi's section-0 words at qi * sec0, its
+// section-1 words after all nq queries' section 0, at nq * sec0 + qi * sec1. Grid:
+// (entries of the template, queries q0 .. q0 + gridDim.y - 1).
+__global__ void k_gather_queries(const QueryReq* __restrict__ tmpl, uint32_t count, const uint64_t* __restrict__ p0s,
+                                 uint32_t q0, uint32_t nq, uint64_t shift, unsigned log_N, uint32_t sec0,
+                                 uint32_t sec1, uint32_t* __restrict__ out) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x, qi = q0 + blockIdx.y;
+  if (e >= count) return;
+  const QueryReq r = tmpl[e];
+  const uint64_t p0 = p0s[qi], low = p0 & (((uint64_t)1 << r.modlog) - 1);
+  uint64_t p = p0;
+  if (r.mode == kQLow) p = low;
+  else if (r.mode == kQHigh) p = low + ((uint64_t)1 << r.modlog);
+  else if (r.mode == kQShift) p = (p0 + shift) & (((uint64_t)1 << log_N) - 1);
+  const uint64_t idx = r.lvl == kQValue ? p : ((p >> r.lvl) ^ 1);
+  uint32_t* dst = out + (r.sec == 0 ? (size_t)qi * sec0 : (size_t)nq * sec0 + (size_t)qi * sec1) + r.off;
+  for (uint32_t w = 0; w < r.words; ++w) dst[w] = r.base[idx * r.words + w];
 }
 
 template <typename T>
@@ -624,6 +643,7 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
   const WireColumns trace = locate_columns(trace_b, trace_len);
   const unsigned tl = sp.trace_log, lb = sp.log_blowup, lN = tl + lb;
   if (lN > 26) throw Error(ZS_EMALFORMED, "trace_log + log_blowup above 26");
+  if (sp.num_queries > ((uint64_t)1 << 24)) throw Error(ZS_EMALFORMED, "more than 2^24 queries");
   const uint32_t n = 1u << tl, N = 1u << lN, shift = 1u << lb;
   if (air.fixed_n && n != air.fixed_n) throw Error(ZS_EMALFORMED, "the AIR is defined for a fixed trace length");
   if (air.id == AIR_RESCUE_STACKED && n < 8) throw Error(ZS_EMALFORMED, "stacked rescue needs at least 8 rows");
@@ -969,57 +989,54 @@ std::vector<uint8_t> stark_prove(uint32_t air_id, const uint8_t* params_b, size_
 
   // ---- queries (fri.zig:236-256, stark.zig:595-625) -----------------------------
   // Every revealed value and Merkle sibling is gathered by one kernel, in the order the
-  // proof lists them, so serialization copies contiguous runs of the gathered words.
+  // proof lists them, so serialization copies contiguous runs of the gathered words. The
+  // gather list is the same for every query but for the positions, so the host builds
+  // one query's template and the kernel applies it to all of them.
   std::vector<uint64_t> p0s(sp.num_queries);
   for (auto& p : p0s) p = ch.sample_index(N);
-  std::vector<GatherReq> reqs;
-  {
-    size_t fri_levels = 0;
-    for (unsigned i = 0; i < L; ++i) fri_levels += lN - i;
-    reqs.reserve((size_t)sp.num_queries * (2 * L + 2 * fri_levels + (size_t)reveal_len * (1 + lN)));
-  }
-  uint32_t off = 0;
-  auto want_value = [&](const qm31* base, uint64_t idx) {
-    reqs.push_back({reinterpret_cast<const uint32_t*>(base), idx, 4, off});
-    off += 4;
+  std::vector<QueryReq> tmpl;
+  uint32_t sec_words[2] = {0, 0};
+  auto want = [&](int sec, const void* base, uint32_t words, uint8_t mode, unsigned modlog, uint8_t lvl) {
+    tmpl.push_back({reinterpret_cast<const uint32_t*>(base), sec_words[sec], (uint16_t)words, (uint8_t)sec, mode,
+                    (uint8_t)modlog, lvl});
+    sec_words[sec] += words;
   };
-  auto want_path = [&](const DeviceTree& t, uint64_t idx) {
-    for (unsigned lvl = 0; lvl < t.log_n; ++lvl) {
-      reqs.push_back({t.level(lvl), (idx >> lvl) ^ 1, 8, off});
-      off += 8;
-    }
+  auto want_path = [&](int sec, const DeviceTree& t, uint8_t mode, unsigned modlog) {
+    for (unsigned lvl = 0; lvl < t.log_n; ++lvl) want(sec, t.level(lvl), 8, mode, modlog, (uint8_t)lvl);
   };
-  // FRI pairs: per layer the two values, then their two paths
-  for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
-    uint64_t p = p0s[qi];
-    for (unsigned i = 0; i < L; ++i) {
-      const uint64_t nn = (uint64_t)N >> (i + 1), pn = p % nn;
-      want_value(layers[i]->p, pn);
-      want_value(layers[i]->p, pn + nn);
-      want_path(ftrees[i]->t, pn);
-      want_path(ftrees[i]->t, pn + nn);
-      p = pn;
-    }
+  // FRI pairs, per query: per layer i the two values at p0 mod 2^(lN-i-1) and that plus
+  // 2^(lN-i-1), then their two paths
+  for (unsigned i = 0; i < L; ++i) {
+    const unsigned ml = lN - (i + 1);
+    want(0, layers[i]->p, 4, kQLow, ml, kQValue);
+    want(0, layers[i]->p, 4, kQHigh, ml, kQValue);
+    want_path(0, ftrees[i]->t, kQLow, ml);
+    want_path(0, ftrees[i]->t, kQHigh, ml);
   }
-  // STARK reveals: per query the values (columns at p0, columns at p0 + shift, the
+  // STARK reveals, per query: the values (columns at p0, columns at p0 + shift, the
   // quotient, preprocessed columns), then their paths in the same order
-  for (uint64_t qi = 0; qi < sp.num_queries; ++qi) {
-    const uint64_t p0 = p0s[qi], pn = (p0 + shift) % N;
-    for (uint32_t j = 0; j < m_total; ++j) want_value(cw.p + (size_t)(n_pre + j) * N, p0);
-    for (uint32_t j = 0; j < m_total; ++j) want_value(cw.p + (size_t)(n_pre + j) * N, pn);
-    want_value(q.p, p0);
-    for (uint32_t j = 0; j < n_pre; ++j) want_value(cw.p + (size_t)j * N, p0);
-    for (uint32_t j = 0; j < m_total; ++j) want_path(trees[n_pre + j]->t, p0);
-    for (uint32_t j = 0; j < m_total; ++j) want_path(trees[n_pre + j]->t, pn);
-    want_path(qtree.t, p0);
-    for (uint32_t j = 0; j < n_pre; ++j) want_path(trees[j]->t, p0);
-  }
+  for (uint32_t j = 0; j < m_total; ++j) want(1, cw.p + (size_t)(n_pre + j) * N, 4, kQP0, lN, kQValue);
+  for (uint32_t j = 0; j < m_total; ++j) want(1, cw.p + (size_t)(n_pre + j) * N, 4, kQShift, lN, kQValue);
+  want(1, q.p, 4, kQP0, lN, kQValue);
+  for (uint32_t j = 0; j < n_pre; ++j) want(1, cw.p + (size_t)j * N, 4, kQP0, lN, kQValue);
+  for (uint32_t j = 0; j < m_total; ++j) want_path(1, trees[n_pre + j]->t, kQP0, lN);
+  for (uint32_t j = 0; j < m_total; ++j) want_path(1, trees[n_pre + j]->t, kQShift, lN);
+  want_path(1, qtree.t, kQP0, lN);
+  for (uint32_t j = 0; j < n_pre; ++j) want_path(1, trees[j]->t, kQP0, lN);
+  const uint32_t nq = (uint32_t)sp.num_queries;
+  const size_t off = (size_t)nq * (sec_words[0] + sec_words[1]);
   std::vector<uint32_t> gathered(off);
-  if (!reqs.empty()) {
-    DevBuf<GatherReq> d_reqs(reqs.size(), st);
+  if (off > 0) {
+    DevBuf<QueryReq> d_tmpl(tmpl.size(), st);
+    DevBuf<uint64_t> d_p0s(nq, st);
     DevBuf<uint32_t> d_out(off, st);
-    h2d_small(d_reqs.p, reqs.data(), reqs.size() * sizeof(GatherReq), st);
-    k_gather<<<((uint32_t)reqs.size() + kT - 1) / kT, kT, 0, st>>>(d_reqs.p, (uint32_t)reqs.size(), d_out.p);
+    h2d_small(d_tmpl.p, tmpl.data(), tmpl.size() * sizeof(QueryReq), st);
+    h2d_small(d_p0s.p, p0s.data(), nq * sizeof(uint64_t), st);
+    for (uint32_t q0 = 0; q0 < nq; q0 += 65535) {  // grid.y is at most 65535
+      const dim3 grid(((uint32_t)tmpl.size() + kT - 1) / kT, std::min<uint32_t>(65535, nq - q0));
+      k_gather_queries<<<grid, kT, 0, st>>>(d_tmpl.p, (uint32_t)tmpl.size(), d_p0s.p, q0, nq, shift, lN,
+                                            sec_words[0], sec_words[1], d_out.p);
+    }
     ZS_CUDA(cudaGetLastError());
     d2h_small(gathered.data(), d_out.p, off * sizeof(uint32_t), st);
   }
