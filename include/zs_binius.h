@@ -68,8 +68,8 @@ int32_t zs_binius_sumcheck_fold_device(uint32_t field_bits, const void *d_cur, s
 /* Sumcheck(F).proveCombination (src/binius/sumcheck.zig:208-395) with its optional
  * transcript seed (Transcript.initBytes(seed) when has_seed is set, else
  * Transcript.init(claimed sum)): m tables of 2^k elements (host memory, m * 2^k element
- * sizes), copied to the device once; every round's values and fold run on the device,
- * the interpolation and the SHA-256 transcript on the host.
+ * sizes), copied to the device once; every round (values, interpolation, the SHA-256
+ * transcript step, fold) runs on the device, and the host waits once, for the proof.
  * claimed_out: one element (the hypercube sum). rounds_out: k * (dmax + 1) elements, round
  * i's low-first coefficients at i * (dmax + 1), dmax = the longest term (dmax + 1 <= 64).
  * Synchronous. */

@@ -32,6 +32,11 @@
 // of the table. Over GF(2^128) the product by a fixed r is GF(2^8)-linear in the 16 byte
 // coordinates of (a + b): a 16 x 256 table of r * (v X^byte k), built once per fold, turns
 // it into 16 lookups of 16 bytes.
+//
+// Prover. The tables go to the device once; each round is the values kernel, k_sc_step
+// (the coefficients from a Lagrange matrix built once per proof, then the SHA-256
+// transcript step in one thread, the challenge left in device memory) and the fold, which
+// reads the challenge there: the rounds run back to back and the host waits once.
 #include <algorithm>
 #include <cstring>
 #include <memory>
@@ -161,91 +166,6 @@ const HostTower& host_tower() {
   static const HostTower t;
   return t;
 }
-
-// ---- host: SHA-256 (FIPS 180-4), the sum-check transcript's hash --------------------
-
-class Sha256 {
- public:
-  Sha256() { reset(); }
-  void update(const uint8_t* p, size_t n) {
-    total_ += n;
-    while (n) {
-      const size_t take = std::min(n, (size_t)64 - fill_);
-      std::memcpy(buf_ + fill_, p, take);
-      fill_ += take;
-      p += take;
-      n -= take;
-      if (fill_ == 64) {
-        block(buf_);
-        fill_ = 0;
-      }
-    }
-  }
-  void final(uint8_t out[32]) {
-    const uint64_t bits = total_ * 8;
-    const uint8_t one = 0x80, zero = 0;
-    update(&one, 1);
-    while (fill_ != 56) update(&zero, 1);
-    uint8_t len[8];
-    for (int i = 0; i < 8; ++i) len[i] = (uint8_t)(bits >> (56 - 8 * i));
-    update(len, 8);
-    for (int i = 0; i < 8; ++i)
-      for (int j = 0; j < 4; ++j) out[4 * i + j] = (uint8_t)(h_[i] >> (24 - 8 * j));
-    reset();
-  }
-  static void hash(const uint8_t* p, size_t n, uint8_t out[32]) {
-    Sha256 s;
-    s.update(p, n);
-    s.final(out);
-  }
-
- private:
-  static uint32_t rotr(uint32_t x, unsigned r) { return (x >> r) | (x << (32 - r)); }
-  void reset() {
-    static const uint32_t iv[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a,
-                                   0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
-    std::memcpy(h_, iv, sizeof(iv));
-    fill_ = 0;
-    total_ = 0;
-  }
-  void block(const uint8_t* p) {
-    static const uint32_t K[64] = {
-        0x428a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4, 0xab1c5ed5,
-        0xd807aa98, 0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe, 0x9bdc06a7, 0xc19bf174,
-        0xe49b69c1, 0xefbe4786, 0x0fc19dc6, 0x240ca1cc, 0x2de92c6f, 0x4a7484aa, 0x5cb0a9dc, 0x76f988da,
-        0x983e5152, 0xa831c66d, 0xb00327c8, 0xbf597fc7, 0xc6e00bf3, 0xd5a79147, 0x06ca6351, 0x14292967,
-        0x27b70a85, 0x2e1b2138, 0x4d2c6dfc, 0x53380d13, 0x650a7354, 0x766a0abb, 0x81c2c92e, 0x92722c85,
-        0xa2bfe8a1, 0xa81a664b, 0xc24b8b70, 0xc76c51a3, 0xd192e819, 0xd6990624, 0xf40e3585, 0x106aa070,
-        0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
-        0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
-    uint32_t w[64];
-    for (int i = 0; i < 16; ++i)
-      w[i] = (uint32_t)p[4 * i] << 24 | (uint32_t)p[4 * i + 1] << 16 | (uint32_t)p[4 * i + 2] << 8 | p[4 * i + 3];
-    for (int i = 16; i < 64; ++i) {
-      const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
-      const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
-      w[i] = w[i - 16] + s0 + w[i - 7] + s1;
-    }
-    uint32_t a = h_[0], b = h_[1], c = h_[2], d = h_[3], e = h_[4], f = h_[5], g = h_[6], h = h_[7];
-    for (int i = 0; i < 64; ++i) {
-      const uint32_t t1 = h + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + K[i] + w[i];
-      const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
-      h = g;
-      g = f;
-      f = e;
-      e = d + t1;
-      d = c;
-      c = b;
-      b = a;
-      a = t1 + t2;
-    }
-    h_[0] += a, h_[1] += b, h_[2] += c, h_[3] += d, h_[4] += e, h_[5] += f, h_[6] += g, h_[7] += h;
-  }
-  uint32_t h_[8];
-  uint8_t buf_[64];
-  size_t fill_;
-  uint64_t total_;
-};
 
 // ---- device: the product table and the kernels -----------------------------------
 
@@ -509,10 +429,12 @@ __global__ void __launch_bounds__(kBThreads, (D >= 1 && D <= 4) ? 2 : 1) k_value
 }
 
 // next[f][rest] = a + r (a + b) over GF(2^8); grid.y runs over the tables.
+// d_r: the challenge in device memory (the prover's device transcript), else r.
 __global__ void __launch_bounds__(kBThreads) k_fold8(const uint8_t* __restrict__ cur, uint32_t len, uint32_t half,
-                                                     uint32_t r, const uint8_t* __restrict__ gT,
-                                                     uint8_t* __restrict__ next) {
+                                                     uint32_t r, const uint8_t* __restrict__ d_r,
+                                                     const uint8_t* __restrict__ gT, uint8_t* __restrict__ next) {
   __shared__ uint8_t row[256];
+  if (d_r) r = d_r[0];
   for (uint32_t k = threadIdx.x; k < 256; k += blockDim.x) row[k] = gT[(r << 8) | k];
   __syncthreads();
   const uint8_t* src = cur + (size_t)blockIdx.y * len;
@@ -524,9 +446,13 @@ __global__ void __launch_bounds__(kBThreads) k_fold8(const uint8_t* __restrict__
 }
 
 // R[k][v] = r * (v at byte k), the GF(2^8)-linear map x -> r x on byte coordinates.
-__global__ void __launch_bounds__(kBThreads) k_mul_table128(uint64_t r_lo, uint64_t r_hi,
+__global__ void __launch_bounds__(kBThreads) k_mul_table128(uint64_t r_lo, uint64_t r_hi, const uint8_t* __restrict__ d_r,
                                                             const uint8_t* __restrict__ gT, uint4* __restrict__ R) {
   extern __shared__ uint4 smem_b[];
+  if (d_r) {  // the challenge in device memory: 16 little-endian bytes
+    r_lo = r_hi = 0;
+    for (int b = 7; b >= 0; --b) r_lo = (r_lo << 8) | d_r[b], r_hi = (r_hi << 8) | d_r[8 + b];
+  }
   uint8_t* s_T = reinterpret_cast<uint8_t*>(smem_b);
   load_table(s_T, gT);
   __syncthreads();
@@ -557,6 +483,144 @@ __global__ void __launch_bounds__(kBThreads) k_fold128(const uint4* __restrict__
     }
     dst[rest] = o;
   }
+}
+
+// ---- device: one round's transcript step of the combination prover ----------------
+// After a round's values are on the device: the round's coefficients by the Lagrange
+// matrix (sumcheck.zig:124-162), then the SHA-256 transcript step (sumcheck.zig:66-87)
+// that absorbs them and samples the next challenge, so the rounds of a proof run back to
+// back on the device with no trip to the host between them.
+
+__constant__ uint32_t kSha256K[64] = {
+    0x428a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4, 0xab1c5ed5,
+    0xd807aa98, 0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe, 0x9bdc06a7, 0xc19bf174,
+    0xe49b69c1, 0xefbe4786, 0x0fc19dc6, 0x240ca1cc, 0x2de92c6f, 0x4a7484aa, 0x5cb0a9dc, 0x76f988da,
+    0x983e5152, 0xa831c66d, 0xb00327c8, 0xbf597fc7, 0xc6e00bf3, 0xd5a79147, 0x06ca6351, 0x14292967,
+    0x27b70a85, 0x2e1b2138, 0x4d2c6dfc, 0x53380d13, 0x650a7354, 0x766a0abb, 0x81c2c92e, 0x92722c85,
+    0xa2bfe8a1, 0xa81a664b, 0xc24b8b70, 0xc76c51a3, 0xd192e819, 0xd6990624, 0xf40e3585, 0x106aa070,
+    0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
+    0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
+
+// SHA-256 (FIPS 180-4) in one thread: update over byte runs, then final.
+struct Sha256Dev {
+  uint32_t h[8];
+  uint8_t buf[64];
+  uint32_t fill;
+  uint64_t total;
+  __device__ void init() {
+    h[0] = 0x6a09e667, h[1] = 0xbb67ae85, h[2] = 0x3c6ef372, h[3] = 0xa54ff53a;
+    h[4] = 0x510e527f, h[5] = 0x9b05688c, h[6] = 0x1f83d9ab, h[7] = 0x5be0cd19;
+    fill = 0;
+    total = 0;
+  }
+  __device__ static uint32_t rotr(uint32_t x, unsigned r) { return __funnelshift_r(x, x, r); }
+  __device__ void block() {
+    uint32_t w[64];
+    for (int i = 0; i < 16; ++i)
+      w[i] = (uint32_t)buf[4 * i] << 24 | (uint32_t)buf[4 * i + 1] << 16 | (uint32_t)buf[4 * i + 2] << 8 |
+             buf[4 * i + 3];
+    for (int i = 16; i < 64; ++i) {
+      const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
+      const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
+      w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+    }
+    uint32_t a = h[0], b = h[1], c = h[2], d = h[3], e = h[4], f = h[5], g = h[6], hh = h[7];
+    for (int i = 0; i < 64; ++i) {
+      const uint32_t t1 = hh + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + kSha256K[i] + w[i];
+      const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+      hh = g, g = f, f = e, e = d + t1, d = c, c = b, b = a, a = t1 + t2;
+    }
+    h[0] += a, h[1] += b, h[2] += c, h[3] += d, h[4] += e, h[5] += f, h[6] += g, h[7] += hh;
+  }
+  __device__ void update(const uint8_t* p, uint32_t n) {
+    total += n;
+    for (uint32_t i = 0; i < n; ++i) {
+      buf[fill++] = p[i];
+      if (fill == 64) {
+        block();
+        fill = 0;
+      }
+    }
+  }
+  __device__ void final(uint8_t out[32]) {
+    const uint64_t bits = total * 8;
+    buf[fill++] = 0x80;
+    if (fill > 56) {
+      while (fill < 64) buf[fill++] = 0;
+      block();
+      fill = 0;
+    }
+    while (fill < 56) buf[fill++] = 0;
+    for (int i = 0; i < 8; ++i) buf[56 + i] = (uint8_t)(bits >> (56 - 8 * i));
+    block();
+    for (int i = 0; i < 8; ++i)
+      for (int j = 0; j < 4; ++j) out[4 * i + j] = (uint8_t)(h[i] >> (24 - 8 * j));
+  }
+};
+
+// The device transcript: the SHA-256 state (32 bytes) and the last challenge (1 or 16
+// bytes), in device memory between rounds.
+struct ScTranscript {
+  uint8_t state[32];
+  uint8_t r[16];
+};
+
+// Round `round`'s step: coefficient d = sum_i values[i] * lag[i][d] for d < n (one lane
+// per coefficient, the product table in global memory), written to rounds_out; the first
+// round also forms the claimed sum (values[0] + values[1]) and starts the transcript
+// (from `seed`, or from the claimed sum); thread 0 absorbs the coefficients and samples
+// the challenge (the digest's last byte over GF(2^8), its last 16 bytes over GF(2^128)).
+template <bool WIDE>
+__global__ void __launch_bounds__(64) k_sc_step(const uint8_t* __restrict__ vals, const uint8_t* __restrict__ lag,
+                                                uint32_t n, uint32_t round, const uint8_t* __restrict__ gT,
+                                                const uint8_t* __restrict__ seed, uint32_t seed_len, int has_seed,
+                                                ScTranscript* __restrict__ tx, uint8_t* __restrict__ claimed,
+                                                uint8_t* __restrict__ rounds_out) {
+  constexpr uint32_t ES = WIDE ? 16 : 1;
+  __shared__ uint8_t s_coef[kProveMaxPoints * 16];
+  const Tower F{gT};
+  auto ld = [](const uint8_t* p) {
+    uint64_t lo = 0, hi = 0;
+    for (int b = 7; b >= 0; --b) lo = (lo << 8) | p[b], hi = (hi << 8) | p[8 + b];
+    return g128{lo, hi};
+  };
+  for (uint32_t d = threadIdx.x; d < n; d += blockDim.x) {
+    uint8_t* out = s_coef + ES * d;
+    if constexpr (WIDE) {
+      g128 acc{0, 0};
+      for (uint32_t i = 0; i < n; ++i) {
+        const g128 v = ld(vals + 16 * i);
+        if (v.lo | v.hi) acc = gxor(acc, F.m128(v, ld(lag + 16 * ((size_t)i * n + d))));
+      }
+      for (int b = 0; b < 8; ++b) out[b] = (uint8_t)(acc.lo >> (8 * b)), out[8 + b] = (uint8_t)(acc.hi >> (8 * b));
+    } else {
+      uint32_t acc = 0;
+      for (uint32_t i = 0; i < n; ++i) acc ^= F.m8(vals[i], lag[(size_t)i * n + d]);
+      out[0] = (uint8_t)acc;
+    }
+    for (uint32_t b = 0; b < ES; ++b) rounds_out[((size_t)round * n + d) * ES + b] = out[b];
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  Sha256Dev sh;
+  if (round == 0) {
+    uint8_t h[16];
+    for (uint32_t b = 0; b < ES; ++b) {  // one point: the sum of 2^k copies of a constant is 0
+      h[b] = n >= 2 ? (uint8_t)(vals[b] ^ vals[ES + b]) : 0;
+      claimed[b] = h[b];
+    }
+    sh.init();
+    if (has_seed)
+      sh.update(seed, seed_len);
+    else
+      sh.update(h, ES);
+    sh.final(tx->state);
+  }
+  sh.init();
+  sh.update(tx->state, 32);
+  sh.update(s_coef, n * ES);
+  sh.final(tx->state);
+  for (uint32_t b = 0; b < ES; ++b) tx->r[b] = WIDE ? tx->state[16 + b] : tx->state[31];
 }
 
 // ---- host: argument checks and launches -------------------------------------------
@@ -676,8 +740,8 @@ void values_async(bool wide, const void* d_cur, size_t len, size_t half, size_t 
 
 // next (m tables of len / 2) = fold of cur (m tables of len) at r, asynchronously on `st`.
 // r_mul: a 64 KB device buffer for the GF(2^128) multiply table.
-void fold_async(bool wide, const void* d_cur, size_t len, size_t m, u128 r, void* d_next, uint4* r_mul,
-                cudaStream_t st) {
+void fold_async(bool wide, const void* d_cur, size_t len, size_t m, u128 r, const uint8_t* d_r, void* d_next,
+                uint4* r_mul, cudaStream_t st) {
   const size_t half = len / 2;
   if (half == 0) return;
   const DeviceState& ds = device_state(st);
@@ -686,9 +750,9 @@ void fold_async(bool wide, const void* d_cur, size_t len, size_t m, u128 r, void
   const dim3 grid(bx, (unsigned)m);
   if (!wide) {
     k_fold8<<<grid, kBThreads, 0, st>>>(static_cast<const uint8_t*>(d_cur), (uint32_t)len, (uint32_t)half,
-                                        (uint32_t)r, ds.table, static_cast<uint8_t*>(d_next));
+                                        (uint32_t)r, d_r, ds.table, static_cast<uint8_t*>(d_next));
   } else {
-    k_mul_table128<<<4096 / kBThreads, kBThreads, 65536, st>>>((uint64_t)r, (uint64_t)(r >> 64), ds.table, r_mul);
+    k_mul_table128<<<4096 / kBThreads, kBThreads, 65536, st>>>((uint64_t)r, (uint64_t)(r >> 64), d_r, ds.table, r_mul);
     k_fold128<<<grid, kBThreads, 65536, st>>>(static_cast<const uint4*>(d_cur), (uint32_t)len, (uint32_t)half,
                                               r_mul, static_cast<uint4*>(d_next));
   }
@@ -759,8 +823,8 @@ void store_elem(uint8_t* p, size_t es, u128 v) {
 
 // Lagrange interpolation through the points 0..n-1 (sumcheck.zig:124-162) as a matrix:
 // row i holds the low-first coefficients of prod_{j != i} (x + j) / (i + j), so a round's
-// coefficients are coeffs[d] = sum_i values[i] * lag[i][d]. The matrix depends on the
-// points only and is built once per proof.
+// coefficients are coeffs[d] = sum_i values[i] * lag[i][d] (k_sc_step). The matrix
+// depends on the points only and is built once per proof, on the host.
 std::vector<std::vector<u128>> lagrange_matrix(const HostTower& ht, unsigned level, size_t n) {
   std::vector<std::vector<u128>> lag(n, std::vector<u128>(n, 0));
   for (size_t i = 0; i < n; ++i) {
@@ -782,16 +846,6 @@ std::vector<std::vector<u128>> lagrange_matrix(const HostTower& ht, unsigned lev
   return lag;
 }
 
-std::vector<u128> interpolate(const HostTower& ht, unsigned level, const std::vector<u128>& values,
-                              const std::vector<std::vector<u128>>& lag) {
-  const size_t n = values.size();
-  std::vector<u128> coeffs(n, 0);
-  for (size_t i = 0; i < n; ++i)
-    if (values[i])
-      for (size_t d = 0; d < n; ++d) coeffs[d] ^= ht.mul(level, values[i], lag[i][d]);
-  return coeffs;
-}
-
 int32_t prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k, size_t m, const uint8_t* coeffs,
                           size_t nterms, const uint32_t* indices, size_t n_indices, const uint32_t* offsets,
                           const uint8_t* seed, size_t seed_len, int32_t has_seed, uint8_t* claimed_out,
@@ -810,29 +864,6 @@ int32_t prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k, 
     const size_t n = (size_t)1 << k;
     if (m > (((size_t)1 << 36) / es) / n) throw Error(ZS_EMALFORMED, "tables larger than 64 GB");
     const HostTower& ht = host_tower();
-
-    // the transcript (sumcheck.zig:47-87)
-    uint8_t state[32];
-    auto absorb = [&](const std::vector<u128>& cs) {
-      Sha256 h;
-      h.update(state, 32);
-      uint8_t b[16];
-      for (u128 c : cs) {
-        store_elem(b, es, c);
-        h.update(b, es);
-      }
-      h.final(state);
-      return wide ? load_elem(state + 16, 16) : (u128)state[31];
-    };
-    auto start = [&](u128 claimed) {
-      if (has_seed) {
-        Sha256::hash(seed, seed_len, state);
-      } else {
-        uint8_t b[16];
-        store_elem(b, es, claimed);
-        Sha256::hash(b, es, state);
-      }
-    };
 
     if (k == 0) {  // one row: the claimed sum is g at it, no rounds
       u128 h = 0;
@@ -853,34 +884,44 @@ int32_t prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k, 
     DevMem<uint4> d_a((m * n * es + 15) / 16, st), d_b((m * (n / 2) * es + 15) / 16, st);
     DevMem<uint32_t> d_vals(words, st);
     DevMem<uint4> d_rmul(wide ? 4096 : 0, st);
-    std::vector<uint32_t> h_vals(words);
+    // the device transcript's inputs and outputs: the Lagrange matrix, the seed, the
+    // state and challenge, the claimed sum and every round's coefficients
+    const size_t pts = dmax + 1;
+    std::vector<uint8_t> lag_b(pts * pts * es);
+    for (size_t a = 0; a < pts; ++a)
+      for (size_t d = 0; d < pts; ++d) store_elem(lag_b.data() + (a * pts + d) * es, es, lag[a][d]);
+    DevMem<uint8_t> d_lag(lag_b.size(), st), d_seed(has_seed ? seed_len : 0, st), d_claimed(es, st),
+        d_rounds(k * pts * es, st);
+    DevMem<ScTranscript> d_tx(1, st);
+    ZS_CUDA(cudaMemcpyAsync(d_lag.p, lag_b.data(), lag_b.size(), cudaMemcpyHostToDevice, st));
+    if (has_seed && seed_len) ZS_CUDA(cudaMemcpyAsync(d_seed.p, seed, seed_len, cudaMemcpyHostToDevice, st));
     ZS_CUDA(cudaMemcpyAsync(d_a.p, tables, m * n * es, cudaMemcpyHostToDevice, st));
+    const uint8_t* T = device_state(st).table;
 
+    // every round on the device, back to back: values, the transcript step, the fold
     void* cur = d_a.p;
     void* nxt = d_b.p;
     size_t len = n;
-    std::vector<u128> values(dmax + 1);
     for (size_t i = 0; i < k; ++i) {
       const size_t half = len / 2;
       values_async(wide, cur, len, half, dmax, tm, d_vals.p, st);
-      ZS_CUDA(cudaMemcpyAsync(h_vals.data(), d_vals.p, words * 4, cudaMemcpyDeviceToHost, st));
-      ZS_CUDA(cudaStreamSynchronize(st));
-      const uint8_t* vb = reinterpret_cast<const uint8_t*>(h_vals.data());
-      for (size_t t = 0; t <= dmax; ++t) values[t] = load_elem(vb + es * t, es);
-      if (i == 0) {  // the hypercube sum: g over the even rows plus g over the odd rows
-        const u128 h = values[0] ^ (dmax >= 1 ? values[1] : values[0]);
-        store_elem(claimed_out, es, h);
-        start(h);
-      }
-      const std::vector<u128> cs = interpolate(ht, level, values, lag);
-      for (size_t t = 0; t <= dmax; ++t) store_elem(rounds_out + es * ((dmax + 1) * i + t), es, cs[t]);
-      const u128 r = absorb(cs);
+      const uint8_t* vb = reinterpret_cast<const uint8_t*>(d_vals.p);
+      if (wide)
+        k_sc_step<true><<<1, 64, 0, st>>>(vb, d_lag.p, (uint32_t)pts, (uint32_t)i, T, d_seed.p, (uint32_t)seed_len,
+                                          has_seed ? 1 : 0, d_tx.p, d_claimed.p, d_rounds.p);
+      else
+        k_sc_step<false><<<1, 64, 0, st>>>(vb, d_lag.p, (uint32_t)pts, (uint32_t)i, T, d_seed.p, (uint32_t)seed_len,
+                                           has_seed ? 1 : 0, d_tx.p, d_claimed.p, d_rounds.p);
+      ZS_CUDA(cudaGetLastError());
       if (i + 1 < k) {
-        fold_async(wide, cur, len, m, r, nxt, d_rmul.p, st);
+        fold_async(wide, cur, len, m, 0, reinterpret_cast<const uint8_t*>(d_tx.p) + offsetof(ScTranscript, r), nxt,
+                   d_rmul.p, st);
         std::swap(cur, nxt);
       }
       len = half;
     }
+    ZS_CUDA(cudaMemcpyAsync(claimed_out, d_claimed.p, es, cudaMemcpyDeviceToHost, st));
+    ZS_CUDA(cudaMemcpyAsync(rounds_out, d_rounds.p, k * pts * es, cudaMemcpyDeviceToHost, st));
     ZS_CUDA(cudaStreamSynchronize(st));
   });
 }
@@ -928,7 +969,8 @@ extern "C" int32_t zs_binius_sumcheck_fold_device(uint32_t field_bits, const voi
                   reinterpret_cast<uintptr_t>(d_scratch)) & 15))
       throw zs::Error(zs::ZS_EMALFORMED, "misaligned buffer");
     if (len > 0xffffffffu || m == 0 || m > zs::kMaxTables) throw zs::Error(zs::ZS_EMALFORMED, "table shape");
-    zs::fold_async(wide, d_cur, len, m, zs::load_elem(r, wide ? 16 : 1), d_next, static_cast<uint4*>(d_scratch),
+    zs::fold_async(wide, d_cur, len, m, zs::load_elem(r, wide ? 16 : 1), nullptr, d_next,
+                   static_cast<uint4*>(d_scratch),
                    (cudaStream_t)stream);
   });
 }
