@@ -501,62 +501,52 @@ __constant__ uint32_t kSha256K[64] = {
     0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a, 0x5b9cca4f, 0x682e6ff3,
     0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7, 0xc67178f2};
 
-// SHA-256 (FIPS 180-4) in one thread: update over byte runs, then final.
-struct Sha256Dev {
-  uint32_t h[8];
-  uint8_t buf[64];
-  uint32_t fill;
-  uint64_t total;
-  __device__ void init() {
-    h[0] = 0x6a09e667, h[1] = 0xbb67ae85, h[2] = 0x3c6ef372, h[3] = 0xa54ff53a;
-    h[4] = 0x510e527f, h[5] = 0x9b05688c, h[6] = 0x1f83d9ab, h[7] = 0x5be0cd19;
-    fill = 0;
-    total = 0;
-  }
-  __device__ static uint32_t rotr(uint32_t x, unsigned r) { return __funnelshift_r(x, x, r); }
-  __device__ void block() {
-    uint32_t w[64];
-    for (int i = 0; i < 16; ++i)
-      w[i] = (uint32_t)buf[4 * i] << 24 | (uint32_t)buf[4 * i + 1] << 16 | (uint32_t)buf[4 * i + 2] << 8 |
-             buf[4 * i + 3];
-    for (int i = 16; i < 64; ++i) {
-      const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
-      const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
-      w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+// SHA-256 (FIPS 180-4) of the message prefix || body in one thread. Each 64-byte block's
+// words are assembled from the message bytes (and the padding, computed on the fly), and
+// the 64 rounds are unrolled so the message schedule stays in registers.
+__device__ __forceinline__ uint32_t sha_rotr(uint32_t x, unsigned r) { return __funnelshift_r(x, x, r); }
+
+__device__ void sha256_dev(const uint8_t* prefix, uint32_t plen, const uint8_t* body, uint32_t blen,
+                           uint8_t out[32]) {
+  uint32_t h[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a, 0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+  const uint64_t len = (uint64_t)plen + blen;
+  const uint64_t nblocks = (len + 9 + 63) / 64;
+  const uint64_t bits = len * 8;
+  auto byte_at = [&](uint64_t i) -> uint32_t {
+    if (i < plen) return prefix[i];
+    if (i < len) return body[i - plen];
+    if (i == len) return 0x80;
+    const uint64_t end = nblocks * 64;
+    if (i >= end - 8) return (uint32_t)(bits >> (8 * (end - 1 - i))) & 0xff;
+    return 0;
+  };
+  for (uint64_t blk = 0; blk < nblocks; ++blk) {
+    uint32_t w[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const uint64_t o = blk * 64 + 4 * i;
+      w[i] = byte_at(o) << 24 | byte_at(o + 1) << 16 | byte_at(o + 2) << 8 | byte_at(o + 3);
     }
     uint32_t a = h[0], b = h[1], c = h[2], d = h[3], e = h[4], f = h[5], g = h[6], hh = h[7];
+#pragma unroll
     for (int i = 0; i < 64; ++i) {
-      const uint32_t t1 = hh + (rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25)) + ((e & f) ^ (~e & g)) + kSha256K[i] + w[i];
-      const uint32_t t2 = (rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+      if (i >= 16) {
+        const uint32_t x = w[(i - 15) & 15], y = w[(i - 2) & 15];
+        w[i & 15] += (sha_rotr(x, 7) ^ sha_rotr(x, 18) ^ (x >> 3)) + w[(i - 7) & 15] +
+                     (sha_rotr(y, 17) ^ sha_rotr(y, 19) ^ (y >> 10));
+      }
+      const uint32_t t1 =
+          hh + (sha_rotr(e, 6) ^ sha_rotr(e, 11) ^ sha_rotr(e, 25)) + ((e & f) ^ (~e & g)) + kSha256K[i] + w[i & 15];
+      const uint32_t t2 = (sha_rotr(a, 2) ^ sha_rotr(a, 13) ^ sha_rotr(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
       hh = g, g = f, f = e, e = d + t1, d = c, c = b, b = a, a = t1 + t2;
     }
     h[0] += a, h[1] += b, h[2] += c, h[3] += d, h[4] += e, h[5] += f, h[6] += g, h[7] += hh;
   }
-  __device__ void update(const uint8_t* p, uint32_t n) {
-    total += n;
-    for (uint32_t i = 0; i < n; ++i) {
-      buf[fill++] = p[i];
-      if (fill == 64) {
-        block();
-        fill = 0;
-      }
-    }
-  }
-  __device__ void final(uint8_t out[32]) {
-    const uint64_t bits = total * 8;
-    buf[fill++] = 0x80;
-    if (fill > 56) {
-      while (fill < 64) buf[fill++] = 0;
-      block();
-      fill = 0;
-    }
-    while (fill < 56) buf[fill++] = 0;
-    for (int i = 0; i < 8; ++i) buf[56 + i] = (uint8_t)(bits >> (56 - 8 * i));
-    block();
-    for (int i = 0; i < 8; ++i)
-      for (int j = 0; j < 4; ++j) out[4 * i + j] = (uint8_t)(h[i] >> (24 - 8 * j));
-  }
-};
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) out[4 * i + j] = (uint8_t)(h[i] >> (24 - 8 * j));
+}
 
 // The device transcript: the SHA-256 state (32 bytes) and the last challenge (1 or 16
 // bytes), in device memory between rounds.
@@ -565,11 +555,14 @@ struct ScTranscript {
   uint8_t r[16];
 };
 
-// Round `round`'s step: coefficient d = sum_i values[i] * lag[i][d] for d < n (one lane
-// per coefficient, the product table in global memory), written to rounds_out; the first
-// round also forms the claimed sum (values[0] + values[1]) and starts the transcript
-// (from `seed`, or from the claimed sum); thread 0 absorbs the coefficients and samples
-// the challenge (the digest's last byte over GF(2^8), its last 16 bytes over GF(2^128)).
+// Round `round`'s step. The points 0..n-1 lie in GF(2^8), so the Lagrange matrix `lag`
+// (n x n bytes) does too, and coefficient d = sum_i values[i] * lag[i][d] takes products by
+// a subfield scalar (one lookup over GF(2^8), 16 independent ones over GF(2^128)); one lane
+// per coefficient, the product table in global memory. The coefficients go to rounds_out;
+// the first round also forms the claimed sum (values[0] + values[1]) and starts the
+// transcript (from `seed`, or from the claimed sum); then thread 0 absorbs the
+// coefficients and samples the challenge (the digest's last byte over GF(2^8), its last
+// 16 bytes over GF(2^128)).
 template <bool WIDE>
 __global__ void __launch_bounds__(64) k_sc_step(const uint8_t* __restrict__ vals, const uint8_t* __restrict__ lag,
                                                 uint32_t n, uint32_t round, const uint8_t* __restrict__ gT,
@@ -577,50 +570,49 @@ __global__ void __launch_bounds__(64) k_sc_step(const uint8_t* __restrict__ vals
                                                 ScTranscript* __restrict__ tx, uint8_t* __restrict__ claimed,
                                                 uint8_t* __restrict__ rounds_out) {
   constexpr uint32_t ES = WIDE ? 16 : 1;
-  __shared__ uint8_t s_coef[kProveMaxPoints * 16];
+  __shared__ uint8_t s_msg[32 + kProveMaxPoints * 16];  // the absorbed message: state || coefficients
   const Tower F{gT};
-  auto ld = [](const uint8_t* p) {
-    uint64_t lo = 0, hi = 0;
-    for (int b = 7; b >= 0; --b) lo = (lo << 8) | p[b], hi = (hi << 8) | p[8 + b];
-    return g128{lo, hi};
-  };
   for (uint32_t d = threadIdx.x; d < n; d += blockDim.x) {
-    uint8_t* out = s_coef + ES * d;
+    uint8_t* out = s_msg + 32 + ES * d;
     if constexpr (WIDE) {
-      g128 acc{0, 0};
+      uint64_t lo = 0, hi = 0;
       for (uint32_t i = 0; i < n; ++i) {
-        const g128 v = ld(vals + 16 * i);
-        if (v.lo | v.hi) acc = gxor(acc, F.m128(v, ld(lag + 16 * ((size_t)i * n + d))));
+        const uint32_t c = lag[(size_t)i * n + d];
+        const uint8_t* v = vals + 16 * i;
+        uint64_t vlo = 0, vhi = 0;
+#pragma unroll
+        for (int b = 7; b >= 0; --b) vlo = (vlo << 8) | v[b], vhi = (vhi << 8) | v[8 + b];
+        lo ^= F.s64(c, vlo);
+        hi ^= F.s64(c, vhi);
       }
-      for (int b = 0; b < 8; ++b) out[b] = (uint8_t)(acc.lo >> (8 * b)), out[8 + b] = (uint8_t)(acc.hi >> (8 * b));
+#pragma unroll
+      for (int b = 0; b < 8; ++b) out[b] = (uint8_t)(lo >> (8 * b)), out[8 + b] = (uint8_t)(hi >> (8 * b));
     } else {
       uint32_t acc = 0;
-      for (uint32_t i = 0; i < n; ++i) acc ^= F.m8(vals[i], lag[(size_t)i * n + d]);
+      for (uint32_t i = 0; i < n; ++i) acc ^= F.m8(lag[(size_t)i * n + d], vals[i]);
       out[0] = (uint8_t)acc;
     }
     for (uint32_t b = 0; b < ES; ++b) rounds_out[((size_t)round * n + d) * ES + b] = out[b];
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
-  Sha256Dev sh;
   if (round == 0) {
     uint8_t h[16];
     for (uint32_t b = 0; b < ES; ++b) {  // one point: the sum of 2^k copies of a constant is 0
       h[b] = n >= 2 ? (uint8_t)(vals[b] ^ vals[ES + b]) : 0;
       claimed[b] = h[b];
     }
-    sh.init();
     if (has_seed)
-      sh.update(seed, seed_len);
+      sha256_dev(seed, seed_len, nullptr, 0, s_msg);
     else
-      sh.update(h, ES);
-    sh.final(tx->state);
+      sha256_dev(h, ES, nullptr, 0, s_msg);
+  } else {
+    for (int b = 0; b < 32; ++b) s_msg[b] = tx->state[b];
   }
-  sh.init();
-  sh.update(tx->state, 32);
-  sh.update(s_coef, n * ES);
-  sh.final(tx->state);
-  for (uint32_t b = 0; b < ES; ++b) tx->r[b] = WIDE ? tx->state[16 + b] : tx->state[31];
+  uint8_t st[32];
+  sha256_dev(s_msg, 32 + n * ES, nullptr, 0, st);
+  for (int b = 0; b < 32; ++b) tx->state[b] = st[b];
+  for (uint32_t b = 0; b < ES; ++b) tx->r[b] = WIDE ? st[16 + b] : st[31];
 }
 
 // ---- host: argument checks and launches -------------------------------------------
@@ -876,7 +868,7 @@ int32_t prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k, 
       return;
     }
 
-    const std::vector<std::vector<u128>> lag = lagrange_matrix(ht, level, dmax + 1);
+    const std::vector<std::vector<u128>> lag = lagrange_matrix(ht, 3, dmax + 1);  // in GF(2^8) (points < 256)
 
     cudaStream_t st = (cudaStream_t)stream;
     retain_pool_memory();
@@ -887,9 +879,9 @@ int32_t prove_combination(uint32_t field_bits, const uint8_t* tables, size_t k, 
     // the device transcript's inputs and outputs: the Lagrange matrix, the seed, the
     // state and challenge, the claimed sum and every round's coefficients
     const size_t pts = dmax + 1;
-    std::vector<uint8_t> lag_b(pts * pts * es);
+    std::vector<uint8_t> lag_b(pts * pts);  // GF(2^8) entries: the points lie in GF(2^8)
     for (size_t a = 0; a < pts; ++a)
-      for (size_t d = 0; d < pts; ++d) store_elem(lag_b.data() + (a * pts + d) * es, es, lag[a][d]);
+      for (size_t d = 0; d < pts; ++d) lag_b[a * pts + d] = (uint8_t)lag[a][d];
     DevMem<uint8_t> d_lag(lag_b.size(), st), d_seed(has_seed ? seed_len : 0, st), d_claimed(es, st),
         d_rounds(k * pts * es, st);
     DevMem<ScTranscript> d_tx(1, st);
