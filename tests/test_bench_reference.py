@@ -1,6 +1,6 @@
 """The bench's reference arm on CPU: `bench.py --impl reference` times the oracle port of
 the reference's CPU algorithm on a bounded sample of the commit workload and prints one
-JSON line with the same metric, unit and direction as the GPU arm."""
+JSON line with the same metric, unit, direction and config as the GPU arm."""
 import json
 import os
 import subprocess
@@ -24,6 +24,9 @@ def test_reference_arm_json_line():
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
     assert d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"] == {"value": d["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # the GPU arm's config, with the sample described in cpu_baseline
+    assert d["config"] == bench.commit_config(bench.LOG_ROWS, 1)
+    assert "2^16" in d["cpu_baseline"]["sample"]
 
 
 def test_reference_arm_under_torchrun_two_ranks():
