@@ -20,9 +20,10 @@
 // Each transform is split into HBM passes over groups held in shared memory: the
 // butterflies of layers [0, K) connect elements inside aligned runs of 2^K
 // positions, layers [K, lg) connect elements that share the low K position bits.
-// Inside a pass, each thread moves 2^r elements (r <= 4 layers) between shared
+// Inside a pass, each thread moves 2^r elements (r <= 5 layers) between shared
 // memory and registers per chunk, so a pass costs one shared-memory round trip per
-// four layers. Every butterfly is the reference's exact M31 butterfly with the
+// five layers; for groups of 2^10 the chunks next to global memory load and store
+// their registers directly, and shared memory carries only the transpose between them. Every butterfly is the reference's exact M31 butterfly with the
 // reference's twiddle, so outputs are bit-identical.
 #include "circle.cuh"
 
@@ -508,6 +509,85 @@ __global__ void __launch_bounds__(kLowThreads, 3) k_low(const uint32_t* __restri
   }
 }
 
+// Groups of 2^10 elements in two 5-layer chunks, 8 groups per batch, 256 threads. The
+// chunks take two thread layouts over a batch:
+//   strided:     group gs = tid / 32, r = tid % 32, elements r + 32 m;
+//   consecutive: group gc = tid % 8,  r = tid / 8,  elements 32 r + m   (m < 32).
+// The chunk next to a global-memory side moves its 32 values between registers and
+// global memory directly, in the layout that keeps that side coalesced (strided for a
+// contiguous group: 128-byte rows; consecutive for the bit-reversed order and the
+// middle pass's interleaved groups: 8 groups' words side by side), so shared memory
+// only carries the transpose between the two chunks. Groups sit kGS10 words apart;
+// kGS10 = 4 (mod 32) and padx() put both layouts' 32 lanes on 32 distinct banks.
+constexpr uint32_t kGS10 = 1060;
+constexpr size_t kBatch10Words = 8 * kGS10;
+
+__device__ __forceinline__ uint32_t* strided_at(uint32_t* s, uint32_t gs, uint32_t r) { return s + gs * kGS10 + r; }
+__device__ __forceinline__ uint32_t* consecutive_at(uint32_t* s, uint32_t gc, uint32_t r) {
+  return s + gc * kGS10 + 33 * r;
+}
+
+// k_low for K = 10, G = 8 (every size-2^LG transform with LG >= 13 that splits at 10):
+// the same layers and orders, one barrier per batch, the batches alternating between two
+// shared buffers (batch j + 2 overwrites batch j's buffer only after every thread has
+// passed batch j + 1's barrier, so after batch j's reads).
+template <bool INV>
+__global__ void __launch_bounds__(kLowThreads, 3) k_low10(const uint32_t* __restrict__ src, size_t src_stride,
+                                                        uint32_t* __restrict__ dst, size_t dst_stride, unsigned LG,
+                                                        unsigned iters, const uint32_t* __restrict__ TW) {
+  extern __shared__ uint32_t sm[];
+  const uint32_t N = 1u << LG;
+  const unsigned hb = LG - 10;
+  const uint32_t* col = src + (size_t)blockIdx.y * src_stride;
+  uint32_t* out = dst + (size_t)blockIdx.y * dst_stride;
+  const uint32_t gs = threadIdx.x >> 5, rs = threadIdx.x & 31;
+  const uint32_t gc = threadIdx.x & 7, rc = threadIdx.x >> 3;
+  // element 32 rc + m of a group is bit-reversed row ((bitrev_5(m) << 5) | bitrev_5(rc))
+  const size_t brc_row = (size_t)(__brev(rc) >> 27) << hb;
+  for (uint32_t j = 0; j < iters; ++j) {
+    uint32_t* s = sm + (j & 1) * kBatch10Words;
+    const uint32_t g0 = (blockIdx.x * iters + j) * 8;
+    uint32_t v[32];
+    if (!INV) {
+      // layers [5, 10) on contiguous groups, then [0, 5), stored in bit-reversed order
+      const uint32_t vs = bitrev(g0 + gs, hb);
+      const uint32_t* gp = col + ((size_t)vs << 10) + rs;
+#pragma unroll
+      for (int m = 0; m < 32; ++m) v[m] = __ldg(gp + 32 * m);
+      chunk_layers<5, false, 0>(v, TW, N, 5, vs);
+      uint32_t* wp = strided_at(s, gs, rs);
+#pragma unroll
+      for (int m = 0; m < 32; ++m) wp[33 * m] = v[m];
+      __syncthreads();
+      const uint32_t* rp = consecutive_at(s, gc, rc);
+#pragma unroll
+      for (int m = 0; m < 32; ++m) v[m] = rp[m];
+      chunk_layers<5, false, 0>(v, TW, N, 0, (bitrev(g0 + gc, hb) << 5) + rc);
+      uint32_t* op = out + brc_row + g0 + gc;
+#pragma unroll
+      for (int m = 0; m < 32; ++m) op[(size_t)cbitrev(m, 5) << (hb + 5)] = v[m];
+    } else {
+      // layers [0, 5) read in bit-reversed order, then [5, 10), stored contiguous
+      const uint32_t* gp = col + brc_row + g0 + gc;
+#pragma unroll
+      for (int m = 0; m < 32; ++m) v[m] = __ldg(gp + ((size_t)cbitrev(m, 5) << (hb + 5)));
+      chunk_layers<5, true, 0>(v, TW, N, 0, (bitrev(g0 + gc, hb) << 5) + rc);
+      uint32_t* wp = consecutive_at(s, gc, rc);
+#pragma unroll
+      for (int m = 0; m < 32; ++m) wp[m] = v[m];
+      __syncthreads();
+      const uint32_t* rp = strided_at(s, gs, rs);
+#pragma unroll
+      for (int m = 0; m < 32; ++m) v[m] = rp[33 * m];
+      const uint32_t vs = bitrev(g0 + gs, hb);
+      chunk_layers<5, true, 0>(v, TW, N, 5, vs);
+      uint32_t* op = out + ((size_t)vs << 10) + rs;
+#pragma unroll
+      for (int m = 0; m < 32; ++m) op[32 * m] = v[m];
+    }
+  }
+}
+
 // Middle pass over groups that share the low K position bits (M = L - K layers).
 //   mode LDE:       inverse layers [K, L), scale 1/n, then for each of the 2^B
 //                   quarters the forward layers [K, L) of the size-2^(L+B) transform
@@ -566,6 +646,54 @@ __global__ void __launch_bounds__(kMidThreads, 3) k_mid(const uint32_t* __restri
   const uint32_t lo0 = blockIdx.x * G;
   const uint32_t* src = in + (size_t)blockIdx.y * in_stride;
   uint32_t* dst = out + (size_t)blockIdx.y * out_stride;
+  if constexpr (FAST) {
+    if (mode == MID_LDE && KC == 10 && MC == 10 && GC == 8) {
+      // Two chunks per transform in the layouts of k_low10: the inverse's first chunk
+      // reads global memory in the consecutive layout, its second chunk ends in the
+      // strided layout, which is where each quarter's first forward chunk starts, so a
+      // thread keeps its scaled inverse values in its own strided slots of s_in (no
+      // barrier: only it reads them back); each quarter's second chunk writes global
+      // memory from the consecutive layout. Element hi of group t is global word
+      // (hi << 10) + lo0 + t.
+      uint32_t* s_q = sm + kBatch10Words;
+      const uint32_t gs = threadIdx.x >> 5, rs = threadIdx.x & 31;
+      const uint32_t gc = threadIdx.x & 7, rc = threadIdx.x >> 3;
+      const unsigned inv_n_shift = (31 - L) % 31;
+      const size_t io = ((size_t)rc << 15) + lo0 + gc;  // hi = 32 rc + m
+      uint32_t v[32];
+#pragma unroll
+      for (int m = 0; m < 32; ++m) v[m] = __ldg(src + io + ((size_t)m << 10));
+      chunk_layers<5, true, 0>(v, ITW_small, n, 10, rc);
+      uint32_t* cp = consecutive_at(s_in, gc, rc);
+#pragma unroll
+      for (int m = 0; m < 32; ++m) cp[m] = v[m];
+      __syncthreads();
+      uint32_t* sp = strided_at(s_in, gs, rs);
+#pragma unroll
+      for (int m = 0; m < 32; ++m) v[m] = sp[33 * m];
+      chunk_layers<5, true, 0>(v, ITW_small, n, 15, 0);
+#pragma unroll
+      for (int m = 0; m < 32; ++m) sp[33 * m] = mshl(v[m], inv_n_shift);
+      uint32_t* wq = strided_at(s_q, gs, rs);
+      const uint32_t* rq = consecutive_at(s_q, gc, rc);
+      for (uint32_t q = 0; q < (1u << B); ++q) {
+#pragma unroll
+        for (int m = 0; m < 32; ++m) v[m] = sp[33 * m];
+        chunk_layers<5, false, 0>(v, TW_big, n << B, 15, q);
+#pragma unroll
+        for (int m = 0; m < 32; ++m) wq[33 * m] = v[m];
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < 32; ++m) v[m] = rq[m];
+        chunk_layers<5, false, 0>(v, TW_big, n << B, 10, (q << 5) + rc);
+        uint32_t* dq = dst + (size_t)q * n + io;
+#pragma unroll
+        for (int m = 0; m < 32; ++m) dq[(size_t)m << 10] = v[m];
+        __syncthreads();  // s_q is rewritten by the next quarter
+      }
+      return;
+    }
+  }
   const unsigned lg_g = 31 - __clz(G);
   if (threadIdx.x < G) vb[threadIdx.x] = 0;
   if (mode == MID_FFT_ONLY) {
@@ -656,10 +784,10 @@ void launch_low(const uint32_t* src, size_t src_stride, uint32_t* dst, size_t ds
   unsigned iters = 1;
   while (iters < 8 && batches % (iters * 2) == 0 && batches / (iters * 2) >= 16) iters *= 2;
   const size_t sb = ((size_t)2 * G * group_stride(K) + 2 * G) * sizeof(uint32_t);
-  if (K == 10 && G == 8) {  // the 2^20 -> 2^22 LDE's groups: compile-time layout
-    set_smem((const void*)k_low<INV, 10, 8>, sb);
-    k_low<INV, 10, 8><<<dim3(batches / iters, C), kLowThreads, sb, st>>>(src, src_stride, dst, dst_stride, LG, K, G,
-                                                                         iters, tw);
+  if (K == 10 && G == 8) {  // groups of 2^10 (every LG >= 13 split at 10): register-direct chunks
+    const size_t sb10 = 2 * kBatch10Words * sizeof(uint32_t);
+    set_smem((const void*)k_low10<INV>, sb10);
+    k_low10<INV><<<dim3(batches / iters, C), kLowThreads, sb10, st>>>(src, src_stride, dst, dst_stride, LG, iters, tw);
   } else {
     set_smem((const void*)k_low<INV>, sb);
     k_low<INV><<<dim3(batches / iters, C), kLowThreads, sb, st>>>(src, src_stride, dst, dst_stride, LG, K, G, iters,
@@ -672,9 +800,10 @@ void launch_mid(const uint32_t* in, size_t in_stride, uint32_t* out, size_t out_
   const unsigned M = L - K;
   const uint32_t ngroups = 1u << K;
   const unsigned G = pick_groups(M, ngroups, kGroupWords / 2);
-  const size_t sb = smem_bytes(M, G, 2);
+  size_t sb = smem_bytes(M, G, 2);
   const dim3 grid(ngroups / G, C);
   if (K == 10 && M == 10 && G == 8) {  // the 2^20 -> 2^22 LDE: compile-time layout
+    sb = std::max(sb, 2 * kBatch10Words * sizeof(uint32_t));
     set_smem((const void*)k_mid<10, 10, 8>, sb);
     k_mid<10, 10, 8><<<grid, kMidThreads, sb, st>>>(in, in_stride, out, out_stride, L, K, B, G, itw, tw, mode);
   } else {
