@@ -30,6 +30,10 @@ sys.path.insert(0, os.path.join(ROOT, "zig-stark_b200"))
 N_COLS, LOG_ROWS, LOG_BLOWUP, N_FOLDS = 64, 20, 2, 16
 METRIC = "M31 LDE+Merkle commit rows/s (64 cols x 2^20, blowup 4, + 16-fold FRI chain)"
 UNIT = "rows/s"
+# The oracle's LDE root of the timed workload (oracle.circle_commit on
+# workload.commit_inputs(64, 20, 16), blowup 4), so the timed configuration is checked
+# against the oracle without running it at full size on every bench.
+ORACLE_LDE_ROOT = {20: "0482a2ea4854035e11838b72cc7360faaacf1779a8d52908dd28ccba2b1cb397"}
 
 
 def parse():
@@ -739,9 +743,10 @@ def main():
     plan.upload(pinned.data_ptr(), sp)
     torch.cuda.synchronize()
 
-    # correctness of the timed configuration: the first run against a stored digest
+    # correctness of the timed configuration: the first run against the oracle's root
     plan.run(None, sp)
     ref_root = plan.results(sp)["lde_root"]
+    root_ok = ref_root.hex() == ORACLE_LDE_ROOT[log_rows] if log_rows in ORACLE_LDE_ROOT else None
 
     def timed(fn, k):
         barrier(world)
@@ -908,6 +913,7 @@ def main():
         "vs_baseline": None, "dtype": "u32 (M31 / QM31 exact)", "data": "synthetic (SplitMix64 seeded)",
         "config": commit_config(log_rows, world),
         "phases_ms": phase_ms,
+        "parity": {"lde_root_equal_oracle": root_ok},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": traffic,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
