@@ -250,6 +250,27 @@ __device__ __forceinline__ void load_twiddles(uint32_t* dst, const uint32_t* __r
   }
 }
 
+// The butterflies of local layer l of a chunk on the 2^R values in registers, with the
+// layer's 2^(R-1-l) twiddles in tws.
+template <int R, bool INV, int l>
+__device__ __forceinline__ void layer_butterflies(uint32_t* v, const uint32_t* tws) {
+#pragma unroll
+  for (int m0 = 0; m0 < (1 << R); ++m0) {
+    if (m0 & (1 << l)) continue;
+    const int m1 = m0 | (1 << l);
+    const uint32_t t = tws[m0 >> (l + 1)];
+    if (!INV) {
+      const uint32_t x1 = mmul2(v[m1], t), x0 = v[m0];
+      v[m1] = msub(x0, x1);
+      v[m0] = madd(x0, x1);
+    } else {
+      const uint32_t x0 = v[m0], x1 = v[m1];
+      v[m0] = madd(x0, x1);
+      v[m1] = mmul2(msub(x0, x1), t);
+    }
+  }
+}
+
 // The R layers of one chunk on the 2^R values in registers: layer LL of the chunk's
 // order (top-down forward, bottom-up inverse), then the rest. base_i: the global layer
 // of the chunk's lowest layer; Vh: the virtual block index of the slot's lowest
@@ -262,22 +283,64 @@ __device__ __forceinline__ void chunk_layers(uint32_t* v, const uint32_t* __rest
     const unsigned i = base_i + l;
     uint32_t tws[1 << (R - 1 - l)];
     load_twiddles<(1 << (R - 1 - l))>(tws, TW + (n_dom - (n_dom >> i)) + (Vh << (R - l - 1)));
-#pragma unroll
-    for (int m0 = 0; m0 < (1 << R); ++m0) {
-      if (m0 & (1 << l)) continue;
-      const int m1 = m0 | (1 << l);
-      const uint32_t t = tws[m0 >> (l + 1)];
-      if (!INV) {
-        const uint32_t x1 = mmul2(v[m1], t), x0 = v[m0];
-        v[m1] = msub(x0, x1);
-        v[m0] = madd(x0, x1);
-      } else {
-        const uint32_t x0 = v[m0], x1 = v[m1];
-        v[m0] = madd(x0, x1);
-        v[m1] = mmul2(msub(x0, x1), t);
-      }
-    }
+    layer_butterflies<R, INV, l>(v, tws);
     chunk_layers<R, INV, LL + 1>(v, TW, n_dom, base_i, Vh);
+  }
+}
+
+// The circle layer (global layer 0) on 32 values in registers whose twiddles at layer 0
+// start at block 16 Vh, with the first line layer's eight twiddles t1 = T_1[8 Vh ..]. A
+// table of lg >= 3 holds at layer-0 entries 4k .. 4k + 3 the values f1, -f1, -f0, f0 of
+// its layer-1 entries f0 = T_1[2k], f1 = T_1[2k + 1] (k_tw_circle_layer; the inverse
+// table, elementwise inverses, keeps the pattern), so layer 0 needs no loads of its own:
+// a butterfly with the negated twiddle swaps its two outputs (forward) or the operands
+// of its subtraction (inverse), and gives the same canonical values.
+template <bool INV>
+__device__ __forceinline__ void circle_layer32(uint32_t* v, const uint32_t* t1) {
+#pragma unroll
+  for (int hb = 0; hb < 16; ++hb) {
+    const int m0 = 2 * hb, m1 = m0 + 1, j = hb & 3;
+    const uint32_t t = t1[2 * (hb >> 2) + (j < 2 ? 1 : 0)];
+    const bool neg = j == 1 || j == 2;
+    if (!INV) {
+      const uint32_t y = mmul2(v[m1], t), x0 = v[m0];
+      v[m1] = neg ? madd(x0, y) : msub(x0, y);
+      v[m0] = neg ? msub(x0, y) : madd(x0, y);
+    } else {
+      const uint32_t x0 = v[m0], x1 = v[m1];
+      v[m0] = madd(x0, x1);
+      v[m1] = mmul2(neg ? msub(x1, x0) : msub(x0, x1), t);
+    }
+  }
+}
+
+// Global layers [0, 5) of a size-N transform (lg >= 3) on 32 values in registers whose
+// top virtual block is Vh: chunk_layers<5, INV, 0>(v, TW, N, 0, Vh) with the circle
+// layer's twiddles taken from the first line layer's.
+template <bool INV>
+__device__ __forceinline__ void low_chunk32(uint32_t* v, const uint32_t* __restrict__ TW, uint32_t N, uint32_t Vh) {
+  uint32_t t1[8];
+  load_twiddles<8>(t1, TW + (N >> 1) + (Vh << 3));
+  if (INV) {
+    circle_layer32<true>(v, t1);
+    layer_butterflies<5, true, 1>(v, t1);
+    uint32_t t2[4], t3[2], t4[1];
+    load_twiddles<4>(t2, TW + (N - (N >> 2)) + (Vh << 2));
+    layer_butterflies<5, true, 2>(v, t2);
+    load_twiddles<2>(t3, TW + (N - (N >> 3)) + (Vh << 1));
+    layer_butterflies<5, true, 3>(v, t3);
+    load_twiddles<1>(t4, TW + (N - (N >> 4)) + Vh);
+    layer_butterflies<5, true, 4>(v, t4);
+  } else {
+    uint32_t t2[4], t3[2], t4[1];
+    load_twiddles<1>(t4, TW + (N - (N >> 4)) + Vh);
+    layer_butterflies<5, false, 4>(v, t4);
+    load_twiddles<2>(t3, TW + (N - (N >> 3)) + (Vh << 1));
+    layer_butterflies<5, false, 3>(v, t3);
+    load_twiddles<4>(t2, TW + (N - (N >> 2)) + (Vh << 2));
+    layer_butterflies<5, false, 2>(v, t2);
+    layer_butterflies<5, false, 1>(v, t1);
+    circle_layer32<false>(v, t1);
   }
 }
 
@@ -582,7 +645,7 @@ __global__ void __launch_bounds__(kLowThreads, 2) k_low10(const uint32_t* __rest
       const uint32_t* rp = consecutive_at(s, gc, rc);
 #pragma unroll
       for (int m = 0; m < 32; ++m) v[m] = rp[m];
-      chunk_layers<5, false, 0>(v, TW, N, 0, (bitrev(g0 + gc, hb) << 5) + rc);
+      low_chunk32<false>(v, TW, N, (bitrev(g0 + gc, hb) << 5) + rc);
       uint32_t* op = out + brc_row + g0 + gc;
 #pragma unroll
       for (int m = 0; m < 32; ++m) op[(size_t)cbitrev(m, 5) << (hb + 5)] = v[m];
@@ -595,7 +658,7 @@ __global__ void __launch_bounds__(kLowThreads, 2) k_low10(const uint32_t* __rest
 #pragma unroll
         for (int m = 0; m < 32; ++m) w[m] = __ldg(gp + ((size_t)cbitrev(m, 5) << (hb + 5)));
       }
-      chunk_layers<5, true, 0>(v, TW, N, 0, (bitrev(g0 + gc, hb) << 5) + rc);
+      low_chunk32<true>(v, TW, N, (bitrev(g0 + gc, hb) << 5) + rc);
       uint32_t* wp = consecutive_at(s, gc, rc);
 #pragma unroll
       for (int m = 0; m < 32; ++m) wp[m] = v[m];
