@@ -879,9 +879,13 @@ def main():
     }
     dom = max(phase_ms, key=phase_ms.get)
     achieved = alg[dom] / (phase_ms[dom] / 1e3) / 1e9
-    # DRAM read + write bytes of the LDE's three kernels from an ncu capture of this
-    # workload at 2^19 rows (1.98 GB), scaled by the rows; the other phases have none.
-    traffic = {"lde": 1.9825e9 * 2.0 ** (log_rows - 19)}.get(dom)
+    # DRAM read + write bytes per launch of each phase's kernels from ncu, scaled by the
+    # rows. LDE: its three kernels at 32 columns x 2^20 rows (1.945 GB; the intermediate
+    # buffers are larger than L2 there too) scaled to 64 columns. Row leaves + trees: the
+    # row leaves and the row and g trees at 32 columns (845.1 MB read, 428.5 MB written)
+    # plus the second half of the LDE read (536.9 MB), their only column-dependent term.
+    traffic = {"lde": 1.9454e9 * (N_COLS / 32) * 2.0 ** (log_rows - 20),
+               "row_tree": 1.8105e9 * 2.0 ** (log_rows - 20)}.get(dom)
     # Integer co-roof. The path is exact integer work, so next to the HBM roof each phase
     # is set against the SMs' issue rate (148 SMs x 4 schedulers x 1 warp instruction per
     # cycle at the sampled SM clock) and against the ALU pipe's (a warp instruction every
@@ -890,7 +894,7 @@ def main():
     # sm__inst_executed_pipe_alu.sum of one step at 64 x 2^20; the capture and the
     # per-kernel figures are in profiles/circle_commit_64x2p20.md), over the CUDA-event
     # phase time of this run. Other row counts scale the counts by the rows (marked).
-    counted = {"lde": (1052.4e6, 512.5e6), "row_tree": (1059.4e6, 735.3e6), "folds": (342.0e6, 237.1e6)}
+    counted = {"lde": (946.8e6, 488.4e6), "row_tree": (1059.4e6, 735.3e6), "folds": (342.0e6, 237.1e6)}
     cs = clocks.summary()
     sm_mhz = cs.get("sm_mhz") or cs.get("sm_max_mhz") or 1965.0
     n_sm = torch.cuda.get_device_properties(local).multi_processor_count
