@@ -882,10 +882,10 @@ def main():
     # DRAM read + write bytes per launch of each phase's kernels from ncu, scaled by the
     # rows. LDE: its three kernels at 32 columns x 2^20 rows (1.945 GB; the intermediate
     # buffers are larger than L2 there too) scaled to 64 columns. Row leaves + trees: the
-    # row leaves and the row and g trees at 32 columns (845.1 MB read, 428.5 MB written)
-    # plus the second half of the LDE read (536.9 MB), their only column-dependent term.
+    # row leaves and the row and g trees of this workload (1381.5 MB read, 443.0 MB
+    # written; one pass per launch, checked on the 32-column case first).
     traffic = {"lde": 1.9454e9 * (N_COLS / 32) * 2.0 ** (log_rows - 20),
-               "row_tree": 1.8105e9 * 2.0 ** (log_rows - 20)}.get(dom)
+               "row_tree": 1.8245e9 * 2.0 ** (log_rows - 20)}.get(dom)
     # Integer co-roof. The path is exact integer work, so next to the HBM roof each phase
     # is set against the SMs' issue rate (148 SMs x 4 schedulers x 1 warp instruction per
     # cycle at the sampled SM clock) and against the ALU pipe's (a warp instruction every
