@@ -44,6 +44,26 @@ def test_commit_matches_oracle(orc, n_cols, log_rows, log_blowup, n_folds):
     assert np.array_equal(one["final_layer"], want["final_layer"])
 
 
+@pytest.mark.parametrize("log_blowup", [0, 1, 3])
+def test_commit_2p20_rows_each_blowup_matches_oracle(orc, log_blowup):
+    """2^20 rows run the middle pass's compile-time layout (groups of 2^10 on both
+    sides), whose quarter loop runs 2^log_blowup times: the LDE bytes against the oracle
+    for one, two and eight quarters (the full-size test covers four)."""
+    from zs_b200 import native
+    trace, gammas, alphas = _inputs(2, 20, 4, 20 + log_blowup)
+    want = orc.circle_commit(trace, log_blowup, gammas, alphas, keep_lde=True)
+    plan = native.CommitPlan(2, 20, log_blowup, 4)
+    plan.set_challenges(gammas, alphas)
+    plan.upload(trace)
+    plan.run()
+    got = plan.results()
+    assert np.array_equal(plan.lde(), want["lde"])
+    assert got["lde_root"] == want["lde_root"]
+    assert np.array_equal(got["layer_roots"], want["layer_roots"])
+    assert np.array_equal(got["final_layer"], want["final_layer"])
+    plan.close()
+
+
 def test_commit_full_size_matches_oracle(orc):
     """The 64 x 2^20 blowup-4 workload with 16 folds (2^22 -> 2^6), seeded inputs."""
     from zs_b200 import native
