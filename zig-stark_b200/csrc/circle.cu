@@ -348,11 +348,11 @@ __device__ __forceinline__ void low_chunk32(uint32_t* v, const uint32_t* __restr
 // The chunk's index bits never overlap the slot's, so element m sits at
 // padx(e0) + padx(m << B0): one runtime address per slot, immediate offsets after it.
 // Reads the groups from `src` and writes them to `dst` (the same layout; in place when
-// they are equal); with SCALE, multiplies every output by 2^scale_sh (a rotation).
-template <int R, bool INV, unsigned M, unsigned B0, bool SCALE = false>
+// they are equal).
+template <int R, bool INV, unsigned M, unsigned B0>
 __device__ __forceinline__ void chunk_ct(const uint32_t* src, uint32_t* dst, uint32_t gstride, unsigned G,
                                          unsigned shift, const uint32_t* __restrict__ TW, uint32_t n_dom,
-                                         const uint32_t* vb, unsigned scale_sh = 0) {
+                                         const uint32_t* vb) {
   constexpr unsigned SL = M - R;
   const uint32_t total = G << SL;
   for (uint32_t slot = threadIdx.x; slot < total; slot += blockDim.x) {
@@ -366,28 +366,25 @@ __device__ __forceinline__ void chunk_ct(const uint32_t* src, uint32_t* dst, uin
     const uint32_t Vh = (vb[gi] + e0) >> (B0 + R);
     chunk_layers<R, INV, 0>(v, TW, n_dom, B0 + shift, Vh);
 #pragma unroll
-    for (int m = 0; m < (1 << R); ++m)
-      dst[off + (m << B0) + ((m << B0) >> 5)] = SCALE ? mshl(v[m], scale_sh) : v[m];
+    for (int m = 0; m < (1 << R); ++m) dst[off + (m << B0) + ((m << B0) >> 5)] = v[m];
   }
 }
 
 // All M layers with a compile-time chunk schedule (chunks of <= 5 layers, the
 // largest first), DONE layers already applied. The first chunk reads `src`, every
-// chunk writes `dst`; with SCALE the last chunk multiplies its outputs by 2^scale_sh.
-template <bool INV, unsigned M, unsigned DONE, bool SCALE = false>
+// chunk writes `dst`.
+template <bool INV, unsigned M, unsigned DONE>
 __device__ __forceinline__ void run_layers_ct(const uint32_t* src, uint32_t* dst, uint32_t gstride, unsigned G,
-                                              unsigned shift, const uint32_t* TW, uint32_t n_dom, const uint32_t* vb,
-                                              unsigned scale_sh = 0) {
+                                              unsigned shift, const uint32_t* TW, uint32_t n_dom, const uint32_t* vb) {
   if constexpr (DONE < M) {
     constexpr unsigned REM = M - DONE;
     constexpr unsigned NCH = (REM + 4) / 5;
     constexpr unsigned R = (REM + NCH - 1) / NCH;
     // forward: top-down, the chunk covers [M - DONE - R, M - DONE); inverse: bottom-up
     constexpr unsigned B0 = INV ? DONE : M - DONE - R;
-    constexpr bool LAST = DONE + R == M;
-    chunk_ct<R, INV, M, B0, SCALE && LAST>(src, dst, gstride, G, shift, TW, n_dom, vb, scale_sh);
+    chunk_ct<R, INV, M, B0>(src, dst, gstride, G, shift, TW, n_dom, vb);
     __syncthreads();
-    run_layers_ct<INV, M, DONE + R, SCALE>(dst, dst, gstride, G, shift, TW, n_dom, vb, scale_sh);
+    run_layers_ct<INV, M, DONE + R>(dst, dst, gstride, G, shift, TW, n_dom, vb);
   }
 }
 
@@ -450,35 +447,16 @@ constexpr unsigned kLowThreads = 256;
 // size-2^LG transform split at K (groups of 2^K), hb = LG - K. Two orders:
 //   contiguous: element e of group t is global word gbase(t) + e;
 //   bit-reversed: element bitrev_K(v) of group t is global word (v << hb) + g0 + t.
-// KC, GC: 0, or K and G known at compile time with 2^K >= kLowThreads >= G and
-// kLowThreads / G = 2^a, K - a >= 5. Then a thread keeps one (t, low bits of v) or
-// one e for the whole batch and every other offset is a constant: in the bit-reversed
-// order, bitrev_K(vlo + (k << a)) = (bitrev_a(vlo) << (K - a)) | bitrev_(K-a)(k), and
-// padx() of a multiple of 32 plus r < 32 is padx of the first plus r.
-template <unsigned KC, unsigned GC>
 struct LowIO {
-  static constexpr bool kFast = KC != 0;
-  static constexpr unsigned A = kFast ? 31 - __builtin_clz(kLowThreads / GC) : 0;  // log2(threads / G)
-  static_assert(!kFast || ((1u << KC) >= kLowThreads && KC >= A + 5), "fast low-pass layout");
-
   // Calls f(smem offset, global offset) for every element of the bit-reversed order.
   template <typename F>
   __device__ __forceinline__ static void bitrev_order(unsigned K, unsigned G, unsigned hb, uint32_t g0, F&& f) {
-    if constexpr (kFast) {
-      const uint32_t t = threadIdx.x & (GC - 1), vlo = threadIdx.x >> (31 - __builtin_clz(GC));
-      const uint32_t s0 = t * group_stride(KC) + padx((vlo ? (__brev(vlo) >> (32 - A)) : 0u) << (KC - A));
-      const size_t g0v = ((size_t)vlo << hb) + g0 + t;
-      const size_t gstep = (size_t)1 << (A + hb);
-#pragma unroll
-      for (uint32_t k = 0; k < (1u << (KC - A)); ++k) f(s0 + cbitrev(k, KC - A), g0v + k * gstep);
-    } else {
-      const unsigned lg_g = 31 - __clz(G);
-      const uint32_t gstride = group_stride(K);
+    const unsigned lg_g = 31 - __clz(G);
+    const uint32_t gstride = group_stride(K);
 #pragma unroll 8
-      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-        const uint32_t t = idx & (G - 1), v = idx >> lg_g;
-        f(t * gstride + padx(bitrev(v, K)), ((size_t)v << hb) + g0 + t);
-      }
+    for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+      const uint32_t t = idx & (G - 1), v = idx >> lg_g;
+      f(t * gstride + padx(bitrev(v, K)), ((size_t)v << hb) + g0 + t);
     }
   }
 
@@ -486,22 +464,11 @@ struct LowIO {
   // gbase(t) gives group t's first global word.
   template <typename B, typename F>
   __device__ __forceinline__ static void contiguous_order(unsigned K, unsigned G, B&& gbase, F&& f) {
-    if constexpr (kFast) {
-      const uint32_t pt = padx(threadIdx.x);
-#pragma unroll
-      for (uint32_t t = 0; t < GC; ++t) {
-        const size_t gb = gbase(t) + threadIdx.x;
-#pragma unroll
-        for (uint32_t e = 0; e < (1u << KC); e += kLowThreads)
-          f(t * group_stride(KC) + pt + e + (e >> 5), gb + e);
-      }
-    } else {
-      const uint32_t gsz = 1u << K, gstride = group_stride(K);
+    const uint32_t gsz = 1u << K, gstride = group_stride(K);
 #pragma unroll 8
-      for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
-        const uint32_t t = idx >> K, e = idx & (gsz - 1);
-        f(t * gstride + padx(e), gbase(t) + e);
-      }
+    for (uint32_t idx = threadIdx.x; idx < (G << K); idx += blockDim.x) {
+      const uint32_t t = idx >> K, e = idx & (gsz - 1);
+      f(t * gstride + padx(e), gbase(t) + e);
     }
   }
 };
@@ -514,15 +481,15 @@ struct LowIO {
 //   forward: layers [0, K) of a size-2^LG transform over contiguous groups, then the
 //            reference's final bit reversal on the store (natural-order evaluations).
 // Shared memory: two buffers of G padded groups, then two G-entry arrays of virtual
-// group bases. KC, GC: the compile-time layout of LowIO (0, 0: K and G at run time).
-template <bool INV, unsigned KC = 0, unsigned GC = 0>
+// group bases. Groups of 2^10 with G = 8 run k_low10 instead.
+template <bool INV>
 __global__ void __launch_bounds__(kLowThreads, 3) k_low(const uint32_t* __restrict__ src, size_t src_stride,
                                                      uint32_t* __restrict__ dst, size_t dst_stride, unsigned LG,
                                                      unsigned K_, unsigned G_, unsigned iters,
                                                      const uint32_t* __restrict__ TW) {
   extern __shared__ uint32_t sm[];
-  using IO = LowIO<KC, GC>;
-  const unsigned K = KC ? KC : K_, G = GC ? GC : G_;
+  using IO = LowIO;
+  const unsigned K = K_, G = G_;
   const uint32_t N = 1u << LG, gstride = group_stride(K);
   const unsigned hb = LG - K;
   // buffer b at sm + b * G * gstride, its group bases at sm + 2 * G * gstride + b * G
@@ -558,10 +525,7 @@ __global__ void __launch_bounds__(kLowThreads, 3) k_low(const uint32_t* __restri
     uint32_t* s = buf(b);
     const uint32_t* vb = vbs(b);
     const uint32_t g0 = (batch0 + j) * G;
-    if constexpr (KC != 0)
-      run_layers_ct<INV, KC, 0>(s, s, gstride, G, 0, TW, N, vb);  // ends with a barrier
-    else
-      run_layers<INV>(s, gstride, G, K, 0, TW, N, vb);  // ends with a barrier
+    run_layers<INV>(s, gstride, G, K, 0, TW, N, vb);  // ends with a barrier
     if (INV) {
       IO::contiguous_order(
           K, G, [&](uint32_t t) { return (size_t)vb[t]; }, [&](uint32_t so, size_t go) { out[go] = s[so]; });
@@ -712,10 +676,9 @@ __device__ __forceinline__ void mid_order(unsigned K, unsigned M, unsigned G, ui
   }
 }
 
-// KC, MC, GC: the compile-time layout of mid_order (0, 0, 0: K, M and G at run time).
-// In the LDE mode with a compile-time layout, 1/n is applied by the last inverse chunk
-// and each quarter's first forward chunk reads the inverse result in s_in and writes
-// s_w, so s_in is neither rescaled nor copied in a pass of its own.
+// KC, MC, GC: the compile-time layout of mid_order (0, 0, 0: K, M and G at run time);
+// 10, 10, 8 (the 2^20-row LDE) runs the LDE mode in the register-direct layouts of
+// k_low10, with 1/n applied by the last inverse chunk.
 template <unsigned KC = 0, unsigned MC = 0, unsigned GC = 0>
 __global__ void __launch_bounds__(kMidThreads, 3) k_mid(const uint32_t* __restrict__ in, size_t in_stride,
                                                       uint32_t* __restrict__ out, size_t out_stride, unsigned L,
@@ -811,25 +774,17 @@ __global__ void __launch_bounds__(kMidThreads, 3) k_mid(const uint32_t* __restri
     }
     return;
   }
-  if constexpr (FAST) {
-    run_layers_ct<true, MC, 0, true>(s_in, s_in, gstride, G, K, ITW_small, n, vb, inv_n_shift);
-  } else {
-    run_layers<true>(s_in, gstride, G, M, K, ITW_small, n, vb);
-    mid_order<0, 0, 0>(K, M, G, lo0, [&](uint32_t so, size_t) { s_in[so] = mshl(s_in[so], inv_n_shift); });
-    __syncthreads();
-  }
+  // the LDE with a run-time layout (the compile-time layout returned above)
+  run_layers<true>(s_in, gstride, G, M, K, ITW_small, n, vb);
+  mid_order<0, 0, 0>(K, M, G, lo0, [&](uint32_t so, size_t) { s_in[so] = mshl(s_in[so], inv_n_shift); });
+  __syncthreads();
   for (uint32_t q = 0; q < (1u << B); ++q) {
     if (threadIdx.x < G) vb[threadIdx.x] = q << M;
-    if constexpr (FAST) {
-      __syncthreads();
-      run_layers_ct<false, MC, 0>(s_in, s_w, gstride, G, K, TW_big, n << B, vb);
-    } else {
-      for (uint32_t idx = threadIdx.x; idx < G * gstride; idx += blockDim.x) s_w[idx] = s_in[idx];
-      __syncthreads();
-      run_layers<false>(s_w, gstride, G, M, K, TW_big, n << B, vb);
-    }
+    for (uint32_t idx = threadIdx.x; idx < G * gstride; idx += blockDim.x) s_w[idx] = s_in[idx];
+    __syncthreads();
+    run_layers<false>(s_w, gstride, G, M, K, TW_big, n << B, vb);
     uint32_t* dq = dst + (size_t)q * n;
-    mid_order<KC, MC, GC>(K, M, G, lo0, [&](uint32_t so, size_t go) { dq[go] = s_w[so]; });
+    mid_order<0, 0, 0>(K, M, G, lo0, [&](uint32_t so, size_t go) { dq[go] = s_w[so]; });
     __syncthreads();
   }
 }
