@@ -667,7 +667,7 @@ def binius_metrics(clock_mhz):
                           "achieved": achieved, "peak": peak, "unit": "lookups/s", "frac": achieved / peak,
                           "peak_basis": f"{sms} SMs x 32 lanes x {clock_mhz:.0f} MHz",
                           # shared-memory wavefronts per warp lookup at random addresses,
-                          # from the committed capture (profiles/binius_sumcheck_round.md)
+                          # from an ncu capture of the round kernels at these sizes
                           "wavefronts_per_lookup": wavefronts[bits],
                           "frac_of_bank_conflict_ceiling": achieved / peak * wavefronts[bits]}}
         if ref_gpu.sumcheck_available():
@@ -891,9 +891,9 @@ def main():
     # cycle at the sampled SM clock) and against the ALU pipe's (a warp instruction every
     # other cycle per scheduler), with the warp instructions that ncu counted for the
     # phase's kernels on this workload (smsp__inst_executed.sum and
-    # sm__inst_executed_pipe_alu.sum of one step at 64 x 2^20; the capture and the
-    # per-kernel figures are in profiles/circle_commit_64x2p20.md), over the CUDA-event
-    # phase time of this run. Other row counts scale the counts by the rows (marked).
+    # sm__inst_executed_pipe_alu.sum of one captured step at 64 x 2^20, summed over each
+    # phase's kernels), over the CUDA-event phase time of this run. Other row counts
+    # scale the counts by the rows (marked).
     counted = {"lde": (946.8e6, 488.4e6), "row_tree": (1059.4e6, 735.3e6), "folds": (342.0e6, 237.1e6)}
     cs = clocks.summary()
     sm_mhz = cs.get("sm_mhz") or cs.get("sm_max_mhz") or 1965.0
@@ -903,7 +903,7 @@ def main():
     int_roof = {"bound": "integer issue", "unit": "warp instructions/s", "issue_peak": issue_peak,
                 "alu_pipe_peak": issue_peak / 2,
                 "source": "ncu counters of this workload's kernels (smsp__inst_executed.sum, "
-                          "sm__inst_executed_pipe_alu.sum), profiles/circle_commit_64x2p20.md"
+                          "sm__inst_executed_pipe_alu.sum) from one captured step at 64 x 2^20"
                           + ("" if log_rows == LOG_ROWS else f"; scaled by 2^{log_rows - LOG_ROWS} rows"),
                 "phases": {}}
     for k, (inst, alu) in counted.items():
